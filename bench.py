@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""bench.py -- MAS-PCG Newton-step solve on one B200 per rank.
+
+A step is one full Newton-step linear solve of the contact workload (two
+40x20x20 tet blocks stacked 1e-4 m apart, 50,000 point-triangle barrier
+pairs, 96,000 DOF): MAS hierarchy rebuild + Hessian scatter + subdomain
+inverses + PCG to 1e-4 relative residual ||b-Ax||/||b|| (reference stopping
+rule: tested every 10 iterations, true residual).  Inputs are seeded
+synthetic data of the benchmark's shapes.  The headline `value` is the mixed
+precision solve (BF16 subdomain inverses, FP32 apply, FP64 CG); the plain
+FP64 MAS-PCG, the reference-precision FP32 MAS-PCG and block-Jacobi PCG are
+timed beside it.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank solves its own replica (replicas only: one system
+does not shard); times are device times (CUDA events), max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "stiff-gipc_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "MAS-PCG solve ms to 1e-4 rel. residual: learned/mixed vs plain, same B200"
+WORKLOAD = "two 40x20x20-vertex tet blocks 1e-4 m apart + 50k point-triangle barrier pairs (32,000 verts, 96,000 DOF)"
+REL_TOL = 1e-4
+MAX_ITER = 5000  # cap (the reference default is the DOF count); a variant that hits it reports converged=false
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="sgmas", choices=["sgmas", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = benchmark size)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--variants", default="bf16,fp64,fp32,jacobi")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.idx = gpu_index
+        self.p = None
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            t = [x.strip() for x in line.split(",")]
+            if len(t) < 9:
+                continue
+            try:
+                sm.append(float(t[1]))
+                mx = max(mx, float(t[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, t[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        busy = [v for v in sm if v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_problem(scale, seed=0):
+    from sgmas import synth
+    return synth.config2(seed=seed, scale=scale)
+
+
+# ---------------------------------------------------------------------------
+def algorithmic_bytes(s, info, precision):
+    """Bytes each kernel of one PCG iteration must move at minimum:
+    SpMV: upper blocks once (72 B values + 8 B indices) + z, p_old read, p_new, Ap written (8 B/DOF each);
+    update+level-0 MAS: x, p, r, Ap read + x, r written (8 B/DOF each), level-0 inverse tiles,
+    slot map + masks (8 B/slot), level-0 Z written (3 Acc/slot);
+    coarse Schwarz: coarse inverse tiles + coarse R read + Z written;
+    collect: Z over L levels, slot + coarse tables, z written, r read."""
+    n = 3 * s.n_verts
+    nb = len(s.rows)
+    es = {"fp32": 4, "bf16": 2, "fp64": 8}[precision]
+    acc = 8 if precision == "fp64" else 4
+    B = 16
+    bs = B * (B + 1) // 2 * 9
+    Mm = info["part_map_size"]
+    total = info["total"]
+    L = info["levelnum"]
+    coarse = total - Mm
+    N = s.n_verts
+    return {
+        "spmv": nb * 80 + 4 * 8 * n,
+        "update_l0": 6 * 8 * n + (Mm // B) * bs * es + 8 * Mm + 3 * acc * Mm,
+        "coarse": (coarse // B) * bs * es + 2 * 3 * acc * coarse,
+        "collect": 3 * acc * L * N + 4 * N + 4 * (L - 1) * N + 8 * n + 8 * n,
+    }
+
+
+def run_sgmas(args):
+    import torch
+    import sgmas
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    t0 = time.time()
+    s = build_problem(args.scale, seed=rank)
+    gen_s = time.time() - t0
+
+    def tdev(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    vals, rows, cols, b = tdev(s.vals), tdev(s.rows), tdev(s.cols), tdev(s.b)
+    pairs = tdev(s.pairs)
+    dpos = tdev(s.pos)
+    nb_start, nb_num, nb_list = sgmas.vert_neighbors(s.tets, s.n_verts)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    ctxs = {}
+
+    def make(precision):
+        ctx = sgmas.Context(local, bank=16, precision=precision)
+        ctx.set_stream(stream.cuda_stream)
+        pm, rm = ctx.morton_partition(dpos)
+        ctx.mas_init(s.n_verts, nb_start, nb_num, nb_list, pm, rm)
+        ctx.mas_set_contacts(pairs, len(s.pairs))
+        return ctx, len(pm)
+
+    variants = [v for v in args.variants.split(",") if v]
+    results = {}
+    A_full = None
+    clocks = Clocks(local)
+    gpu_launches = None
+    for v in variants:
+        precision = v if v in ("fp32", "bf16", "fp64") else "fp32"
+        precond = "jacobi" if v == "jacobi" else "mas"
+        ctx, pms = make(precision)
+        ctxs[v] = (ctx, pms)
+        x = torch.zeros_like(b)
+        try:
+            for _ in range(args.warmup):
+                rep = ctx.pcg_solve(vals, rows, cols, s.n_verts, b, x, rel_tol=REL_TOL, max_iter=MAX_ITER,
+                                    preconditioner=precond)
+        except sgmas.SgmasError as e:   # same data on every rank: all ranks skip together
+            results[v] = {"error": str(e)}
+            continue
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        times, iters, launches = [], [], []
+        first = not any("ms" in r for r in results.values())
+        if first:
+            clocks.start()
+        for _ in range(args.steps):
+            flush.zero_()                      # L2 flushed between timed steps
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rep = ctx.pcg_solve(vals, rows, cols, s.n_verts, b, x, rel_tol=REL_TOL, max_iter=MAX_ITER, preconditioner=precond)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            iters.append(rep["iterations"])
+            launches.append(rep["kernel_launches"])
+        if first:
+            ck = clocks.stop()
+        torch.cuda.synchronize()
+        # verify: true relative residual of the last solution
+        y = torch.zeros_like(b)
+        ctx.spmv(1.0, vals, rows, cols, s.n_verts, x, 0.0, y)
+        res = float(torch.linalg.norm(b - y) / torch.linalg.norm(b))
+        ms = statistics.mean(times)
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        results[v] = {"ms": ms, "ms_min": min(times), "ms_max": max(times), "iterations": int(statistics.median(iters)),
+                      "rel_residual": res, "converged": bool(rep["converged"]),
+                      "precond_build_ms": rep["precond_ms"], "pcg_graph_ms": rep["solve_ms"],
+                      "kernel_launches": int(statistics.median(launches))}
+        if first:
+            gpu_launches = int(sum(launches))
+            clocks_rec = ck
+    ok = [v for v in variants if "ms" in results.get(v, {}) and results[v]["converged"]]
+    head = ok[0] if ok else next(v for v in variants if "ms" in results.get(v, {}))
+    # ---- per-kernel times and roofline of the headline variant ----
+    ctx, pms = ctxs[head]
+    precision = head if head in ("fp32", "bf16", "fp64") else "fp32"
+    x = torch.zeros_like(b)
+    ctx.pcg_solve(vals, rows, cols, s.n_verts, b, x, rel_tol=REL_TOL, preconditioner="mas" if head != "jacobi" else "jacobi")
+    kms = ctx.pcg_profile(reps=50)
+    info = ctx.mas_info()
+    info["part_map_size"] = pms
+    abytes = algorithmic_bytes(s, info, precision)
+    dom = max(kms, key=lambda k: kms[k])
+    hbm, peak_kind = peaks()
+    achieved = abytes[dom] / (kms[dom] * 1e-3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            traffic = json.load(f).get(f"{dom}_{precision}")
+    except Exception:
+        pass
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": f"{peak_kind} HBM copy",
+                "algorithmic_bytes": abytes[dom], "kernel_ms": kms[dom], "kernel_ms_all": kms,
+                "note": "per-iteration working set < 126 MB L2: achieved can exceed the HBM copy peak"}
+    # ---- e2e through the public API with host buffers ----
+    e2e = run_e2e(args, ctx, s, dev, stream, head)
+    out = {"metric": METRIC, "value": round(results[head]["ms"], 4), "unit": "ms", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(results[head]["ms"], 4),
+           "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+           "dtype": {"bf16": "f64+bf16", "fp32": "f64+f32", "fp64": "f64", "jacobi": "f64"}[head],
+           "data": "synthetic",
+           "config": {"workload": WORKLOAD, "scale": args.scale, "rel_tol": REL_TOL,
+                      "headline": f"{head} MAS-PCG", "partition": "Morton order, 16-vertex subdomains",
+                      "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{world}",
+                      "n_blocks": int(len(s.rows)), "n_pairs": int(len(s.pairs)), "gen_s": round(gen_s, 1)},
+           "variants": results,
+           "speedup_vs_plain_fp64": (round(results["fp64"]["ms"] / results[head]["ms"], 3)
+                                     if "ms" in results.get("fp64", {}) else None),
+           "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "clocks": clocks_rec}
+    if rank == 0 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(s, results)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    for ctx, _ in ctxs.values():
+        ctx.close()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def run_e2e(args, ctx, s, dev, stream, head):
+    """Same solve through the public API with host inputs: H2D of the matrix,
+    right-hand side and contact pairs from pinned memory, the solve, D2H of x."""
+    import torch
+    h = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+         for k, a in (("vals", s.vals), ("rows", s.rows), ("cols", s.cols), ("b", s.b), ("pairs", s.pairs))}
+    d = {k: torch.empty_like(t, device=dev) for k, t in h.items()}
+    hx = torch.empty_like(h["b"]).pin_memory()
+    dx = torch.empty_like(d["b"])
+    ctx.mas_set_contacts(d["pairs"], len(s.pairs))
+    precond = "jacobi" if head == "jacobi" else "mas"
+    times = []
+    for it in range(args.warmup + args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in d:
+            d[k].copy_(h[k], non_blocking=True)
+        ctx.pcg_solve(d["vals"], d["rows"], d["cols"], s.n_verts, d["b"], dx, rel_tol=REL_TOL, max_iter=MAX_ITER, preconditioner=precond)
+        hx.copy_(dx, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if it >= args.warmup:
+            times.append(e0.elapsed_time(e1))
+    h2d = sum(t.numel() * t.element_size() for t in h.values())
+    return {"value": round(statistics.mean(times), 4), "unit": "ms", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(hx.numel() * hx.element_size())}
+
+
+def cpu_baseline(s, results):
+    """The oracle port of the reference's MAS-PCG (FP64 CG, FP32 MAS, the
+    reference stopping rule) on this host's cores: one full solve of the same
+    system (preconditioner build + PCG)."""
+    from oracle import oracle as O
+    nthreads = O.lib().or_omp_max_threads()
+    pm, rm = O.morton_partition(s.pos)
+    st, nn, nl = O.vert_neighbors(s.tets, s.n_verts)
+    t0 = time.perf_counter()
+    m = O.MAS(s.n_verts, st, nn, nl, pm, rm)
+    m.reorder(s.pairs)
+    m.assemble(s.vals, s.rows, s.cols, precision=0)
+    t1 = time.perf_counter()
+    x, rep = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=2, rel_tol=REL_TOL, mas=m, nthreads=nthreads, max_iter=MAX_ITER)
+    t2 = time.perf_counter()
+    tj = time.perf_counter()
+    xj, repj = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=1, rel_tol=REL_TOL, nthreads=nthreads, max_iter=MAX_ITER)
+    tj = time.perf_counter() - tj
+    return {"value": round((t2 - t0) * 1e3, 1), "unit": "ms", "cores": nthreads, "kind": "port",
+            "sample": "one full solve of the benchmark system: MAS build + FP64 PCG with FP32 MAS to 1e-4",
+            "iterations": rep["iterations"], "rel_residual": rep["rel_residual"],
+            "build_ms": round((t1 - t0) * 1e3, 1),
+            "jacobi_pcg": {"ms": round(tj * 1e3, 1), "iterations": repj["iterations"]}}
+
+
+def run_reference(args):
+    """--impl reference: the reference's own algorithm on the host cores (the
+    reference cannot be built here -- its device code needs Eigen -- so this
+    is the oracle port of PCGSolver::pcg + MASPreconditioner, OpenMP)."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    s = build_problem(args.scale, seed=0)
+    nthreads = O.lib().or_omp_max_threads()
+    pm, rm = O.morton_partition(s.pos)
+    st, nn, nl = O.vert_neighbors(s.tets, s.n_verts)
+    times, iters = [], []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        m = O.MAS(s.n_verts, st, nn, nl, pm, rm)
+        m.reorder(s.pairs)
+        m.assemble(s.vals, s.rows, s.cols, precision=0)
+        x, rep = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=2, rel_tol=REL_TOL, mas=m, nthreads=nthreads, max_iter=MAX_ITER)
+        dt = (time.perf_counter() - t0) * 1e3
+        if it >= args.warmup:
+            times.append(dt)
+            iters.append(rep["iterations"])
+    ms = statistics.mean(times)
+    sample = "full solves of the benchmark system (MAS build + FP64 PCG with FP32 MAS to 1e-4), OpenMP"
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": round(ms, 2), "unit": "ms", "n_gpus": world,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2),
+                      "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+                      "data": "synthetic",
+                      "config": {"workload": WORKLOAD, "scale": args.scale, "rel_tol": REL_TOL},
+                      "iterations": int(statistics.median(iters)),
+                      "cpu_baseline": {"value": round(ms, 2), "unit": "ms", "cores": nthreads, "kind": "port",
+                                       "sample": sample},
+                      "e2e": {"value": round(ms, 2), "unit": "ms", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_sgmas(args)
+
+
+if __name__ == "__main__":
+    main()

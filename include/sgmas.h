@@ -1,0 +1,180 @@
+/*
+ * sgmas.h -- C-ABI of the B200-native MAS-PCG Newton-step solve.
+ *
+ * Drop-in boundary for StiffGIPC's linear solve (paths below are relative to
+ * the StiffGIPC project; "SG/" = StiffGIPC/).  Every entry point returns
+ * SGMAS_OK (0) or a negative status and never aborts; sgmas_last_error()
+ * gives the message.  Device pointers ("d_") are borrowed for the duration of
+ * the call (or until replaced, for contact pairs); the context owns its
+ * internal arrays.  Calls on one context are stream-ordered on the context's
+ * stream and are not re-entrant.
+ *
+ * Matrix layout (GIPCTripletMatrix, SG/linear_system/linear_system/
+ * global_matrix.h:18-203): merged upper-triangular 3x3 block COO, sorted by
+ * (row, col), row <= col, values 9 doubles column-major per block
+ * (Eigen::Matrix3d), rows/cols int32 block indices.  Vectors are double[3n].
+ */
+#ifndef SGMAS_H
+#define SGMAS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SGMAS_OK 0
+#define SGMAS_ERR_ARG -1      /* invalid argument */
+#define SGMAS_ERR_CUDA -2     /* CUDA runtime error */
+#define SGMAS_ERR_STATE -3    /* call out of order (e.g. apply before assemble) */
+#define SGMAS_ERR_CAPACITY -4 /* a size exceeds an allocated or stated maximum */
+#define SGMAS_ERR_DEVICE -5   /* a kernel reported an error (bounded wait expired, bad index) */
+#define SGMAS_ERR_NUMERIC -6  /* non-finite value in the solve */
+
+typedef struct sgmas_context sgmas_context;
+
+/* precision of the stored subdomain inverses and of the MAS apply */
+#define SGMAS_MAS_FP32 0 /* reference parity: FP64 build, FP32 inverses and apply */
+#define SGMAS_MAS_BF16 1 /* BF16 inverses, FP32 accumulate */
+#define SGMAS_MAS_FP64 2 /* FP64 inverses and apply (plain FP64 MAS-PCG) */
+
+typedef struct {
+    int device;        /* CUDA device ordinal */
+    int bank_size;     /* subdomain size; 16 = BANKSIZE (SG/eigen_data.h:17) */
+    int mas_precision; /* SGMAS_MAS_* */
+} sgmas_config;
+
+/* gipc::PCGSolverConfig (SG/linear_system/solver/pcg_solver.h:6-15) plus the
+ * preconditioner selection of GIPC::create_LinearSystem (SG/gipc/gipc.cu:42-73). */
+typedef struct {
+    int max_iter;                /* 0 -> number of DOF, as the reference */
+    double rel_tol;
+    double abs_tol;
+    int use_preconditioned_norm; /* 1: r.z <= rel^2 r0.z0; 0: ||r||^2 <= rel^2 ||r0||^2 */
+    int preconditioner;          /* 0: 3x3 block-Jacobi (P_type 0); 1: MAS (P_type 1) */
+    int abd_bodies;              /* 12x12 block-Jacobi on block rows [0, 4*abd_bodies) */
+    int fem_offset;              /* first FEM block row (MAS sub-range) */
+    int check_every;             /* convergence-test cadence; 10 = reference (pcg_solver.cu:240,260) */
+} sgmas_pcg_config;
+
+typedef struct {
+    int iterations;      /* value returned by PCGSolver::pcg (pcg_solver.cu:303) */
+    int converged;
+    double rz0, rr0;     /* initial r.z and r.r */
+    double rr_last;      /* r.r at the last convergence test */
+    float solve_ms;      /* device time of the PCG loop (CUDA events) */
+    float precond_ms;    /* device time of the preconditioner build */
+    int kernel_launches; /* kernels this solve launched (graph nodes executed) */
+} sgmas_pcg_report;
+
+/* One BCOO matrix on the device (borrowed). */
+typedef struct {
+    const double* d_values; /* [n_blocks][9], column-major 3x3 */
+    const int* d_rows;
+    const int* d_cols;
+    int n_blocks;
+    int n_block_rows;       /* block rows = DOF / 3 */
+} sgmas_bcoo;
+
+/* ---- context ---------------------------------------------------------- */
+int sgmas_create(const sgmas_config* cfg, sgmas_context** out);
+/* MASPreconditioner::FreeMAS (SG/MASPreconditioner.cu:2321-2350) + release */
+void sgmas_destroy(sgmas_context* ctx);
+const char* sgmas_last_error(const sgmas_context* ctx);
+/* the reference runs on the per-thread default stream (CMakeLists.txt:101) */
+int sgmas_set_stream(sgmas_context* ctx, void* cuda_stream);
+int sgmas_synchronize(sgmas_context* ctx);
+
+/* ---- MASPreconditioner (SG/MASPreconditioner.cuh:14-102) --------------- */
+/* initPreconditioner_Neighbor (:2253-2290) + the uploads of the public
+ * neighbour / slot-map arrays done by the caller at SG/main.cu:998-1027 +
+ * initPreconditioner_Matrix (:2292-2319).  Host arrays; neighbour CSR as
+ * tetrahedra_obj::getVertNeighbors (SG/load_mesh.cpp:894-999); slot maps as
+ * setMAS_partition (SG/main.cu:47-75). */
+int sgmas_mas_init(sgmas_context* ctx, int vert_num, int collision_node_offset,
+                   int neighbor_list_size, const unsigned* neighbor_list,
+                   const unsigned* neighbor_start, const unsigned* neighbor_num,
+                   const int* part_map, int part_map_size, const int* real_map);
+/* the int4 contact pairs the reference keeps as _collisonPairs (device, borrowed) */
+int sgmas_mas_set_contacts(sgmas_context* ctx, const int* d_pairs_int4, int cp_num);
+/* setPreconditioner_bcoo (:2169-2207): hierarchy rebuild + Hessian scatter +
+ * dense subdomain inverses.  d_indices selects the FEM blocks (NULL = every
+ * block whose row and column lie in [offset, offset + vert_num)). */
+int sgmas_mas_assemble(sgmas_context* ctx, const double* d_values, const int* d_rows,
+                       const int* d_cols, const uint32_t* d_indices, int offset,
+                       int triplet_num, int cp_num);
+/* preconditioning (:2210-2251): d_z = MAS(d_r) over the FEM range */
+int sgmas_mas_apply(sgmas_context* ctx, const double* d_r, double* d_z);
+int sgmas_mas_info(sgmas_context* ctx, int* levelnum, int* total_clusters, int* n_mas_blocks);
+/* copies of the hierarchy tables (host arrays, any may be NULL): fine_mask[N],
+ * coarse_space[levelnum*N], going_next[cap], level_size[2*(levelnum+1)],
+ * prefix_orig[part_map_size/bank], coarse_table[6*N] */
+int sgmas_mas_download_tables(sgmas_context* ctx, unsigned* fine_mask, int* coarse_space,
+                              int* going_next, int going_next_cap, int* level_size,
+                              int* prefix_orig, int* coarse_table);
+/* assembled FP64 subdomain matrices and their inverses as stored
+ * (float for FP32 / BF16 widened to float, double for FP64); host arrays of
+ * n_mas_blocks * bank*(bank+1)/2 * 9 entries */
+int sgmas_mas_download_matrices(sgmas_context* ctx, double* hess64, double* inv_as_double);
+/* invert host FP64 packed subdomain matrices with the device kernel (tests) */
+int sgmas_mas_invert_host(sgmas_context* ctx, const double* hess64, int nblocks, double* inv64);
+
+/* ---- PCGSolver (SG/linear_system/solver/pcg_solver.cu:155-304) -------- */
+/* x = 0, then PCG on the device with device-side scalars; the whole loop is
+ * one CUDA graph (conditional WHILE node).  Requires sgmas_mas_init (and
+ * assembles the MAS itself) when cfg->preconditioner == 1. */
+int sgmas_pcg_solve(sgmas_context* ctx, const sgmas_bcoo* A, const double* d_b, double* d_x,
+                    const sgmas_pcg_config* cfg, sgmas_pcg_report* report);
+/* the same with host arrays: uploads A and b, solves, downloads x */
+int sgmas_pcg_solve_host(sgmas_context* ctx, const double* values, const int* rows,
+                         const int* cols, int n_blocks, int n_block_rows, const double* b,
+                         double* x, const sgmas_pcg_config* cfg, sgmas_pcg_report* report);
+
+/* Device time of each kernel of one PCG iteration, replayed `reps` times on
+ * the buffers of the last sgmas_pcg_solve (which it overwrites): ms[0] SpMV
+ * with the fused p update and p.Ap, ms[1] update + level-0 MAS (or the
+ * block-Jacobi tail), ms[2] coarse Schwarz, ms[3] CollectFinalZ + r.z. */
+int sgmas_pcg_profile(sgmas_context* ctx, int reps, float* ms, int n_ms);
+
+/* ---- MAS set-up data on the host (no GPU needed) ----------------------- */
+/* tetrahedra_obj::getVertNeighbors (SG/load_mesh.cpp:894-999): undirected
+ * edges of the tets and triangles (global ids, FEM vertices from
+ * abd_vert_offset) -> neighbour CSR; returns the list size or a negative
+ * status.  nb_start/nb_num have n_verts entries, nb_list nb_cap. */
+int sgmas_vert_neighbors(const int* tets, int n_tets, const int* tris, int n_tris, int n_verts,
+                         int abd_vert_offset, unsigned* nb_start, unsigned* nb_num, unsigned* nb_list,
+                         int nb_cap);
+/* setMAS_partition (SG/main.cu:47-75) after load_parts (SG/load_mesh.cpp:449-480):
+ * part ids (sorted-mesh order) -> part_map[part_offset*bank], real_map[n] */
+int sgmas_part_maps(const int* part_id, int n, int bank, int* part_map, int part_map_cap,
+                    int* part_map_size, int* real_map);
+
+/* ---- kernels of the path, callable on their own ------------------------ */
+/* Spmv::warp_reduce_sym_spmv (SG/linear_system/utils/spmv.cu:8-133): y = a A x + b y */
+int sgmas_spmv(sgmas_context* ctx, double a, const sgmas_bcoo* A, const double* d_x, double b,
+               double* d_y);
+/* Converter::convert (SG/linear_system/utils/converter.cu:23-189): raw
+ * triplets -> merged sorted BCOO; *n_unique receives the merged count
+ * (h_unique_key_number, global_matrix.h:197).  Outputs need n entries. */
+int sgmas_convert(sgmas_context* ctx, const double* d_values, const int* d_rows, const int* d_cols,
+                  int n, double* d_out_values, int* d_out_rows, int* d_out_cols, int* n_unique);
+/* write_triplet_fem / write_triplet<12,12> with SymGH (SG/femEnergy.cu:14-62,
+ * SG/GIPC.cu:82-139): element matrices [n_elem][3k][3k] row-major with node
+ * lists [n_elem][k] -> k(k+1)/2 upper triplets per element */
+int sgmas_write_upper_blocks(sgmas_context* ctx, const double* d_H, int n_elem, int nodes_per_elem,
+                             const int* d_nodes, double* d_values, int* d_rows, int* d_cols);
+/* _calcVertMChash (SG/GIPC.cu:412-461, hash_code type -1 at :142-168):
+ * (morton30 << 32) | vertex index; aabb = {lo.xyz, hi.xyz} or NULL for the
+ * vertices' own bounding box */
+int sgmas_morton_codes(sgmas_context* ctx, const double* d_pos, int n, const double* aabb,
+                       uint64_t* d_codes);
+/* Morton order cut into bank-size subdomains: slot maps in the layout of
+ * setMAS_partition (part_map[part_map_size], real_map[n]; host arrays) */
+int sgmas_morton_partition(sgmas_context* ctx, const double* d_pos, int n, int* part_map,
+                           int part_map_cap, int* part_map_size, int* real_map);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,151 @@
+// ctx.hpp -- the opaque context behind the sgmas C-ABI (host side).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "common.cuh"
+
+struct PcgState {
+    double rz, rz0, rr0, rr, pAp, alpha, beta, rz_new;
+    int k, done, iters, converged;
+    int max_iter, check_every;
+    double rel2, abs2;
+    int use_prec_norm, pad;
+};
+
+struct PcgRunCfgLite {
+    int precond, abd_bodies, valid;
+};
+
+struct BsrMatrix {
+    int nrows = 0, nblocks = 0;       // upper blocks in
+    long long nnz_pad = 0, cap = 0;   // full (both triangles), rows padded to even length
+    int* row_ptr = nullptr;           // [nrows + 1]
+    int* cols = nullptr;              // [cap]
+    uint32_t* src = nullptr;          // [cap] source block | transposed bit
+    double* vals = nullptr;           // 9 * cap, SoA: vals[q * cap + p], row-major component q
+    int* cnt = nullptr;               // [nrows] entries per row
+    int* cnt_lower = nullptr;         // [nrows]
+    int* fill = nullptr;              // [nrows]
+    int* first = nullptr;             // [nrows] first upper block of each row
+    int rows_cap = 0;
+};
+
+struct sgmas_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;      // stream all work is ordered on
+    cudaStream_t cap_stream = nullptr;  // the context's own stream (default)
+    cudaStream_t rec_stream = nullptr;  // graph recording
+    std::string err;
+    int bank = 16;
+    int precision = 0;
+    int* d_err = nullptr;             // device error flag
+
+    // ---- MAS setup ----
+    bool mas_init = false, mas_assembled = false;
+    int N = 0, Mm = 0, L = 0, node_offset = 0, nb_size = 0;
+    unsigned *d_nb_list0 = nullptr, *d_nb_num0 = nullptr, *d_nb_start = nullptr;
+    unsigned *d_nb_list = nullptr, *d_nb_num = nullptr;
+    int *d_part_map = nullptr, *d_real_map = nullptr;
+    unsigned *d_fine_mask = nullptr, *d_next_mask = nullptr;
+    int *d_prefix_orig = nullptr;     // level-0 clusters per bank
+    int *d_bank_cnt = nullptr, *d_bank_pre = nullptr;  // per-level scratch
+    int *d_coarse_space = nullptr, *d_going_next = nullptr;
+    int gn_cap = 0;
+    int *d_level_size = nullptr;      // 2 * (kMaxLevels + 2)
+    int h_level_size[2 * (sgmas::kMaxLevels + 2)] = {0};
+    int *d_coarse_table = nullptr;    // 6 * N
+    int total = 0, cap_total = 0;     // clusters (nodes over all levels)
+    double* d_hess = nullptr;         // [cap_total / bank][bsym][9]
+    void* d_inv = nullptr;            // same shape in the storage precision
+    void* d_R = nullptr;              // 3 * cap_total accumulators
+    void* d_Z = nullptr;
+    const int* d_pairs = nullptr;
+    int cp_num = 0;
+    int mas_launches = 0;             // kernels per apply
+    int apply_parts = 7;              // which apply kernels to launch (profiling)
+
+    // ---- PCG ----
+    BsrMatrix bsr;
+    double *d_r = nullptr, *d_z = nullptr, *d_p0 = nullptr, *d_p1 = nullptr, *d_Ap = nullptr;
+    double* d_diag_inv = nullptr;     // 9 * nrows (3x3 block-Jacobi)
+    double* d_abd_inv = nullptr;      // 144 * bodies
+    int vec_cap = 0, diag_cap = 0, abd_cap = 0;
+    double* d_partials = nullptr;     // reduction partials
+    unsigned* d_ticket = nullptr;
+    int partial_cap = 0;
+    PcgState* d_state = nullptr;
+    // uploaded host systems (sgmas_pcg_solve_host)
+    double *d_hvals = nullptr, *d_hb = nullptr, *d_hx = nullptr;
+    int *d_hrows = nullptr, *d_hcols = nullptr;
+    long long hcap_blocks = 0, hcap_vec = 0;
+    // graph cache
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    unsigned long long graph_key[8] = {0};
+    int graph_kernels_prologue = 0, graph_kernels_body = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    PcgRunCfgLite last_cfg = {0, 0, 0};
+    const double* last_b = nullptr;
+    double* last_x = nullptr;
+    bool solved = false;
+    // converter scratch
+    void* d_sort_scratch = nullptr;
+    size_t sort_scratch_bytes = 0;
+};
+
+// error helpers
+int ctx_fail(sgmas_context* c, int code, const char* fmt, ...);
+#define SG_CUDA(c, expr)                                                                      \
+    do {                                                                                      \
+        cudaError_t _e = (expr);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            return ctx_fail((c), SGMAS_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #expr, \
+                            cudaGetErrorString(_e));                                          \
+    } while (0)
+
+template <typename T>
+int ctx_alloc(sgmas_context* c, T** p, size_t count) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) return ctx_fail(c, -2, "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+    return 0;
+}
+
+struct PcgRunCfg {
+    int max_iter;
+    double rel_tol, abs_tol;
+    int use_prec_norm;
+    int precond;       // 0 Jacobi, 1 MAS
+    int abd_bodies;
+    int fem_offset;
+    int check_every;
+};
+
+// internal entry points across translation units
+int mas_build_hierarchy(sgmas_context* c);   // ReorderRealtime on the device
+int mas_scatter_and_invert(sgmas_context* c, const double* vals, const int* rows, const int* cols,
+                           const uint32_t* indices, int offset, int n);
+int mas_launch_apply(sgmas_context* c, const double* r, double* z, int mode, const PcgState* st,
+                     double* x, const double* p, const double* Ap, double* partials, unsigned* ticket,
+                     int iter_kind, unsigned long long cond_handle, int* launches);
+int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* cols, int nblocks,
+              int nrows);
+int bsr_spmv_plain(sgmas_context* c, double a, const double* x, double b, double* y);
+int bcoo_spmv_ref(sgmas_context* c, double a, const double* vals, const int* rows, const int* cols,
+                  int nblocks, int nrows, const double* x, double b, double* y);
+int pcg_run(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg,
+            float* solve_ms, int* launches);
+int convert_triplets(sgmas_context* c, const double* vals, const int* rows, const int* cols, int n,
+                     double* out_vals, int* out_rows, int* out_cols, int* n_unique);
+int write_upper_blocks(sgmas_context* c, const double* H, int n_elem, int k, const int* nodes,
+                       double* vals, int* rows, int* cols);
+int morton_codes(sgmas_context* c, const double* pos, int n, const double* aabb, uint64_t* codes);
+int sort_u64_pairs(sgmas_context* c, uint64_t* keys, uint32_t* vals, int n, int key_bits);
+int mas_invert_blocks_dev(sgmas_context* c, const double* hess, int nblk, double* out64);
+int pcg_profile(sgmas_context* c, int reps, float* ms, int n_ms);
+

@@ -1,0 +1,846 @@
+// mas.cu -- MAS preconditioner on sm_100a: hierarchy build, Hessian scatter,
+// dense subdomain inverses and the apply.
+//
+// Restates SG/MASPreconditioner.cu (StiffGIPC) with a B200 layout:
+//  * a subdomain ("bank") of B=16 slots is a half-warp; bank-local masks,
+//    closures, cluster counts and ids use shuffles and ballots instead of the
+//    reference's racy shared-memory patterns;
+//  * every level count stays on the device (grids are sized by upper bounds),
+//    so the build has one host read (the total cluster count) per rebuild;
+//  * the apply stages each bank's packed inverse tile into shared memory with
+//    one cp.async.bulk per CTA and fuses the PCG update, the level-0 Schwarz
+//    product and the component sums of the residual into one kernel.
+#include <stdio.h>
+
+#include "../../include/sgmas.h"
+#include "ctx.hpp"
+#include "pcg_state.cuh"
+
+using namespace sgmas;
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__host__ __device__ constexpr int bsym_of(int B) { return B * (B + 1) / 2; }
+__host__ __device__ __forceinline__ int sym_index(int B, int r, int c) { return B * r - r * (r + 1) / 2 + c; }
+__host__ __device__ __forceinline__ int round_up(int v, int b) { return (v + b - 1) / b * b; }
+
+template <int B>
+__device__ __forceinline__ unsigned seg_ballot(bool pred) {
+    unsigned bal = __ballot_sync(0xffffffffu, pred);
+    if (B == 32) return bal;
+    const int base = (threadIdx.x & 31) & ~(B - 1);
+    return (bal >> base) & ((1u << (B & 31)) - 1u);
+}
+
+// ---------------------------------------------------------------------------
+// Hierarchy build (MASPreconditioner::ReorderRealtime, :1768-1807)
+// ---------------------------------------------------------------------------
+
+// _buildCML0_new (:63-103): same-bank neighbour mask; out-of-bank neighbours
+// compacted into the working list (read from the initial copy, so no reset).
+template <int B>
+__global__ void k_l0_masks(int Mm, int N, const int* __restrict__ part_map, const int* __restrict__ real_map,
+                           const unsigned* __restrict__ nb_start, const unsigned* __restrict__ nb_num0,
+                           const unsigned* __restrict__ nb_list0, unsigned* nb_num, unsigned* nb_list,
+                           unsigned* fine_mask, int* err) {
+    const int tdx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tdx >= Mm) return;
+    const int idx = part_map[tdx];
+    if (idx < 0) return;
+    if (idx >= N) { set_error(err, kDevBadIndex); return; }
+    const int w = tdx / B, lane = tdx % B;
+    unsigned msk = 1u << lane, nk = 0;
+    const unsigned st = nb_start[idx], cnt = nb_num0[idx];
+    for (unsigned i = 0; i < cnt; ++i) {
+        const unsigned v = nb_list0[st + i];
+        if (v >= (unsigned)N) { set_error(err, kDevBadIndex); continue; }
+        const int s = real_map[v];
+        if (s / B == w) msk |= 1u << (s % B);
+        else nb_list[st + nk++] = v;
+    }
+    nb_num[idx] = nk;
+    fine_mask[idx] = msk;
+}
+
+// _buildCollisionConnection_new (:1126-1538): decode the int4 contact and OR
+// same-bank bits between its nodes; level 0 ORs into mask[vertex] through the
+// slot map, level >= 1 into mask[coarse id].
+template <int B>
+__global__ void k_collision(int cp, const int4* __restrict__ pairs, int level, int node_offset, int N,
+                           const int* __restrict__ real_map, const int* __restrict__ coarse_space,
+                           unsigned* mask) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= cp) return;
+    int4 P = pairs[q];
+    int v[4], id[4], nv = 4;
+    if (P.x >= 0) {
+        if (P.w < 0) P.w = -P.w - 1;
+        v[0] = P.x; v[1] = P.y; v[2] = P.z; v[3] = P.w;
+    } else {
+        const int x = -P.x - 1;
+        if (P.z < 0) {
+            if (P.y < 0) { v[0] = x; v[1] = -P.y - 1; v[2] = -P.z - 1; v[3] = -P.w - 1; }
+            else { v[0] = x; v[1] = P.y; nv = 2; }
+        } else if (P.w < 0) {
+            if (P.y < 0) { v[0] = x; v[1] = -P.y - 1; v[2] = P.z; v[3] = -P.w - 1; }
+            else { v[0] = x; v[1] = P.y; v[2] = P.z; nv = 3; }
+        } else { v[0] = x; v[1] = P.y; v[2] = P.z; v[3] = P.w; }
+    }
+    unsigned cm[4] = {0u, 0u, 0u, 0u};
+    for (int i = 0; i < nv; ++i) {
+        v[i] -= node_offset;
+        if (v[i] >= 0 && v[i] < N) id[i] = level >= 1 ? coarse_space[(size_t)(level - 1) * N + v[i]] : real_map[v[i]];
+        else id[i] = -1;
+    }
+    for (int i = 0; i < nv; ++i)
+        for (int j = i + 1; j < nv; ++j) {
+            if (id[i] == id[j] || id[i] < 0 || id[j] < 0) continue;
+            if (id[i] / B == id[j] / B) {
+                cm[i] |= 1u << (id[j] % B);
+                cm[j] |= 1u << (id[i] % B);
+            }
+        }
+    for (int i = 0; i < nv; ++i) {
+        if (!cm[i]) continue;
+        if (level >= 1) { if (id[i] >= 0) atomicOr(mask + id[i], cm[i]); }
+        else if (v[i] >= 0 && v[i] < N) atomicOr(mask + v[i], cm[i]);
+    }
+}
+
+// Bank-local transitive closure (the BFS of _preparePrefixSumL0_new :157-214
+// and _nextLevelCluster :480-528) with a fixed trip count so every lane
+// takes part in every shuffle.  Returns the closure; *leader = lowest lane.
+template <int B>
+__device__ __forceinline__ unsigned bank_closure(unsigned orig, bool valid, int lane, bool* leader) {
+    unsigned msk = orig, visited = 1u << lane;
+    #pragma unroll 1
+    for (int it = 0; it < B; ++it) {
+        const unsigned todo = valid ? (visited ^ msk) : 0u;
+        const int nv = todo ? (__ffs(todo) - 1) : lane;
+        const unsigned other = __shfl_sync(0xffffffffu, orig, nv, B);
+        if (todo) { visited |= 1u << nv; msk |= other; }
+    }
+    *leader = valid && __popc(msk & lanemask_lt(lane)) == 0;
+    return msk;
+}
+
+template <int B>
+__global__ void k_l0_closure(int Mm, const int* __restrict__ part_map, unsigned* fine_mask, int* prefix_orig) {
+    const int tdx = blockIdx.x * blockDim.x + threadIdx.x;  // all threads stay for the shuffles
+    const int lane = tdx % B;
+    const int idx = tdx < Mm ? part_map[tdx] : -1;
+    const unsigned orig = idx >= 0 ? fine_mask[idx] : 0u;
+    bool leader;
+    const unsigned msk = bank_closure<B>(orig, idx >= 0, lane, &leader);
+    const unsigned el = seg_ballot<B>(leader);
+    if (tdx < Mm && lane == 0) prefix_orig[tdx / B] = __popc(el);  // all-padding bank -> 0
+    if (idx >= 0) fine_mask[idx] = msk;
+}
+
+// Exclusive scan of per-bank cluster counts in one CTA (thrust::exclusive_scan
+// at :1604-1606 / :1698-1700) and the level size bookkeeping of
+// _buildLevel1_new (:305-309) / _prefixSumLx (:553-557).
+// from_level == 0: n = Mm/B banks, next begin = round(Mm);
+// from_level >= 1: n = ceil(count/B), next begin = begin + round(count).
+template <int B>
+__global__ void k_level_scan(const int* __restrict__ cnt, int* pre, int Mm, int from_level, int* level_size) {
+    __shared__ int sh[1024];
+    __shared__ int carry;
+    int n, next_begin;
+    if (from_level == 0) {
+        n = Mm / B;
+        next_begin = round_up(Mm, B);
+    } else {
+        const int count = level_size[2 * from_level], begin = level_size[2 * from_level + 1];
+        n = (count + B - 1) / B;
+        next_begin = begin + round_up(count, B);
+    }
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int v = i < n ? cnt[i] : 0;
+        sh[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            const int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+            __syncthreads();
+            sh[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (i < n) pre[i] = carry + sh[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += sh[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        level_size[2 * (from_level + 1)] = carry;
+        level_size[2 * (from_level + 1) + 1] = next_begin;
+    }
+}
+
+// _buildLevel1_new (:271-328): level-1 id = bank prefix + rank of the
+// component's lowest lane among the bank's leaders.
+template <int B>
+__global__ void k_l1_ids(int Mm, const int* __restrict__ part_map, const unsigned* __restrict__ fine_mask,
+                         const int* __restrict__ pre, int* coarse_space, int* going_next) {
+    const int tdx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = tdx % B;
+    const int idx = tdx < Mm ? part_map[tdx] : -1;
+    const unsigned msk = idx >= 0 ? fine_mask[idx] : 0u;
+    const bool leader = idx >= 0 && __popc(msk & lanemask_lt(lane)) == 0;
+    const unsigned el = seg_ballot<B>(leader);
+    if (idx < 0) return;
+    const int id = __popc(el & lanemask_lt(__ffs(msk) - 1)) + pre[tdx / B];
+    coarse_space[idx] = id;
+    going_next[idx] = id + round_up(Mm, B);
+}
+
+// _buildConnectMaskLx_new (:401-477): neighbours whose level-`level` node
+// shares this vertex's coarse bank set bits of its coarse mask; the others
+// stay in the compacted list.  (The reference's per-component OR equals this
+// per-vertex OR: all members of a level-0 component share every coarse id.)
+template <int B>
+__global__ void k_lx_connect(int Mm, int N, int level, const int* __restrict__ part_map,
+                             const unsigned* __restrict__ nb_start, unsigned* nb_num, unsigned* nb_list,
+                             const int* __restrict__ coarse_space, unsigned* next_mask) {
+    const int tdx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tdx >= Mm) return;
+    const int idx = part_map[tdx];
+    if (idx < 0) return;
+    const int* cs = coarse_space + (size_t)(level - 1) * N;
+    const int ci = cs[idx];
+    unsigned conn = 0u, nk = 0u;
+    const unsigned st = nb_start[idx], cnt = nb_num[idx];
+    for (unsigned i = 0; i < cnt; ++i) {
+        const unsigned v = nb_list[st + i];
+        const int cc = cs[v];
+        if (ci / B == cc / B) conn |= 1u << (cc % B);
+        else nb_list[st + nk++] = v;
+    }
+    nb_num[idx] = nk;
+    if (conn) atomicOr(next_mask + ci, conn);
+}
+
+// _nextLevelCluster (:480-528): closure over the coarse banks at `level`.
+template <int B>
+__global__ void k_lx_closure(int level, const int* __restrict__ level_size, unsigned* next_mask, int* cnt) {
+    const int count = level_size[2 * level];
+    if ((int)(blockIdx.x * blockDim.x) >= round_up(count, B)) return;  // whole CTA beyond the level
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = idx % B;
+    const bool valid = idx < count;
+    const unsigned orig = valid ? ((1u << lane) | next_mask[idx]) : 0u;
+    bool leader;
+    const unsigned msk = bank_closure<B>(orig, valid, lane, &leader);
+    const unsigned el = seg_ballot<B>(leader);
+    if (lane == 0 && idx < count) cnt[idx / B] = __popc(el);
+    if (valid) next_mask[idx] = msk;
+}
+
+// _prefixSumLx (:530-577): ids for level+1 and goingNext of level `level`.
+template <int B>
+__global__ void k_lx_ids(int level, const int* __restrict__ level_size, unsigned* next_mask,
+                         const int* __restrict__ pre, int* going_next, int gn_cap, int* err) {
+    const int count = level_size[2 * level];
+    const int begin = level_size[2 * level + 1];
+    if ((int)(blockIdx.x * blockDim.x) >= round_up(count, B)) return;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = idx % B;
+    const bool valid = idx < count;
+    const unsigned msk = valid ? next_mask[idx] : 0u;
+    const bool leader = valid && __popc(msk & lanemask_lt(lane)) == 0;
+    const unsigned el = seg_ballot<B>(leader);
+    if (!valid) return;
+    const int id = __popc(el & lanemask_lt(__ffs(msk) - 1)) + pre[idx / B];
+    next_mask[idx] = (unsigned)id;
+    const int g = idx + begin;
+    if (g < gn_cap) going_next[g] = id + begin + round_up(count, B);
+    else set_error(err, kDevCapacity);
+}
+
+// _computeNextLevel (:579-590)
+__global__ void k_next_table(int N, int level, int* coarse_space, const unsigned* __restrict__ next_mask) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N) return;
+    const int nx = coarse_space[(size_t)(level - 1) * N + v];
+    coarse_space[(size_t)level * N + v] = (int)next_mask[nx];
+}
+
+// _aggregationKernel (:592-625)
+__global__ void k_aggregate(int N, int L, const int* __restrict__ going_next, int gn_cap, int* coarse_table,
+                            int* err) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N) return;
+    int cur = v;
+    int t[kMaxLevels] = {0, 0, 0, 0, 0, 0};
+    for (int l = 0; l < L - 1; ++l) {
+        if (cur < 0 || cur >= gn_cap) { set_error(err, kDevBadIndex); break; }
+        cur = going_next[cur];
+        t[l] = cur;
+    }
+    #pragma unroll
+    for (int l = 0; l < kMaxLevels; ++l) coarse_table[(size_t)kMaxLevels * v + l] = t[l];
+}
+
+// ---------------------------------------------------------------------------
+// Hessian scatter (PrepareHessian_bcoo, :1810-2054)
+// ---------------------------------------------------------------------------
+template <int B>
+__device__ __forceinline__ double* blk_ptr(double* hess, int r, int c) {
+    return hess + ((size_t)(c / B) * bsym_of(B) + sym_index(B, r % B, c % B)) * 9;
+}
+
+// phase 1: every FEM block.  Same-bank blocks are stored (transposed when the
+// column slot precedes the row slot -- the reference drops that case, which
+// its own slot maps never produce); other blocks climb goingNext and add into
+// each level where both ends share a bank.
+template <int B>
+__global__ void k_scatter1(int n, const double* __restrict__ vals, const int* __restrict__ rows,
+                           const int* __restrict__ cols, const uint32_t* __restrict__ indices, int offset, int N,
+                           int L, const int* __restrict__ real_map, const int* __restrict__ going_next,
+                           double* hess, const int* __restrict__ level_size, int* err) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= n) return;
+    const int k = indices ? (int)indices[I] : I;
+    const int rr = rows[k] - offset, cc = cols[k] - offset;
+    if (rr < 0 || rr >= N || cc < 0 || cc >= N) return;
+    const int total = level_size[2 * L + 1];
+    double H[9];
+    #pragma unroll
+    for (int q = 0; q < 9; ++q) H[q] = vals[(size_t)9 * k + q];
+    const int sr = real_map[rr], sc = real_map[cc];
+    if (sr / B == sc / B) {
+        if (sc >= sr) {
+            double* D = blk_ptr<B>(hess, sr, sc);
+            #pragma unroll
+            for (int q = 0; q < 9; ++q) D[q] = H[q];
+        } else {
+            double* D = blk_ptr<B>(hess, sc, sr);
+            #pragma unroll
+            for (int i = 0; i < 3; ++i)
+                #pragma unroll
+                for (int j = 0; j < 3; ++j) D[i + 3 * j] = H[j + 3 * i];
+        }
+        return;
+    }
+    int vr = rr, vc = cc;
+    for (int level = 1; level < L; ++level) {
+        vr = going_next[vr];
+        vc = going_next[vc];
+        if (vr >= total || vc >= total || vr < 0 || vc < 0) { set_error(err, kDevBadIndex); return; }
+        if (vr / B != vc / B) continue;
+        if (vc >= vr) {
+            double* D = blk_ptr<B>(hess, vr, vc);
+            #pragma unroll
+            for (int q = 0; q < 9; ++q) atomicAdd(D + q, H[q]);
+            if (vc == vr) {
+                #pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    #pragma unroll
+                    for (int j = 0; j < 3; ++j) atomicAdd(D + i + 3 * j, H[j + 3 * i]);
+            }
+        } else {
+            double* D = blk_ptr<B>(hess, vc, vr);
+            #pragma unroll
+            for (int i = 0; i < 3; ++i)
+                #pragma unroll
+                for (int j = 0; j < 3; ++j) atomicAdd(D + i + 3 * j, H[j + 3 * i]);
+        }
+    }
+}
+
+// phase 2: one CTA of B*B threads per level-0 bank; thread (r, c).
+template <int B>
+__global__ void k_scatter2(int nbank0, int L, const int* __restrict__ part_map, const int* __restrict__ prefix_orig,
+                           const int* __restrict__ going_next, double* hess) {
+    __shared__ double sh[32];
+    __shared__ int lead;
+    const int h = blockIdx.x;
+    const int r = threadIdx.x / B, c = threadIdx.x % B;
+    const int rdx = part_map[h * B + r], cdx = part_map[h * B + c];
+    const bool ok = rdx >= 0 && cdx >= 0;
+    const int prefix = prefix_orig[h];
+    double m[9];
+    const double* T = hess + ((size_t)h * bsym_of(B) + sym_index(B, c >= r ? r : c, c >= r ? c : r)) * 9;
+    #pragma unroll
+    for (int i = 0; i < 3; ++i)
+        #pragma unroll
+        for (int j = 0; j < 3; ++j) m[i + 3 * j] = ok ? (c >= r ? T[i + 3 * j] : T[j + 3 * i]) : 0.0;
+    if (prefix == 1) {
+        if (threadIdx.x == 0) {
+            lead = -1;
+            for (int q = 0; q < B; ++q)
+                if (part_map[h * B + q] >= 0) { lead = part_map[h * B + q]; break; }
+        }
+        double s[9];
+        #pragma unroll
+        for (int q = 0; q < 9; ++q) s[q] = block_sum<B * B>(m[q], sh);
+        if (threadIdx.x == 0 && lead >= 0) {
+            int nx = going_next[lead];
+            for (int level = 1; level < L; ++level) {
+                double* D = blk_ptr<B>(hess, nx, nx);
+                #pragma unroll
+                for (int q = 0; q < 9; ++q) atomicAdd(D + q, s[q]);
+                nx = going_next[nx];
+            }
+        }
+        return;
+    }
+    if (!ok) return;
+    int vr = rdx, vc = cdx;
+    for (int level = 1; level < L; ++level) {
+        vr = going_next[vr];
+        vc = going_next[vc];
+        if (vr / B == vc / B && vc >= vr) {
+            double* D = blk_ptr<B>(hess, vr, vc);
+            #pragma unroll
+            for (int q = 0; q < 9; ++q) atomicAdd(D + q, m[q]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Dense subdomain inverse (__inverse6_P96x96, :626-724): Gauss-Jordan without
+// pivoting, zero diagonal -> 1, partial symmetrisation of the diagonal 3x3
+// blocks.  One warp per matrix, the matrix in shared memory, lane-owned
+// columns; each element sees the reference's exact operation sequence
+// (IEEE divide, fused multiply-add), so the FP64 result is reproducible.
+// ---------------------------------------------------------------------------
+template <int B>
+__host__ __device__ constexpr int inv_warps() { return B == 16 ? 4 : 1; }
+
+template <int B, typename S>
+__global__ void __launch_bounds__(32 * inv_warps<B>()) k_invert(int nblk, const double* __restrict__ hess, S* inv,
+                                                               double* inv64, const int* __restrict__ level_size,
+                                                               int L) {
+    constexpr int n = 3 * B;
+    constexpr int bs = bsym_of(B);
+    extern __shared__ double smem_inv[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mat = blockIdx.x * inv_warps<B>() + w;
+    const int limit = level_size ? level_size[2 * L + 1] / B : nblk;
+    if (mat >= nblk || mat >= limit) return;
+    double* A = smem_inv + (size_t)w * (n * n + n);
+    double* col = A + n * n;
+    const double* P = hess + (size_t)mat * bs * 9;
+    for (int e = lane; e < n * n; e += 32) {
+        const int j = e / n, i = e % n;
+        const int rb = j / 3, cb = i / 3;
+        double v = cb >= rb ? P[sym_index(B, rb, cb) * 9 + (j % 3) + 3 * (i % 3)]
+                            : P[sym_index(B, cb, rb) * 9 + (i % 3) + 3 * (j % 3)];
+        if (i == j && v == 0.0) v = 1.0;
+        A[e] = v;
+    }
+    __syncwarp();
+    for (int j = 0; j < n; ++j) {
+        const double rt = A[j * n + j];
+        for (int k = lane; k < n; k += 32) col[k] = A[k * n + j];
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            const double piv = (i == j ? 1.0 : A[j * n + i]) / rt;
+            A[j * n + i] = piv;
+            for (int k = 0; k < n; ++k) {
+                if (k == j) continue;
+                const double base = (i == j) ? 0.0 : A[k * n + i];
+                A[k * n + i] = __fma_rn(-col[k], piv, base);
+            }
+        }
+        __syncwarp();
+    }
+    for (int i = lane; i < n; i += 32) {
+        if (i % 3 < 2) A[(i + 1) * n + i] = A[i * n + i + 1];
+        else A[i * n + i - 2] = A[(i - 2) * n + i];
+    }
+    __syncwarp();
+    S* out = inv + (size_t)mat * bs * 9;
+    for (int e = lane; e < bs * 9; e += 32) {
+        const int b = e / 9, q = e % 9;
+        int rb = 0, off = 0;
+        while (off + (B - rb) <= b) { off += B - rb; ++rb; }
+        const int cb = rb + (b - off);
+        const int a = q % 3, cc = q / 3;
+        const double v = A[(rb * 3 + a) * n + cb * 3 + cc];
+        out[e] = Store<S>::from_double(v);
+        if (inv64) inv64[(size_t)mat * bs * 9 + e] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Apply (preconditioning, :2210-2251)
+// ---------------------------------------------------------------------------
+template <typename Acc>
+__device__ __forceinline__ Acc shfl_acc(Acc v, int src, int width) { return __shfl_sync(0xffffffffu, v, src, width); }
+
+// z_lane = sum_c P(lane, c) r_c over one bank; columns ascending, each 3x3
+// row an fma chain (the order the oracle restates).
+template <int B, typename S, typename Acc>
+__device__ __forceinline__ void schwarz_rows(const S* tile, int lane, Acc r0, Acc r1, Acc r2, Acc& z0, Acc& z1,
+                                             Acc& z2) {
+    Acc a0 = 0, a1 = 0, a2 = 0;
+    #pragma unroll 4
+    for (int c = 0; c < B; ++c) {
+        const Acc x0 = shfl_acc(r0, c, B), x1 = shfl_acc(r1, c, B), x2 = shfl_acc(r2, c, B);
+        const bool tr = c < lane;
+        const S* P = tile + (tr ? sym_index(B, c, lane) : sym_index(B, lane, c)) * 9;
+        const int s1 = tr ? 1 : 3, s2 = tr ? 3 : 1;  // element (a, k) at a*s2 + k*s1
+        a0 = fma_acc(Store<S>::to_acc(P[0]), x0, a0);
+        a0 = fma_acc(Store<S>::to_acc(P[s1]), x1, a0);
+        a0 = fma_acc(Store<S>::to_acc(P[2 * s1]), x2, a0);
+        a1 = fma_acc(Store<S>::to_acc(P[s2]), x0, a1);
+        a1 = fma_acc(Store<S>::to_acc(P[s2 + s1]), x1, a1);
+        a1 = fma_acc(Store<S>::to_acc(P[s2 + 2 * s1]), x2, a1);
+        a2 = fma_acc(Store<S>::to_acc(P[2 * s2]), x0, a2);
+        a2 = fma_acc(Store<S>::to_acc(P[2 * s2 + s1]), x1, a2);
+        a2 = fma_acc(Store<S>::to_acc(P[2 * s2 + 2 * s1]), x2, a2);
+    }
+    z0 = a0; z1 = a1; z2 = a2;
+}
+
+// Stage `nb` consecutive bank tiles into shared memory with one bulk copy.
+template <typename S>
+__device__ __forceinline__ bool stage_tiles(S* tile, const S* src, int nb, int bs, uint64_t* bar, int* err) {
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const unsigned bytes = (unsigned)(nb * bs * 9 * sizeof(S));
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(bar, bytes);
+        bulk_g2s(tile, src, bytes, bar);
+    }
+    return mbar_wait(bar, 0, err);
+}
+
+constexpr int kApplyThreads = 128;
+
+// Level-0 kernel: (mode 1: x += alpha p, r -= alpha Ap first) r -> Acc,
+// level-0 Schwarz from the staged tile, component sums pushed up the chain
+// (BuildMultiLevelR :727-845 with the level-0 part of _schwarzLocalXSym6).
+template <int B, typename S, typename Acc>
+__global__ void __launch_bounds__(kApplyThreads) k_apply_l0(int Mm, int L, const int* __restrict__ part_map,
+                                                            const unsigned* __restrict__ fine_mask,
+                                                            const int* __restrict__ going_next, const S* __restrict__ inv,
+                                                            double* r, Acc* R, Acc* Z, int mode, double* x,
+                                                            const double* __restrict__ p, const double* __restrict__ Ap,
+                                                            const PcgState* st, int* err) {
+    if (st && st->done) return;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ uint64_t bar;
+    constexpr int bs = bsym_of(B);
+    constexpr int BPC = kApplyThreads / B;
+    S* tile = reinterpret_cast<S*>(smem_raw);
+    const int bank0 = blockIdx.x * BPC;
+    const int nbank = Mm / B;
+    const int nb = min(BPC, nbank - bank0);
+    const bool ok = stage_tiles<S>(tile, inv + (size_t)bank0 * bs * 9, nb, bs, &bar, err);
+
+    const int tdx = blockIdx.x * kApplyThreads + threadIdx.x;
+    const int lane = threadIdx.x % B;
+    const int idx = tdx < Mm ? part_map[tdx] : -1;
+    double rv0 = 0.0, rv1 = 0.0, rv2 = 0.0;
+    if (idx >= 0) {
+        double* rp = r + 3 * (size_t)idx;
+        rv0 = rp[0]; rv1 = rp[1]; rv2 = rp[2];
+        if (mode == 1) {
+            const double a = st->alpha;
+            double* xp = x + 3 * (size_t)idx;
+            const double* pp = p + 3 * (size_t)idx;
+            const double* ap = Ap + 3 * (size_t)idx;
+            xp[0] = xp[0] + a * pp[0]; xp[1] = xp[1] + a * pp[1]; xp[2] = xp[2] + a * pp[2];
+            rv0 = rv0 - a * ap[0]; rv1 = rv1 - a * ap[1]; rv2 = rv2 - a * ap[2];
+            rp[0] = rv0; rp[1] = rv1; rp[2] = rv2;
+        }
+    }
+    const Acc r0 = (Acc)rv0, r1 = (Acc)rv1, r2 = (Acc)rv2;
+    // component sums (members ascending) and the push up the chain
+    const unsigned msk = idx >= 0 ? fine_mask[idx] : 0u;
+    Acc s0 = 0, s1 = 0, s2 = 0;
+    #pragma unroll 4
+    for (int j = 0; j < B; ++j) {
+        const Acc y0 = shfl_acc(r0, j, B), y1 = shfl_acc(r1, j, B), y2 = shfl_acc(r2, j, B);
+        if (msk & (1u << j)) { s0 += y0; s1 += y1; s2 += y2; }
+    }
+    if (idx >= 0 && __popc(msk & lanemask_lt(lane)) == 0) {
+        int nx = idx;
+        for (int level = 1; level < L; ++level) {
+            nx = going_next[nx];
+            atomicAdd(R + 3 * (size_t)nx, s0);
+            atomicAdd(R + 3 * (size_t)nx + 1, s1);
+            atomicAdd(R + 3 * (size_t)nx + 2, s2);
+        }
+    }
+    if (!ok) return;
+    Acc z0, z1, z2;
+    const int lb = threadIdx.x / B;
+    schwarz_rows<B, S, Acc>(tile + (size_t)lb * bs * 9, lane, r0, r1, r2, z0, z1, z2);
+    if (tdx < Mm) {
+        Z[3 * (size_t)tdx] = z0; Z[3 * (size_t)tdx + 1] = z1; Z[3 * (size_t)tdx + 2] = z2;
+    }
+}
+
+// Coarse banks: z = P r for every bank of levels >= 1 (_schwarzLocalXSym6).
+template <int B, typename S, typename Acc>
+__global__ void __launch_bounds__(kApplyThreads) k_apply_coarse(int Mm, int L, const int* __restrict__ level_size,
+                                                                const S* __restrict__ inv, const Acc* __restrict__ R,
+                                                                Acc* Z, const PcgState* st, int* err) {
+    if (st && st->done) return;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ uint64_t bar;
+    constexpr int bs = bsym_of(B);
+    constexpr int BPC = kApplyThreads / B;
+    const int total = level_size[2 * L + 1];
+    const int first = round_up(Mm, B) / B;
+    const int nbank = total / B;
+    const int bank0 = first + blockIdx.x * BPC;
+    if (bank0 >= nbank) return;
+    const int nb = min(BPC, nbank - bank0);
+    S* tile = reinterpret_cast<S*>(smem_raw);
+    const bool ok = stage_tiles<S>(tile, inv + (size_t)bank0 * bs * 9, nb, bs, &bar, err);
+    const int lb = threadIdx.x / B, lane = threadIdx.x % B;
+    const int node = (bank0 + lb) * B + lane;
+    const bool valid = bank0 + lb < nbank;
+    const Acc r0 = valid ? R[3 * (size_t)node] : (Acc)0;
+    const Acc r1 = valid ? R[3 * (size_t)node + 1] : (Acc)0;
+    const Acc r2 = valid ? R[3 * (size_t)node + 2] : (Acc)0;
+    if (!ok) return;
+    Acc z0, z1, z2;
+    schwarz_rows<B, S, Acc>(tile + (size_t)(valid ? lb : 0) * bs * 9, lane, r0, r1, r2, z0, z1, z2);
+    if (valid) {
+        Z[3 * (size_t)node] = z0; Z[3 * (size_t)node + 1] = z1; Z[3 * (size_t)node + 2] = z2;
+    }
+}
+
+}  // namespace
+
+namespace {
+
+// CollectFinalZ (:848-877) + r.z and r.r (kind >= 1) + clearing the coarse
+// accumulators for the next apply.
+template <typename Acc>
+__global__ void __launch_bounds__(kThreads) k_collect(int N, int L, int Mm, const int* __restrict__ level_size,
+                                                      const int* __restrict__ real_map,
+                                                      const int* __restrict__ coarse_table, const Acc* __restrict__ Z,
+                                                      Acc* R, const double* __restrict__ r, double* z, int kind,
+                                                      PcgState* st, double* partials, unsigned* ticket,
+                                                      int set_cond, unsigned long long cond) {
+    if (st && st->done) {
+        // the last kernel of a WHILE body must always leave the condition set
+        if (set_cond && blockIdx.x == 0 && threadIdx.x == 0)
+            cudaGraphSetConditional((cudaGraphConditionalHandle)cond, 0u);
+        return;
+    }
+    __shared__ double sh[32];
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    double rz = 0.0, rr = 0.0;
+    if (v < N) {
+        const int rd = real_map[v];
+        Acc c0 = Z[3 * (size_t)rd], c1 = Z[3 * (size_t)rd + 1], c2 = Z[3 * (size_t)rd + 2];
+        for (int i = 1; i < L; ++i) {
+            const int now = coarse_table[(size_t)kMaxLevels * v + i - 1];
+            c0 += Z[3 * (size_t)now]; c1 += Z[3 * (size_t)now + 1]; c2 += Z[3 * (size_t)now + 2];
+        }
+        const double z0 = (double)c0, z1 = (double)c1, z2 = (double)c2;
+        z[3 * (size_t)v] = z0; z[3 * (size_t)v + 1] = z1; z[3 * (size_t)v + 2] = z2;
+        if (kind >= 1) {
+            const double r0 = r[3 * (size_t)v], r1 = r[3 * (size_t)v + 1], r2 = r[3 * (size_t)v + 2];
+            rz = r0 * z0 + r1 * z1 + r2 * z2;
+            rr = r0 * r0 + r1 * r1 + r2 * r2;
+        }
+    }
+    // clear the coarse accumulators (levels >= 1) for the next apply
+    const int total = level_size[2 * L + 1];
+    {
+        const size_t beg = 3 * (size_t)level_size[3];  // begin of level 1
+        const size_t end = 3 * (size_t)total;
+        for (size_t i = beg + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += (size_t)gridDim.x * blockDim.x)
+            R[i] = (Acc)0;
+    }
+    if (kind < 1) return;
+    const double brz = block_sum<kThreads>(rz, sh);
+    const double brr = block_sum<kThreads>(rr, sh);
+    __shared__ bool am_last;
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = brz;
+        partials[gridDim.x + blockIdx.x] = brr;
+        __threadfence();
+        am_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    double s1 = 0.0, s2 = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += kThreads) {
+        s1 += ((volatile double*)partials)[i];
+        s2 += ((volatile double*)partials)[gridDim.x + i];
+    }
+    s1 = block_sum<kThreads>(s1, sh);
+    s2 = block_sum<kThreads>(s2, sh);
+    if (threadIdx.x == 0) {
+        *ticket = 0u;
+        pcg_end_iteration(st, s1, s2, kind, set_cond, cond);
+    }
+}
+
+template <int B>
+int build_hierarchy_t(sgmas_context* c) {
+    cudaStream_t s = c->stream;
+    const int Mm = c->Mm, N = c->N, L = c->L;
+    const int gM = (Mm + kThreads - 1) / kThreads, gN = (N + kThreads - 1) / kThreads;
+    SG_CUDA(c, cudaMemsetAsync(c->d_level_size, 0, sizeof(int) * 2 * (kMaxLevels + 2), s));
+    k_l0_masks<B><<<gM, kThreads, 0, s>>>(Mm, N, c->d_part_map, c->d_real_map, c->d_nb_start, c->d_nb_num0,
+                                          c->d_nb_list0, c->d_nb_num, c->d_nb_list, c->d_fine_mask, c->d_err);
+    if (c->cp_num > 0)
+        k_collision<B><<<(c->cp_num + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+            c->cp_num, (const int4*)c->d_pairs, 0, c->node_offset, N, c->d_real_map, c->d_coarse_space,
+            c->d_fine_mask);
+    k_l0_closure<B><<<gM, kThreads, 0, s>>>(Mm, c->d_part_map, c->d_fine_mask, c->d_prefix_orig);
+    k_level_scan<B><<<1, 1024, 0, s>>>(c->d_prefix_orig, c->d_bank_pre, Mm, 0, c->d_level_size);
+    k_l1_ids<B><<<gM, kThreads, 0, s>>>(Mm, c->d_part_map, c->d_fine_mask, c->d_bank_pre, c->d_coarse_space,
+                                        c->d_going_next);
+    for (int level = 1; level < L; ++level) {
+        SG_CUDA(c, cudaMemsetAsync(c->d_next_mask, 0, sizeof(unsigned) * N, s));
+        k_lx_connect<B><<<gM, kThreads, 0, s>>>(Mm, N, level, c->d_part_map, c->d_nb_start, c->d_nb_num,
+                                                c->d_nb_list, c->d_coarse_space, c->d_next_mask);
+        if (c->cp_num > 0)
+            k_collision<B><<<(c->cp_num + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+                c->cp_num, (const int4*)c->d_pairs, level, c->node_offset, N, c->d_real_map, c->d_coarse_space,
+                c->d_next_mask);
+        const int gC = (round_up(N, B) + kThreads - 1) / kThreads;
+        k_lx_closure<B><<<gC, kThreads, 0, s>>>(level, c->d_level_size, c->d_next_mask, c->d_bank_cnt);
+        k_level_scan<B><<<1, 1024, 0, s>>>(c->d_bank_cnt, c->d_bank_pre, Mm, level, c->d_level_size);
+        k_lx_ids<B><<<gC, kThreads, 0, s>>>(level, c->d_level_size, c->d_next_mask, c->d_bank_pre,
+                                            c->d_going_next, c->gn_cap, c->d_err);
+        k_next_table<<<gN, kThreads, 0, s>>>(N, level, c->d_coarse_space, c->d_next_mask);
+    }
+    k_aggregate<<<gN, kThreads, 0, s>>>(N, L, c->d_going_next, c->gn_cap, c->d_coarse_table, c->d_err);
+    SG_CUDA(c, cudaGetLastError());
+    SG_CUDA(c, cudaMemcpyAsync(c->h_level_size, c->d_level_size, sizeof(int) * 2 * (kMaxLevels + 2),
+                               cudaMemcpyDeviceToHost, s));
+    SG_CUDA(c, cudaStreamSynchronize(s));
+    int herr = 0;
+    SG_CUDA(c, cudaMemcpy(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) return ctx_fail(c, SGMAS_ERR_DEVICE, "MAS hierarchy build: device error %d", herr);
+    c->total = c->h_level_size[2 * L + 1];
+    return 0;
+}
+
+template <int B, typename S, typename Acc>
+int scatter_invert_t(sgmas_context* c, const double* vals, const int* rows, const int* cols, const uint32_t* indices,
+                     int offset, int n) {
+    cudaStream_t s = c->stream;
+    const int nblk = c->total / B;
+    const size_t bs = bsym_of(B);
+    SG_CUDA(c, cudaMemsetAsync(c->d_hess, 0, sizeof(double) * nblk * bs * 9, s));
+    if (n > 0)
+        k_scatter1<B><<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+            n, vals, rows, cols, indices, offset, c->N, c->L, c->d_real_map, c->d_going_next, c->d_hess,
+            c->d_level_size, c->d_err);
+    k_scatter2<B><<<c->Mm / B, B * B, 0, s>>>(c->Mm / B, c->L, c->d_part_map, c->d_prefix_orig, c->d_going_next,
+                                             c->d_hess);
+    constexpr int W = inv_warps<B>();
+    const size_t smem = (size_t)W * (9 * B * B + 3 * B) * sizeof(double);
+    auto kern = k_invert<B, S>;
+    SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(nblk + W - 1) / W, 32 * W, smem, s>>>(nblk, c->d_hess, (S*)c->d_inv, nullptr, c->d_level_size, c->L);
+    SG_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+template <int B, typename S, typename Acc>
+int apply_t(sgmas_context* c, const double* r, double* z, int mode, const PcgState* st, double* x, const double* p,
+            const double* Ap, double* partials, unsigned* ticket, int kind, unsigned long long cond, int* launches) {
+    cudaStream_t s = c->stream;
+    constexpr int bs = bsym_of(B);
+    constexpr int BPC = kApplyThreads / B;
+    const size_t smem = (size_t)BPC * bs * 9 * sizeof(S);
+    auto k0 = k_apply_l0<B, S, Acc>;
+    auto k1 = k_apply_coarse<B, S, Acc>;
+    SG_CUDA(c, cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SG_CUDA(c, cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int nbank0 = c->Mm / B;
+    const int parts = c->apply_parts;
+    if (parts & 1)
+    k0<<<(nbank0 + BPC - 1) / BPC, kApplyThreads, smem, s>>>(c->Mm, c->L, c->d_part_map, c->d_fine_mask,
+                                                             c->d_going_next, (const S*)c->d_inv, (double*)r,
+                                                             (Acc*)c->d_R, (Acc*)c->d_Z, mode, x, p, Ap, st, c->d_err);
+    const int coarse_cap = c->cap_total / B - round_up(c->Mm, B) / B;
+    if (parts & 2)
+    k1<<<max(1, (coarse_cap + BPC - 1) / BPC), kApplyThreads, smem, s>>>(c->Mm, c->L, c->d_level_size,
+                                                                         (const S*)c->d_inv, (const Acc*)c->d_R,
+                                                                         (Acc*)c->d_Z, st, c->d_err);
+    const int gN = (c->N + kThreads - 1) / kThreads;
+    if (parts & 4)
+    k_collect<Acc><<<gN, kThreads, 0, s>>>(c->N, c->L, c->Mm, c->d_level_size, c->d_real_map, c->d_coarse_table,
+                                          (const Acc*)c->d_Z, (Acc*)c->d_R, r, z, kind, (PcgState*)st, partials,
+                                          ticket, cond != 0ull, cond);
+    SG_CUDA(c, cudaGetLastError());
+    if (launches) *launches += 3;
+    return 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// internal entry points
+// ---------------------------------------------------------------------------
+int mas_build_hierarchy(sgmas_context* c) {
+    if (c->bank == 16) return build_hierarchy_t<16>(c);
+    return build_hierarchy_t<32>(c);
+}
+
+int mas_scatter_and_invert(sgmas_context* c, const double* vals, const int* rows, const int* cols,
+                           const uint32_t* indices, int offset, int n) {
+#define SG_DISPATCH(B)                                                                                   \
+    switch (c->precision) {                                                                              \
+        case SGMAS_MAS_FP32: return scatter_invert_t<B, float, float>(c, vals, rows, cols, indices, offset, n); \
+        case SGMAS_MAS_BF16:                                                                             \
+            return scatter_invert_t<B, __nv_bfloat16, float>(c, vals, rows, cols, indices, offset, n);   \
+        default: return scatter_invert_t<B, double, double>(c, vals, rows, cols, indices, offset, n);   \
+    }
+    if (c->bank == 16) { SG_DISPATCH(16) }
+    SG_DISPATCH(32)
+#undef SG_DISPATCH
+}
+
+int mas_launch_apply(sgmas_context* c, const double* r, double* z, int mode, const PcgState* st, double* x,
+                     const double* p, const double* Ap, double* partials, unsigned* ticket, int iter_kind,
+                     unsigned long long cond_handle, int* launches) {
+#define SG_DISPATCH(B)                                                                                          \
+    switch (c->precision) {                                                                                     \
+        case SGMAS_MAS_FP32:                                                                                    \
+            return apply_t<B, float, float>(c, r, z, mode, st, x, p, Ap, partials, ticket, iter_kind, cond_handle, \
+                                            launches);                                                          \
+        case SGMAS_MAS_BF16:                                                                                    \
+            return apply_t<B, __nv_bfloat16, float>(c, r, z, mode, st, x, p, Ap, partials, ticket, iter_kind,   \
+                                                    cond_handle, launches);                                     \
+        default:                                                                                                \
+            return apply_t<B, double, double>(c, r, z, mode, st, x, p, Ap, partials, ticket, iter_kind,         \
+                                              cond_handle, launches);                                           \
+    }
+    if (c->bank == 16) { SG_DISPATCH(16) }
+    SG_DISPATCH(32)
+#undef SG_DISPATCH
+}
+
+int mas_invert_blocks_dev(sgmas_context* c, const double* hess, int nblk, double* out64) {
+    cudaStream_t s = c->stream;
+    float* tmp = nullptr;
+    const size_t bs = (size_t)c->bank * (c->bank + 1) / 2;
+    SG_CUDA(c, cudaMallocAsync((void**)&tmp, sizeof(float) * nblk * bs * 9, s));
+    if (c->bank == 16) {
+        const size_t smem = (size_t)inv_warps<16>() * (9 * 16 * 16 + 48) * sizeof(double);
+        SG_CUDA(c, cudaFuncSetAttribute(k_invert<16, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_invert<16, float><<<(nblk + 3) / 4, 128, smem, s>>>(nblk, hess, tmp, out64, nullptr, 0);
+    } else {
+        const size_t smem = (size_t)(9 * 32 * 32 + 96) * sizeof(double);
+        SG_CUDA(c, cudaFuncSetAttribute(k_invert<32, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_invert<32, float><<<nblk, 32, smem, s>>>(nblk, hess, tmp, out64, nullptr, 0);
+    }
+    SG_CUDA(c, cudaGetLastError());
+    SG_CUDA(c, cudaFreeAsync(tmp, s));
+    return 0;
+}

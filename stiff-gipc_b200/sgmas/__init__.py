@@ -1,0 +1,297 @@
+"""Python binding of libsgmas (the C-ABI in include/sgmas.h) via ctypes.
+
+Device arrays are passed as objects with ``data_ptr()`` (torch tensors) or as
+raw integer addresses; host arrays are numpy.  Torch is used only for device
+memory and streams.  There is no CPU fallback: if the library is missing or no
+GPU is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+LIB_PATH = _build.LIB_PATH
+_lib = None
+
+SGMAS_MAS_FP32, SGMAS_MAS_BF16, SGMAS_MAS_FP64 = 0, 1, 2
+PRECISION = {"fp32": 0, "bf16": 1, "fp64": 2}
+
+
+class SgmasError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"sgmas error {code}: {msg}")
+        self.code = code
+
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int), ("bank_size", C.c_int), ("mas_precision", C.c_int)]
+
+
+class PcgConfig(C.Structure):
+    _fields_ = [("max_iter", C.c_int), ("rel_tol", C.c_double), ("abs_tol", C.c_double),
+                ("use_preconditioned_norm", C.c_int), ("preconditioner", C.c_int),
+                ("abd_bodies", C.c_int), ("fem_offset", C.c_int), ("check_every", C.c_int)]
+
+
+class PcgReport(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("rz0", C.c_double), ("rr0", C.c_double),
+                ("rr_last", C.c_double), ("solve_ms", C.c_float), ("precond_ms", C.c_float),
+                ("kernel_launches", C.c_int)]
+
+
+class Bcoo(C.Structure):
+    _fields_ = [("d_values", C.c_void_p), ("d_rows", C.c_void_p), ("d_cols", C.c_void_p),
+                ("n_blocks", C.c_int), ("n_block_rows", C.c_int)]
+
+
+EXPORTS = [
+    "sgmas_create", "sgmas_destroy", "sgmas_last_error", "sgmas_set_stream", "sgmas_synchronize",
+    "sgmas_mas_init", "sgmas_mas_set_contacts", "sgmas_mas_assemble", "sgmas_mas_apply", "sgmas_mas_info",
+    "sgmas_mas_download_tables", "sgmas_mas_download_matrices", "sgmas_mas_invert_host",
+    "sgmas_pcg_solve", "sgmas_pcg_solve_host", "sgmas_spmv", "sgmas_convert", "sgmas_write_upper_blocks",
+    "sgmas_morton_codes", "sgmas_morton_partition", "sgmas_pcg_profile", "sgmas_vert_neighbors",
+    "sgmas_part_maps",
+]
+
+
+def lib(build_if_missing: bool = False):
+    """Load libsgmas.so (built in-tree by sgmas.build / __graft_entry__.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if not build_if_missing:
+            raise SgmasError(-2, f"{LIB_PATH} is missing: run __graft_entry__.build()")
+        _build.build()
+    L = C.CDLL(LIB_PATH)
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    L.sgmas_create.argtypes = [C.POINTER(Config), C.POINTER(vp)]
+    L.sgmas_destroy.argtypes = [vp]
+    L.sgmas_destroy.restype = None
+    L.sgmas_last_error.argtypes = [vp]
+    L.sgmas_last_error.restype = C.c_char_p
+    L.sgmas_set_stream.argtypes = [vp, vp]
+    L.sgmas_synchronize.argtypes = [vp]
+    L.sgmas_mas_init.argtypes = [vp, i, i, i, vp, vp, vp, vp, i, vp]
+    L.sgmas_mas_set_contacts.argtypes = [vp, vp, i]
+    L.sgmas_mas_assemble.argtypes = [vp, vp, vp, vp, vp, i, i, i]
+    L.sgmas_mas_apply.argtypes = [vp, vp, vp]
+    L.sgmas_mas_info.argtypes = [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i)]
+    L.sgmas_mas_download_tables.argtypes = [vp, vp, vp, vp, i, vp, vp, vp]
+    L.sgmas_mas_download_matrices.argtypes = [vp, vp, vp]
+    L.sgmas_mas_invert_host.argtypes = [vp, vp, i, vp]
+    L.sgmas_pcg_solve.argtypes = [vp, C.POINTER(Bcoo), vp, vp, C.POINTER(PcgConfig), C.POINTER(PcgReport)]
+    L.sgmas_pcg_solve_host.argtypes = [vp, vp, vp, vp, i, i, vp, vp, C.POINTER(PcgConfig), C.POINTER(PcgReport)]
+    L.sgmas_spmv.argtypes = [vp, d, C.POINTER(Bcoo), vp, d, vp]
+    L.sgmas_convert.argtypes = [vp, vp, vp, vp, i, vp, vp, vp, C.POINTER(i)]
+    L.sgmas_write_upper_blocks.argtypes = [vp, vp, i, i, vp, vp, vp, vp]
+    L.sgmas_morton_codes.argtypes = [vp, vp, i, vp, vp]
+    L.sgmas_morton_partition.argtypes = [vp, vp, i, vp, i, C.POINTER(i), vp]
+    L.sgmas_pcg_profile.argtypes = [vp, i, vp, i]
+    L.sgmas_vert_neighbors.argtypes = [vp, i, vp, i, i, i, vp, vp, vp, i]
+    L.sgmas_part_maps.argtypes = [vp, i, i, vp, i, C.POINTER(i), vp]
+    _lib = L
+    return L
+
+
+def vert_neighbors(tets, n_verts, tris=None, abd_vert_offset=0):
+    """Neighbour CSR of a tet (+ triangle) mesh (host; getVertNeighbors)."""
+    tets = _h(tets, np.int32).reshape(-1)
+    tris = None if tris is None or len(tris) == 0 else _h(tris, np.int32).reshape(-1)
+    ntet, ntri = len(tets) // 4, 0 if tris is None else len(tris) // 3
+    cap = 12 * ntet + 6 * ntri + 16
+    st = np.zeros(n_verts, np.uint32)
+    nn = np.zeros(n_verts, np.uint32)
+    nl = np.zeros(cap, np.uint32)
+    rc = lib().sgmas_vert_neighbors(_ptr(tets), ntet, _ptr(tris), ntri, n_verts, abd_vert_offset, _ptr(st),
+                                    _ptr(nn), _ptr(nl), cap)
+    if rc < 0:
+        raise SgmasError(rc, "sgmas_vert_neighbors failed")
+    return st, nn, nl[:rc].copy()
+
+
+def part_maps(part_id, bank=16):
+    """Slot maps from per-vertex part ids (host; setMAS_partition)."""
+    part_id = _h(part_id, np.int32)
+    cap = (int(part_id[-1]) + 1) * bank
+    pm = np.zeros(cap, np.int32)
+    rm = np.zeros(len(part_id), np.int32)
+    size = C.c_int()
+    rc = lib().sgmas_part_maps(_ptr(part_id), len(part_id), bank, _ptr(pm), cap, C.byref(size), _ptr(rm))
+    if rc != 0:
+        raise SgmasError(rc, "sgmas_part_maps: parts must be contiguous, <= bank vertices each")
+    return pm[: size.value], rm
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    return x.data_ptr()
+
+
+def _h(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def pcg_config(max_iter=0, rel_tol=1e-4, abs_tol=0.0, use_preconditioned_norm=False, preconditioner="mas",
+               abd_bodies=0, fem_offset=0, check_every=10):
+    pc = {"jacobi": 0, "mas": 1, 0: 0, 1: 1}[preconditioner]
+    return PcgConfig(max_iter, rel_tol, abs_tol, int(use_preconditioned_norm), pc, abd_bodies, fem_offset,
+                     check_every)
+
+
+class Context:
+    """One sgmas_context: a MAS preconditioner + PCG solver on one GPU."""
+
+    def __init__(self, device=0, bank=16, precision="fp32"):
+        self.L = lib()
+        self.h = C.c_void_p()
+        cfg = Config(device, bank, PRECISION.get(precision, precision))
+        rc = self.L.sgmas_create(C.byref(cfg), C.byref(self.h))
+        if rc != 0:
+            raise SgmasError(rc, "sgmas_create failed (no CUDA device?)")
+        self.bank = bank
+        self.precision = precision
+        self._keep = {}
+
+    def close(self):
+        if self.h:
+            self.L.sgmas_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise SgmasError(rc, self.L.sgmas_last_error(self.h).decode())
+
+    def set_stream(self, stream_ptr):
+        self._check(self.L.sgmas_set_stream(self.h, stream_ptr))
+
+    def synchronize(self):
+        self._check(self.L.sgmas_synchronize(self.h))
+
+    # ---- MAS ----
+    def mas_init(self, n_verts, nb_start, nb_num, nb_list, part_map, real_map, node_offset=0):
+        nb_start, nb_num = _h(nb_start, np.uint32), _h(nb_num, np.uint32)
+        nb_list, part_map, real_map = _h(nb_list, np.uint32), _h(part_map, np.int32), _h(real_map, np.int32)
+        self.n_verts = n_verts
+        self.part_map_size = len(part_map)
+        self._check(self.L.sgmas_mas_init(self.h, n_verts, node_offset, len(nb_list), _ptr(nb_list),
+                                          _ptr(nb_start), _ptr(nb_num), _ptr(part_map), len(part_map),
+                                          _ptr(real_map)))
+
+    def mas_set_contacts(self, pairs, cp_num=None):
+        n = 0 if pairs is None else (cp_num if cp_num is not None else pairs.shape[0])
+        self._keep["pairs"] = pairs
+        self._check(self.L.sgmas_mas_set_contacts(self.h, _ptr(pairs) if n else None, n))
+        self.cp_num = n
+
+    def mas_assemble(self, vals, rows, cols, indices=None, offset=0, cp_num=None):
+        if cp_num is None:
+            cp_num = getattr(self, "cp_num", 0)
+        self._check(self.L.sgmas_mas_assemble(self.h, _ptr(vals), _ptr(rows), _ptr(cols), _ptr(indices), offset,
+                                              int(rows.shape[0]), cp_num))
+
+    def mas_apply(self, r, z):
+        self._check(self.L.sgmas_mas_apply(self.h, _ptr(r), _ptr(z)))
+
+    def mas_info(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.L.sgmas_mas_info(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return dict(levelnum=a.value, total=b.value, n_mas_blocks=c.value)
+
+    def mas_tables(self):
+        info = self.mas_info()
+        Ln, n = info["levelnum"], self.n_verts
+        fm = np.zeros(n, np.uint32)
+        cs = np.zeros(Ln * n, np.int32)
+        gn = np.zeros(max(info["total"], n) + 1, np.int32)
+        ls = np.zeros(2 * (Ln + 1), np.int32)
+        po = np.zeros(self.part_map_size // self.bank, np.int32)
+        ct = np.zeros(6 * n, np.int32)
+        self._check(self.L.sgmas_mas_download_tables(self.h, _ptr(fm), _ptr(cs), _ptr(gn), len(gn), _ptr(ls),
+                                                     _ptr(po), _ptr(ct)))
+        return dict(fine_mask=fm, coarse_space=cs.reshape(Ln, n), going_next=gn, level_size=ls.reshape(Ln + 1, 2),
+                    prefix_orig=po, coarse_table=ct.reshape(n, 6))
+
+    def mas_matrices(self):
+        info = self.mas_info()
+        nval = info["n_mas_blocks"] * (self.bank * (self.bank + 1) // 2) * 9
+        h = np.zeros(nval)
+        inv = np.zeros(nval)
+        self._check(self.L.sgmas_mas_download_matrices(self.h, _ptr(h), _ptr(inv)))
+        return h, inv
+
+    def mas_invert_host(self, hess64, nblocks):
+        hess64 = _h(hess64, np.float64)
+        out = np.zeros_like(hess64)
+        self._check(self.L.sgmas_mas_invert_host(self.h, _ptr(hess64), nblocks, _ptr(out)))
+        return out
+
+    # ---- PCG ----
+    @staticmethod
+    def bcoo(vals, rows, cols, n_block_rows):
+        return Bcoo(_ptr(vals), _ptr(rows), _ptr(cols), int(rows.shape[0]), n_block_rows)
+
+    def pcg_solve(self, vals, rows, cols, n_block_rows, b, x, **cfg):
+        A = self.bcoo(vals, rows, cols, n_block_rows)
+        c = pcg_config(**cfg)
+        rep = PcgReport()
+        self._check(self.L.sgmas_pcg_solve(self.h, C.byref(A), _ptr(b), _ptr(x), C.byref(c), C.byref(rep)))
+        return {k: getattr(rep, k) for k, _ in PcgReport._fields_}
+
+    def pcg_solve_host(self, vals, rows, cols, n_block_rows, b, **cfg):
+        vals, rows, cols, b = _h(vals, np.float64), _h(rows, np.int32), _h(cols, np.int32), _h(b, np.float64)
+        x = np.zeros_like(b)
+        c = pcg_config(**cfg)
+        rep = PcgReport()
+        self._check(self.L.sgmas_pcg_solve_host(self.h, _ptr(vals), _ptr(rows), _ptr(cols), len(rows),
+                                                n_block_rows, _ptr(b), _ptr(x), C.byref(c), C.byref(rep)))
+        return x, {k: getattr(rep, k) for k, _ in PcgReport._fields_}
+
+    def pcg_profile(self, reps=20):
+        ms = np.zeros(4, np.float32)
+        self._check(self.L.sgmas_pcg_profile(self.h, reps, _ptr(ms), 4))
+        return dict(spmv=float(ms[0]), update_l0=float(ms[1]), coarse=float(ms[2]), collect=float(ms[3]))
+
+    # ---- path kernels ----
+    def spmv(self, a, vals, rows, cols, n_block_rows, x, b, y):
+        A = self.bcoo(vals, rows, cols, n_block_rows)
+        self._check(self.L.sgmas_spmv(self.h, a, C.byref(A), _ptr(x), b, _ptr(y)))
+
+    def convert(self, vals, rows, cols, out_vals, out_rows, out_cols):
+        nu = C.c_int()
+        self._check(self.L.sgmas_convert(self.h, _ptr(vals), _ptr(rows), _ptr(cols), int(rows.shape[0]),
+                                         _ptr(out_vals), _ptr(out_rows), _ptr(out_cols), C.byref(nu)))
+        return nu.value
+
+    def write_upper_blocks(self, H, nodes, vals, rows, cols):
+        n_elem, k = int(nodes.shape[0]), int(nodes.shape[1])
+        self._check(self.L.sgmas_write_upper_blocks(self.h, _ptr(H), n_elem, k, _ptr(nodes), _ptr(vals),
+                                                    _ptr(rows), _ptr(cols)))
+
+    def morton_codes(self, pos, codes, aabb=None):
+        box = None if aabb is None else _h(aabb, np.float64)
+        self._check(self.L.sgmas_morton_codes(self.h, _ptr(pos), int(pos.shape[0]), _ptr(box), _ptr(codes)))
+
+    def morton_partition(self, pos):
+        n = int(pos.shape[0])
+        cap = (n + self.bank - 1) // self.bank * self.bank
+        pm = np.zeros(cap, np.int32)
+        rm = np.zeros(n, np.int32)
+        size = C.c_int()
+        self._check(self.L.sgmas_morton_partition(self.h, _ptr(pos), n, _ptr(pm), cap, C.byref(size), _ptr(rm)))
+        return pm[: size.value], rm

@@ -1,0 +1,295 @@
+"""Seeded synthetic IPC Newton systems in the reference's BCOO layout.
+
+The reference builds its Hessian from Stable Neo-Hookean tets
+(SG/femEnergy.cu:1789-1927), IPC barrier pairs (SG/GIPC.cu:3108-4947) and a
+lumped mass diagonal (SG/GIPC.cu:10201-10220).  The physics producers are not
+part of the solve; this module stands in for them with seeded inputs of the
+same shapes, sizes and value ranges:
+
+* a structured tet grid (6 tets per cube, Freudenthal split), vertex
+  positions jittered, a random deformation of the given scale;
+* the element Hessian of the stable Neo-Hookean energy
+  psi = mu/2 (tr F^T F - 3) + lam/2 (J - 1 - mu/lam)^2, projected to PSD per
+  element, scaled by volume * dt^2 (reference scaling: A = M + dt^2 K);
+* b = dt^2 * gradient of the elastic energy at the deformed state;
+* synthetic point-triangle barrier pairs between two stacked blocks, each an
+  SPD 12x12 matrix kappa*b''(d) g g^T + kappa*eps*I written as 10 upper blocks
+  and encoded as the reference's PT int4 (-(p+1), t0, t1, t2).
+
+Element matrices are written into upper 3x3 triplets exactly like
+write_triplet_fem (SG/femEnergy.cu:14-62): row <= col, the (jj, ii) block
+transposed when the vertex order is reversed.  Values are column-major 3x3.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+_TET_SPLIT = np.array([  # Freudenthal/Kuhn split of the unit cube along (0,0,0)-(1,1,1)
+    [0, 1, 3, 7], [0, 1, 5, 7], [0, 2, 3, 7],
+    [0, 2, 6, 7], [0, 4, 5, 7], [0, 4, 6, 7]], dtype=np.int64)
+
+# corner c of a cube -> (dx, dy, dz) with c = dx + 2 dy + 4 dz
+_CORNER = np.array([[c & 1, (c >> 1) & 1, (c >> 2) & 1] for c in range(8)], dtype=np.int64)
+
+UPPER_PAIRS_4 = [(ii, jj) for ii in range(4) for jj in range(ii, 4)]
+
+
+@dataclasses.dataclass
+class System:
+    """An upper-triangular 3x3 BCOO system A x = b (reference scaling)."""
+    n_verts: int
+    rows: np.ndarray          # int32 [nb]
+    cols: np.ndarray          # int32 [nb]
+    vals: np.ndarray          # float64 [nb, 9], column-major 3x3
+    b: np.ndarray             # float64 [3 n]
+    pos: np.ndarray           # float64 [n, 3] (rest positions)
+    tets: np.ndarray          # int32 [ntet, 4]
+    pairs: np.ndarray         # int32 [cp, 4] contact pairs (reference int4 encoding)
+    # raw triplets before merging (the scatter-assembly input)
+    raw_rows: np.ndarray = None
+    raw_cols: np.ndarray = None
+    raw_vals: np.ndarray = None
+    info: dict = dataclasses.field(default_factory=dict)
+
+
+def tet_grid(nx: int, ny: int, nz: int, h: float, origin=(0.0, 0.0, 0.0)):
+    """Vertices (x fastest) and 6 tets per cube of an nx*ny*nz vertex grid."""
+    ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    vid = lambda x, y, z: x + nx * (y + ny * z)
+    pos = np.stack([ix.ravel(order="F"), iy.ravel(order="F"), iz.ravel(order="F")], 1).astype(np.float64)
+    pos = pos * h + np.asarray(origin, dtype=np.float64)
+    cx, cy, cz = np.meshgrid(np.arange(nx - 1), np.arange(ny - 1), np.arange(nz - 1), indexing="ij")
+    cx, cy, cz = cx.ravel(order="F"), cy.ravel(order="F"), cz.ravel(order="F")
+    corners = np.stack([vid(cx + d[0], cy + d[1], cz + d[2]) for d in _CORNER], 1)  # [ncube, 8]
+    tets = corners[:, _TET_SPLIT].reshape(-1, 4)
+    return pos, tets.astype(np.int64)
+
+
+def _hat(v):
+    z = np.zeros(v.shape[:-1])
+    return np.stack([np.stack([z, -v[..., 2], v[..., 1]], -1),
+                     np.stack([v[..., 2], z, -v[..., 0]], -1),
+                     np.stack([-v[..., 1], v[..., 0], z], -1)], -2)
+
+
+def neo_hookean_elements(X, x, tets, E, nu):
+    """Per-tet volume-weighted PSD Hessian [ntet,12,12] and gradient [ntet,12]."""
+    mu = E / (2.0 * (1.0 + nu))
+    lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    alpha = 1.0 + mu / lam
+    Xt = X[tets]                                         # [t,4,3]
+    Dm = np.stack([Xt[:, 1] - Xt[:, 0], Xt[:, 2] - Xt[:, 0], Xt[:, 3] - Xt[:, 0]], -1)
+    vol = np.abs(np.linalg.det(Dm)) / 6.0
+    Dminv = np.linalg.inv(Dm)
+    xt = x[tets]
+    Ds = np.stack([xt[:, 1] - xt[:, 0], xt[:, 2] - xt[:, 0], xt[:, 3] - xt[:, 0]], -1)
+    F = Ds @ Dminv
+    f0, f1, f2 = F[:, :, 0], F[:, :, 1], F[:, :, 2]
+    J = np.linalg.det(F)
+    g = np.concatenate([np.cross(f1, f2), np.cross(f2, f0), np.cross(f0, f1)], -1)  # vec(dJ/dF), column-major
+    vecF = np.concatenate([f0, f1, f2], -1)
+    P = mu * vecF + (lam * (J - alpha))[:, None] * g
+    z3 = np.zeros((len(tets), 3, 3))
+    HJ = np.block([[z3, -_hat(f2), _hat(f1)],
+                   [_hat(f2), z3, -_hat(f0)],
+                   [-_hat(f1), _hat(f0), z3]])
+    HF = mu * np.eye(9)[None] + lam * g[:, :, None] * g[:, None, :] + (lam * (J - alpha))[:, None, None] * HJ
+    w, V = np.linalg.eigh(HF)
+    HF = (V * np.maximum(w, 0.0)[:, None, :]) @ np.swapaxes(V, 1, 2)
+    # dvec(F)/dx: vec(F) = (Dminv^T kron I3) vec(Ds); Ds columns x_k - x_0
+    dFdx = np.zeros((len(tets), 9, 12))
+    for col in range(3):          # column of F
+        for k in range(3):        # Ds column k = x_{k+1} - x_0
+            c = Dminv[:, k, col]
+            for d in range(3):
+                dFdx[:, col * 3 + d, (k + 1) * 3 + d] += c
+                dFdx[:, col * 3 + d, d] -= c
+    He = vol[:, None, None] * (np.swapaxes(dFdx, 1, 2) @ HF @ dFdx)
+    ge = vol[:, None] * np.einsum("tij,ti->tj", dFdx, P)
+    return He, ge, vol
+
+
+def upper_triplets(H, nodes):
+    """write_triplet_fem (SG/femEnergy.cu:14-62) for a batch: H [m,3k,3k], nodes [m,k]."""
+    m, k = nodes.shape
+    pairs = [(ii, jj) for ii in range(k) for jj in range(ii, k)]
+    rows = np.empty((m, len(pairs)), np.int64)
+    cols = np.empty((m, len(pairs)), np.int64)
+    vals = np.empty((m, len(pairs), 9))
+    for q, (ii, jj) in enumerate(pairs):
+        r, c = nodes[:, ii], nodes[:, jj]
+        swap = r > c
+        blk = H[:, 3 * ii:3 * ii + 3, 3 * jj:3 * jj + 3]          # (a, c) = H[ii*3+a, jj*3+c]
+        blkT = np.swapaxes(H[:, 3 * jj:3 * jj + 3, 3 * ii:3 * ii + 3], 1, 2)
+        # when swapped the stored block is (jj,ii) block: element (a,c) = H[jj*3+a, ii*3+c]
+        blk_sw = H[:, 3 * jj:3 * jj + 3, 3 * ii:3 * ii + 3]
+        use = np.where(swap[:, None, None], blk_sw, blk)
+        rows[:, q] = np.where(swap, c, r)
+        cols[:, q] = np.where(swap, r, c)
+        vals[:, q] = np.swapaxes(use, 1, 2).reshape(m, 9)           # column-major
+        del blkT
+    return rows.ravel(), cols.ravel(), vals.reshape(-1, 9)
+
+
+def merge_triplets(rows, cols, vals):
+    """Stable sort by (row, col) and sum duplicates (Converter::convert)."""
+    key = (rows.astype(np.uint64) << np.uint64(32)) + cols.astype(np.uint64)
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    head = np.ones(len(ks), bool)
+    head[1:] = ks[1:] != ks[:-1]
+    seg = np.cumsum(head) - 1
+    out = np.zeros((int(seg[-1]) + 1, 9))
+    np.add.at(out, seg, vals[order])
+    uk = ks[head]
+    return (uk >> np.uint64(32)).astype(np.int32), (uk & np.uint64(0xffffffff)).astype(np.int32), out
+
+
+def barrier_hessian(d, dhat, kappa, eps, normal, bary, rng):
+    """kappa*b''(d) g g^T + kappa*eps*I12 for point-triangle pairs (SPD)."""
+    bpp = (-2.0 * np.log(d / dhat) - 4.0 * (d - dhat) / d + (d - dhat) ** 2 / d ** 2)
+    g = np.concatenate([normal, -bary[:, 0:1] * normal, -bary[:, 1:2] * normal, -bary[:, 2:3] * normal], 1)
+    H = (kappa * bpp)[:, None, None] * g[:, :, None] * g[:, None, :]
+    H += kappa * eps * np.eye(12)[None]
+    return H
+
+
+def make_grid_system(nx=10, ny=10, nz=10, h=0.01, E=1e5, nu=0.4, rho=1000.0, dt=0.01,
+                     jitter=1e-4, deform=0.05, seed=0, blocks=1, gap=1e-4,
+                     n_pairs=0, dhat=1e-3, kappa=1e5, eps=1e-6, keep_raw=False):
+    """One or two stacked tet grids (+ barrier pairs between them)."""
+    rng = np.random.default_rng(seed)
+    P, T = [], []
+    off = 0
+    for k in range(blocks):
+        origin = (0.0, k * ((ny - 1) * h + gap), 0.0)
+        p, t = tet_grid(nx, ny, nz, h, origin)
+        P.append(p)
+        T.append(t + off)
+        off += len(p)
+    X = np.concatenate(P)
+    tets = np.concatenate(T)
+    n = len(X)
+    X = X + rng.normal(0.0, jitter, X.shape)
+    G = rng.normal(0.0, 1.0, (3, 3))
+    x = X + deform * (X - X.mean(0)) @ G.T + deform * h * rng.normal(0.0, 1.0, X.shape)
+    He, ge, vol = neo_hookean_elements(X, x, tets, E, nu)
+    He *= dt * dt
+    ge *= dt * dt
+    r_el, c_el, v_el = upper_triplets(He, tets)
+    mass = np.zeros(n)
+    np.add.at(mass, tets.ravel(), np.repeat(rho * vol / 4.0, 4))
+    b = np.zeros(3 * n)
+    np.add.at(b, (3 * tets[:, :, None] + np.arange(3)).ravel(), ge.ravel())
+    # mass diagonal (SG/GIPC.cu:10201-10220): m * I
+    r_m = np.arange(n)
+    v_m = np.zeros((n, 9))
+    v_m[:, 0] = v_m[:, 4] = v_m[:, 8] = mass
+    rows = [r_m, r_el]
+    cols = [r_m, c_el]
+    vals = [v_m, v_el]
+    pairs = np.zeros((0, 4), np.int32)
+    if n_pairs and blocks == 2:
+        nv1 = nx * ny * nz
+        vid = lambda x_, y_, z_, o: o + x_ + nx * (y_ + ny * z_)
+        # points: bottom face (y = 0) of the top block
+        gx, gz = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+        pts = vid(gx.ravel(), 0, gz.ravel(), nv1)
+        # triangles: top face (y = ny-1) of the bottom block, 2 per quad
+        qx, qz = np.meshgrid(np.arange(nx - 1), np.arange(nz - 1), indexing="ij")
+        qx, qz = qx.ravel(), qz.ravel()
+        a = vid(qx, ny - 1, qz, 0); b1 = vid(qx + 1, ny - 1, qz, 0)
+        c1 = vid(qx, ny - 1, qz + 1, 0); d1 = vid(qx + 1, ny - 1, qz + 1, 0)
+        tris = np.concatenate([np.stack([a, b1, d1], 1), np.stack([a, d1, c1], 1)])
+        tri_c = np.concatenate([np.stack([qx + 2 / 3, qz + 1 / 3], 1), np.stack([qx + 1 / 3, qz + 2 / 3], 1)])
+        pxz = np.stack([gx.ravel(), gz.ravel()], 1).astype(np.float64)
+        # candidate (point, triangle) pairs within 3.5 cells
+        cand = []
+        for i in range(len(pts)):
+            dd = np.abs(tri_c - pxz[i]).max(1)
+            js = np.nonzero(dd <= 3.5)[0]
+            cand.append(np.stack([np.full(len(js), i), js], 1))
+        cand = np.concatenate(cand)
+        pick = rng.choice(len(cand), size=min(n_pairs, len(cand)), replace=False)
+        cand = cand[np.sort(pick)]
+        pi, tj = cand[:, 0], cand[:, 1]
+        m = len(cand)
+        d = rng.uniform(0.0, dhat, m)
+        d = np.maximum(d, dhat * 1e-3)
+        normal = np.tile([0.0, 1.0, 0.0], (m, 1)) + rng.normal(0.0, 0.05, (m, 3))
+        normal /= np.linalg.norm(normal, axis=1, keepdims=True)
+        bary = rng.dirichlet(np.ones(3), m)
+        Hc = barrier_hessian(d, dhat, kappa, eps, normal, bary, rng) * dt * dt
+        nodes = np.stack([pts[pi], tris[tj, 0], tris[tj, 1], tris[tj, 2]], 1)
+        r_c, c_c, v_c = upper_triplets(Hc, nodes)
+        rows.append(r_c); cols.append(c_c); vals.append(v_c)
+        pairs = np.stack([-(nodes[:, 0] + 1), nodes[:, 1], nodes[:, 2], nodes[:, 3]], 1).astype(np.int32)
+    raw_r = np.concatenate(rows).astype(np.int32)
+    raw_c = np.concatenate(cols).astype(np.int32)
+    raw_v = np.concatenate(vals)
+    mr, mc, mv = merge_triplets(raw_r, raw_c, raw_v)
+    sysm = System(n_verts=n, rows=mr, cols=mc, vals=mv, b=b, pos=X, tets=tets.astype(np.int32),
+                  pairs=pairs,
+                  info=dict(nx=nx, ny=ny, nz=nz, blocks=blocks, n_pairs=len(pairs), E=E, nu=nu,
+                            dt=dt, h=h, eps=eps, kappa=kappa, dhat=dhat, seed=seed, n_tets=len(tets),
+                            n_raw=len(raw_r), n_blocks=len(mr)))
+    if keep_raw:
+        sysm.raw_rows, sysm.raw_cols, sysm.raw_vals = raw_r, raw_c, raw_v
+    return sysm
+
+
+def mesh_system(X, tets, E=1e5, nu=0.4, rho=1000.0, dt=0.01, deform=0.05, seed=0):
+    """A Neo-Hookean system on a given tet mesh (positions X [n,3], tets [t,4])."""
+    rng = np.random.default_rng(seed)
+    X = np.asarray(X, np.float64)
+    tets = np.asarray(tets, np.int64)
+    n = len(X)
+    h = float(np.median(np.linalg.norm(X[tets[:, 1]] - X[tets[:, 0]], axis=1)))
+    G = rng.normal(0.0, 1.0, (3, 3))
+    x = X + deform * (X - X.mean(0)) @ G.T + deform * h * rng.normal(0.0, 1.0, X.shape)
+    He, ge, vol = neo_hookean_elements(X, x, tets, E, nu)
+    He *= dt * dt
+    ge *= dt * dt
+    r_el, c_el, v_el = upper_triplets(He, tets)
+    mass = np.zeros(n)
+    np.add.at(mass, tets.ravel(), np.repeat(rho * vol / 4.0, 4))
+    mass = np.maximum(mass, 1e-12)
+    b = np.zeros(3 * n)
+    np.add.at(b, (3 * tets[:, :, None] + np.arange(3)).ravel(), ge.ravel())
+    v_m = np.zeros((n, 9))
+    v_m[:, 0] = v_m[:, 4] = v_m[:, 8] = mass
+    raw_r = np.concatenate([np.arange(n), r_el]).astype(np.int32)
+    raw_c = np.concatenate([np.arange(n), c_el]).astype(np.int32)
+    raw_v = np.concatenate([v_m, v_el])
+    mr, mc, mv = merge_triplets(raw_r, raw_c, raw_v)
+    return System(n_verts=n, rows=mr, cols=mc, vals=mv, b=b, pos=X, tets=tets.astype(np.int32),
+                  pairs=np.zeros((0, 4), np.int32), raw_rows=raw_r, raw_cols=raw_c, raw_vals=raw_v,
+                  info=dict(n_tets=len(tets), n_blocks=len(mr), E=E, nu=nu, dt=dt, seed=seed))
+
+
+def config1(seed=0, **kw):
+    """10x10x10 tet grid, Neo-Hookean E=1e5 nu=0.4, no contact (3,000 DOF)."""
+    return make_grid_system(10, 10, 10, 0.01, E=1e5, nu=0.4, seed=seed, **kw)
+
+
+def config2(seed=0, scale=1.0, **kw):
+    """Two 40x20x20 grids stacked 1e-4 m apart with 50k point-triangle pairs."""
+    nx, ny, nz = max(2, int(round(40 * scale))), max(2, int(round(20 * scale))), max(2, int(round(20 * scale)))
+    npairs = int(round(50000 * (nx * nz) / 800.0))
+    return make_grid_system(nx, ny, nz, 0.01, E=1e6, nu=0.45, seed=seed, blocks=2,
+                            n_pairs=npairs, **kw)
+
+
+def full_matrix(s: System):
+    """Dense (small) or scipy-sparse full symmetric matrix for direct solves."""
+    import scipy.sparse as sp
+    n = s.n_verts
+    r3 = (3 * s.rows[:, None, None] + np.arange(3)[None, :, None]) + 0 * np.arange(3)[None, None, :]
+    c3 = (3 * s.cols[:, None, None] + np.arange(3)[None, None, :]) + 0 * np.arange(3)[None, :, None]
+    v3 = s.vals.reshape(-1, 3, 3).transpose(0, 2, 1)   # column-major -> (a, c)
+    A = sp.coo_matrix((v3.ravel(), (r3.ravel(), c3.ravel())), shape=(3 * n, 3 * n)).tocsr()
+    off = s.rows != s.cols
+    AT = sp.coo_matrix((v3[off].ravel(), (r3[off].ravel(), c3[off].ravel())), shape=(3 * n, 3 * n)).tocsr().T
+    return (A + AT).tocsc()

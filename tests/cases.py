@@ -1,0 +1,55 @@
+"""Parity cases shared by the CPU and GPU tests: synthetic systems of the
+benchmark shapes (scaled to oracle-friendly sizes) and the reference's own
+METIS-partitioned meshes from tests/golden/."""
+from __future__ import annotations
+
+import functools
+import os
+
+import numpy as np
+
+from oracle import oracle as O
+from sgmas import synth
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, f"{name}.npz")))
+
+
+class Case:
+    def __init__(self, name, sysm, part_map, real_map, nb_start, nb_num, nb_list):
+        self.name = name
+        self.s = sysm
+        self.part_map = part_map
+        self.real_map = real_map
+        self.nb_start, self.nb_num, self.nb_list = nb_start, nb_num, nb_list
+
+    @property
+    def n(self):
+        return self.s.n_verts
+
+    def oracle_mas(self, pairs=True, precision=0, bank=16):
+        m = O.MAS(self.n, self.nb_start, self.nb_num, self.nb_list, self.part_map, self.real_map, bank=bank)
+        m.reorder(self.s.pairs if pairs else None)
+        m.assemble(self.s.vals, self.s.rows, self.s.cols, precision=precision)
+        return m
+
+
+@functools.lru_cache(maxsize=None)
+def build(name, bank=16):
+    if name == "c1":
+        s = synth.config1(seed=0)
+        pm, rm = O.morton_partition(s.pos, bank)
+    elif name == "c2s":
+        s = synth.config2(seed=1, scale=0.3)
+        pm, rm = O.morton_partition(s.pos, bank)
+    elif name in ("bar", "bunny2", "cube"):
+        g = golden(name)
+        s = synth.mesh_system(g["pos"], g["tets"], seed=2)
+        pm, rm = O.mas_partition(g["part"], bank)
+    else:
+        raise KeyError(name)
+    st, nn, nl = O.vert_neighbors(s.tets, s.n_verts)
+    return Case(name, s, pm, rm, st, nn, nl)
