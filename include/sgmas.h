@@ -82,7 +82,9 @@ int sgmas_create(const sgmas_config* cfg, sgmas_context** out);
 /* MASPreconditioner::FreeMAS (SG/MASPreconditioner.cu:2321-2350) + release */
 void sgmas_destroy(sgmas_context* ctx);
 const char* sgmas_last_error(const sgmas_context* ctx);
-/* the reference runs on the per-thread default stream (CMakeLists.txt:101) */
+/* the reference runs on the per-thread default stream (CMakeLists.txt:101);
+ * a new context uses a stream of its own; NULL selects the legacy default
+ * stream, as everywhere in the CUDA runtime */
 int sgmas_set_stream(sgmas_context* ctx, void* cuda_stream);
 int sgmas_synchronize(sgmas_context* ctx);
 

@@ -1054,17 +1054,49 @@ int or_mas_apply(or_mas* m, const double* r, double* z)
                         s64[d] += R64[3 * (h * b + j) + d];
                         s32[d] += R32[3 * (h * b + j) + d];
                     }
-            int nx = idx;
-            for(int level = 1; level < L; level++)
+            if(L > 1)
             {
-                nx = m->going_next[nx];
+                int nx = m->going_next[idx];
                 for(int d = 0; d < 3; d++)
                 {
-                    R64[3 * (size_t)nx + d] += s64[d];
-                    R32[3 * (size_t)nx + d] += s32[d];
+                    R64[3 * (size_t)nx + d] = s64[d];
+                    R32[3 * (size_t)nx + d] = s32[d];
                 }
             }
         }
+    /* levels >= 2: each coarse node sums its children, which all lie in one
+     * bank of the level below, lanes ascending (the reference pushes every
+     * component up the whole chain with atomics; same sums, defined order) */
+    for(int lvl = 2; lvl < L; lvl++)
+    {
+        const int beg = m->level_size[2 * (lvl - 1) + 1], cnt = m->level_size[2 * (lvl - 1)];
+        for(int k = 0; k * b < cnt; k++)
+            for(int lane = 0; lane < b && k * b + lane < cnt; lane++)
+            {
+                const int node = beg + k * b + lane;
+                const int par  = m->going_next[node];
+                int lead       = 1;
+                for(int j = 0; j < lane; j++)
+                    if(m->going_next[beg + k * b + j] == par)
+                        lead = 0;
+                if(!lead)
+                    continue;
+                double s64[3] = {0, 0, 0};
+                float  s32[3] = {0, 0, 0};
+                for(int j = lane; j < b && k * b + j < cnt; j++)
+                    if(m->going_next[beg + k * b + j] == par)
+                        for(int d = 0; d < 3; d++)
+                        {
+                            s64[d] += R64[3 * (size_t)(beg + k * b + j) + d];
+                            s32[d] += R32[3 * (size_t)(beg + k * b + j) + d];
+                        }
+                for(int d = 0; d < 3; d++)
+                {
+                    R64[3 * (size_t)par + d] = s64[d];
+                    R32[3 * (size_t)par + d] = s32[d];
+                }
+            }
+    }
     /* Schwarz: per bank z = P r, columns ascending, fma chains */
     const size_t bsym = (size_t)m->bsym;
 #pragma omp parallel for schedule(static)

@@ -77,7 +77,8 @@ void free_all(sgmas_context* c) {
                     c->d_coarse_table, c->d_hess, c->d_inv, c->d_R, c->d_Z, c->bsr.row_ptr, c->bsr.cols,
                     c->bsr.src, c->bsr.vals, c->bsr.cnt, c->bsr.cnt_lower, c->bsr.fill, c->bsr.first, c->d_r,
                     c->d_z, c->d_p0, c->d_p1, c->d_Ap, c->d_diag_inv, c->d_abd_inv, c->d_partials, c->d_ticket,
-                    c->d_state, c->d_hvals, c->d_hb, c->d_hx, c->d_hrows, c->d_hcols, c->d_sort_scratch};
+                    c->d_state, c->d_hvals, c->d_hb, c->d_hx, c->d_hrows, c->d_hcols, c->d_sort_scratch,
+                    c->d_coarse_ticket, c->bsr.row_list, c->bsr.d_nlong, c->bsr.tcols, c->bsr.tsrc};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -132,7 +133,7 @@ const char* sgmas_last_error(const sgmas_context* c) { return c ? c->err.c_str()
 
 int sgmas_set_stream(sgmas_context* c, void* stream) {
     if (!c) return SGMAS_ERR_ARG;
-    c->stream = stream ? (cudaStream_t)stream : c->cap_stream;
+    c->stream = (cudaStream_t)stream;  // NULL is the legacy default stream, as in the CUDA runtime
     return SGMAS_OK;
 }
 
@@ -177,8 +178,9 @@ int sgmas_mas_init(sgmas_context* c, int vert_num, int collision_node_offset, in
         ctx_alloc(c, &c->d_prefix_orig, part_map_size / B) || ctx_alloc(c, &c->d_bank_cnt, part_map_size / B + N / B + 2) ||
         ctx_alloc(c, &c->d_bank_pre, part_map_size / B + N / B + 2) || ctx_alloc(c, &c->d_coarse_space, (size_t)N * c->L) ||
         ctx_alloc(c, &c->d_going_next, c->gn_cap) || ctx_alloc(c, &c->d_level_size, 2 * (kMaxLevels + 2)) ||
-        ctx_alloc(c, &c->d_coarse_table, (size_t)kMaxLevels * N))
+        ctx_alloc(c, &c->d_coarse_table, (size_t)kMaxLevels * N) || ctx_alloc(c, &c->d_coarse_ticket, 1))
         return SGMAS_ERR_CUDA;
+    SG_CUDA(c, cudaMemsetAsync(c->d_coarse_ticket, 0, sizeof(unsigned), c->stream));
     cudaStream_t s = c->stream;
     if (nb_size > 0) SG_CUDA(c, cudaMemcpyAsync(c->d_nb_list0, nb_list, sizeof(unsigned) * nb_size, cudaMemcpyHostToDevice, s));
     SG_CUDA(c, cudaMemcpyAsync(c->d_nb_num0, nb_num, sizeof(unsigned) * N, cudaMemcpyHostToDevice, s));
@@ -219,6 +221,10 @@ static int mas_assemble_impl(sgmas_context* c, const double* vals, const int* ro
     if (c->total > c->cap_total) {
         rc = alloc_mas_matrices(c, c->total);
         if (rc) return rc;
+    } else {
+        // padding nodes of a rebuilt hierarchy must hold finite values: they
+        // meet exact zeros of the inverses in the Schwarz products
+        SG_CUDA(c, cudaMemsetAsync(c->d_R, 0, 3 * (size_t)c->total * acc_size(c->precision), c->stream));
     }
     rc = mas_scatter_and_invert(c, vals, rows, cols, indices, offset, n);
     if (rc) return rc;

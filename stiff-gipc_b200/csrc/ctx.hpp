@@ -30,7 +30,23 @@ struct BsrMatrix {
     int* cnt_lower = nullptr;         // [nrows]
     int* fill = nullptr;              // [nrows]
     int* first = nullptr;             // [nrows] first upper block of each row
+    int* tcols = nullptr;             // [cap] lower entries in claim order (scratch)
+    uint32_t* tsrc = nullptr;         // [cap]
+    int* row_list = nullptr;          // [nrows] long rows first, then short rows (row order)
+    int* d_nlong = nullptr;           // [1]
+    int n_long = 0;                   // rows handled by a whole warp
     int rows_cap = 0;
+};
+
+// kernel-argument view of a BsrMatrix
+struct BsrView {
+    const int* row_ptr;
+    const int* cols;
+    const double* vals;
+    long long cap;
+    const int* row_list;
+    int nrows;
+    int n_long;
 };
 
 struct sgmas_context {
@@ -75,6 +91,7 @@ struct sgmas_context {
     int vec_cap = 0, diag_cap = 0, abd_cap = 0;
     double* d_partials = nullptr;     // reduction partials
     unsigned* d_ticket = nullptr;
+    unsigned* d_coarse_ticket = nullptr;  // last-CTA ticket of the coarse MAS kernel
     int partial_cap = 0;
     PcgState* d_state = nullptr;
     // uploaded host systems (sgmas_pcg_solve_host)

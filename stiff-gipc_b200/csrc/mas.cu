@@ -12,6 +12,8 @@
 //    product and the component sums of the residual into one kernel.
 #include <stdio.h>
 
+#include <algorithm>
+
 #include "../../include/sgmas.h"
 #include "ctx.hpp"
 #include "pcg_state.cuh"
@@ -21,6 +23,7 @@ using namespace sgmas;
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kCollectThreads = 128;
 
 __host__ __device__ constexpr int bsym_of(int B) { return B * (B + 1) / 2; }
 __host__ __device__ __forceinline__ int sym_index(int B, int r, int c) { return B * r - r * (r + 1) / 2 + c; }
@@ -293,111 +296,167 @@ __device__ __forceinline__ double* blk_ptr(double* hess, int r, int c) {
     return hess + ((size_t)(c / B) * bsym_of(B) + sym_index(B, r % B, c % B)) * 9;
 }
 
-// phase 1: every FEM block.  Same-bank blocks are stored (transposed when the
-// column slot precedes the row slot -- the reference drops that case, which
-// its own slot maps never produce); other blocks climb goingNext and add into
-// each level where both ends share a bank.
-template <int B>
-__global__ void k_scatter1(int n, const double* __restrict__ vals, const int* __restrict__ rows,
-                           const int* __restrict__ cols, const uint32_t* __restrict__ indices, int offset, int N,
-                           int L, const int* __restrict__ real_map, const int* __restrict__ going_next,
-                           double* hess, const int* __restrict__ level_size, int* err) {
-    const int I = blockIdx.x * blockDim.x + threadIdx.x;
-    if (I >= n) return;
-    const int k = indices ? (int)indices[I] : I;
-    const int rr = rows[k] - offset, cc = cols[k] - offset;
-    if (rr < 0 || rr >= N || cc < 0 || cc >= N) return;
-    const int total = level_size[2 * L + 1];
-    double H[9];
-    #pragma unroll
-    for (int q = 0; q < 9; ++q) H[q] = vals[(size_t)9 * k + q];
-    const int sr = real_map[rr], sc = real_map[cc];
-    if (sr / B == sc / B) {
-        if (sc >= sr) {
-            double* D = blk_ptr<B>(hess, sr, sc);
+// Add 9 values into the block of the warp's group of lanes that share `key`
+// (one set of atomics per group instead of per lane).
+__device__ __forceinline__ void warp_grouped_add(long long key, const double (&m)[9], double* hess) {
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int lane = threadIdx.x & 31;
+    double s[9];
+    if (peers == 0xffffffffu) {  // whole warp on one target: butterfly sum
+        #pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            double v = m[q];
             #pragma unroll
-            for (int q = 0; q < 9; ++q) D[q] = H[q];
-        } else {
-            double* D = blk_ptr<B>(hess, sc, sr);
-            #pragma unroll
-            for (int i = 0; i < 3; ++i)
-                #pragma unroll
-                for (int j = 0; j < 3; ++j) D[i + 3 * j] = H[j + 3 * i];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            s[q] = v;
         }
-        return;
-    }
-    int vr = rr, vc = cc;
-    for (int level = 1; level < L; ++level) {
-        vr = going_next[vr];
-        vc = going_next[vc];
-        if (vr >= total || vc >= total || vr < 0 || vc < 0) { set_error(err, kDevBadIndex); return; }
-        if (vr / B != vc / B) continue;
-        if (vc >= vr) {
-            double* D = blk_ptr<B>(hess, vr, vc);
+    } else {
+        #pragma unroll
+        for (int q = 0; q < 9; ++q) s[q] = 0.0;
+        for (int j = 0; j < 32; ++j) {
+            const bool mine = (peers >> j) & 1u;
             #pragma unroll
-            for (int q = 0; q < 9; ++q) atomicAdd(D + q, H[q]);
-            if (vc == vr) {
-                #pragma unroll
-                for (int i = 0; i < 3; ++i)
-                    #pragma unroll
-                    for (int j = 0; j < 3; ++j) atomicAdd(D + i + 3 * j, H[j + 3 * i]);
+            for (int q = 0; q < 9; ++q) {
+                const double v = __shfl_sync(0xffffffffu, m[q], j);
+                if (mine) s[q] += v;
             }
-        } else {
-            double* D = blk_ptr<B>(hess, vc, vr);
-            #pragma unroll
-            for (int i = 0; i < 3; ++i)
-                #pragma unroll
-                for (int j = 0; j < 3; ++j) atomicAdd(D + i + 3 * j, H[j + 3 * i]);
         }
+    }
+    if (key >= 0 && (peers & lanemask_lt(lane)) == 0) {
+        double* D = hess + key * 9;
+        #pragma unroll
+        for (int q = 0; q < 9; ++q) atomicAdd(D + q, s[q]);
     }
 }
 
-// phase 2: one CTA of B*B threads per level-0 bank; thread (r, c).
+// phase 1: every FEM block.  Same-bank blocks are stored (transposed when the
+// column slot precedes the row slot -- the reference drops that case, which
+// its own slot maps never produce); other blocks climb goingNext and add into
+// each level where both ends share a bank, summed per warp per target block.
 template <int B>
-__global__ void k_scatter2(int nbank0, int L, const int* __restrict__ part_map, const int* __restrict__ prefix_orig,
-                           const int* __restrict__ going_next, double* hess) {
-    __shared__ double sh[32];
-    __shared__ int lead;
-    const int h = blockIdx.x;
-    const int r = threadIdx.x / B, c = threadIdx.x % B;
-    const int rdx = part_map[h * B + r], cdx = part_map[h * B + c];
-    const bool ok = rdx >= 0 && cdx >= 0;
-    const int prefix = prefix_orig[h];
-    double m[9];
-    const double* T = hess + ((size_t)h * bsym_of(B) + sym_index(B, c >= r ? r : c, c >= r ? c : r)) * 9;
-    #pragma unroll
-    for (int i = 0; i < 3; ++i)
+__global__ void __launch_bounds__(256) k_scatter1(int n, const double* __restrict__ vals, const int* __restrict__ rows,
+                                                  const int* __restrict__ cols, const uint32_t* __restrict__ indices,
+                                                  int offset, int N, int L, const int* __restrict__ real_map,
+                                                  const int* __restrict__ going_next, double* hess,
+                                                  const int* __restrict__ level_size, int* err) {
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    bool live = I < n;  // every lane stays for the warp-level sums
+    int rr = 0, cc = 0;
+    double H[9];
+    if (live) {
+        const int k = indices ? (int)indices[I] : I;
+        rr = rows[k] - offset;
+        cc = cols[k] - offset;
+        live = rr >= 0 && rr < N && cc >= 0 && cc < N;
         #pragma unroll
-        for (int j = 0; j < 3; ++j) m[i + 3 * j] = ok ? (c >= r ? T[i + 3 * j] : T[j + 3 * i]) : 0.0;
-    if (prefix == 1) {
-        if (threadIdx.x == 0) {
-            lead = -1;
-            for (int q = 0; q < B; ++q)
-                if (part_map[h * B + q] >= 0) { lead = part_map[h * B + q]; break; }
-        }
-        double s[9];
+        for (int q = 0; q < 9; ++q) H[q] = live ? vals[(size_t)9 * k + q] : 0.0;
+    } else {
         #pragma unroll
-        for (int q = 0; q < 9; ++q) s[q] = block_sum<B * B>(m[q], sh);
-        if (threadIdx.x == 0 && lead >= 0) {
-            int nx = going_next[lead];
-            for (int level = 1; level < L; ++level) {
-                double* D = blk_ptr<B>(hess, nx, nx);
+        for (int q = 0; q < 9; ++q) H[q] = 0.0;
+    }
+    const int total = level_size[2 * L + 1];
+    int sr = 0, sc = 0;
+    if (live) {
+        sr = real_map[rr];
+        sc = real_map[cc];
+        if (sr / B == sc / B) {
+            if (sc >= sr) {
+                double* D = blk_ptr<B>(hess, sr, sc);
                 #pragma unroll
-                for (int q = 0; q < 9; ++q) atomicAdd(D + q, s[q]);
-                nx = going_next[nx];
+                for (int q = 0; q < 9; ++q) D[q] = H[q];
+            } else {
+                double* D = blk_ptr<B>(hess, sc, sr);
+                #pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    #pragma unroll
+                    for (int j = 0; j < 3; ++j) D[i + 3 * j] = H[j + 3 * i];
+            }
+            live = false;
+        }
+    }
+    if (__ballot_sync(0xffffffffu, live) == 0u) return;
+    int vr = rr, vc = cc;
+    for (int level = 1; level < L; ++level) {
+        long long key = -1;
+        double m[9];
+        if (live) {
+            vr = going_next[vr];
+            vc = going_next[vc];
+            if (vr >= total || vc >= total || vr < 0 || vc < 0) {
+                set_error(err, kDevBadIndex);
+                live = false;
             }
         }
-        return;
+        if (live && vr / B == vc / B) {
+            if (vc >= vr) {
+                key = ((long long)(vc / B) * bsym_of(B) + sym_index(B, vr % B, vc % B));
+                #pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    #pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        m[i + 3 * j] = H[i + 3 * j] + (vc == vr ? H[j + 3 * i] : 0.0);
+            } else {
+                key = ((long long)(vr / B) * bsym_of(B) + sym_index(B, vc % B, vr % B));
+                #pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    #pragma unroll
+                    for (int j = 0; j < 3; ++j) m[i + 3 * j] = H[j + 3 * i];
+            }
+        } else {
+            #pragma unroll
+            for (int q = 0; q < 9; ++q) m[q] = 0.0;
+        }
+        warp_grouped_add(key, m, hess);
     }
-    if (!ok) return;
-    int vr = rdx, vc = cdx;
+}
+
+// phase 2: one CTA of B*B threads per level-0 bank; thread (r, c).  A bank's
+// vertices share one coarse node per level-0 component, so the bank's blocks
+// are first summed per component pair in shared memory and each component
+// pair climbs goingNext once (same sums as the reference's per-pair climb).
+template <int B>
+__global__ void k_scatter2(int nbank0, int L, const int* __restrict__ part_map, const unsigned* __restrict__ fine_mask,
+                           const int* __restrict__ going_next, double* hess) {
+    extern __shared__ double S[];  // [B][B][9] component-pair sums
+    __shared__ int comp_of[B], lead_vertex[B], ncomp;
+    const int h = blockIdx.x;
+    const int r = threadIdx.x / B, c = threadIdx.x % B;
+    if (threadIdx.x < 32) {
+        const int t = threadIdx.x;
+        const int idx = t < B ? part_map[h * B + t] : -1;
+        const unsigned msk = idx >= 0 ? fine_mask[idx] : 0u;
+        const bool leader = idx >= 0 && __popc(msk & lanemask_lt(t)) == 0;
+        const unsigned lb = __ballot_sync(0xffffffffu, leader);
+        if (t < B) {
+            comp_of[t] = idx >= 0 ? __popc(lb & lanemask_lt(__ffs(msk) - 1)) : -1;
+            if (leader) lead_vertex[__popc(lb & lanemask_lt(t))] = idx;
+        }
+        if (t == 0) ncomp = __popc(lb);
+    }
+    for (int q = threadIdx.x; q < B * B * 9; q += blockDim.x) S[q] = 0.0;
+    __syncthreads();
+    const int cr = comp_of[r], ccp = comp_of[c];
+    if (cr >= 0 && ccp >= 0) {
+        const double* T = hess + ((size_t)h * bsym_of(B) + sym_index(B, c >= r ? r : c, c >= r ? c : r)) * 9;
+        double* D = S + (cr * B + ccp) * 9;
+        #pragma unroll
+        for (int i = 0; i < 3; ++i)
+            #pragma unroll
+            for (int j = 0; j < 3; ++j) atomicAdd(D + i + 3 * j, c >= r ? T[i + 3 * j] : T[j + 3 * i]);
+    }
+    __syncthreads();
+    const int nc = ncomp;
+    if ((int)threadIdx.x >= nc * nc) return;
+    const int a = threadIdx.x / nc, b = threadIdx.x % nc;
+    const double* M = S + (a * B + b) * 9;
+    int vr = lead_vertex[a], vc = lead_vertex[b];
     for (int level = 1; level < L; ++level) {
         vr = going_next[vr];
         vc = going_next[vc];
         if (vr / B == vc / B && vc >= vr) {
             double* D = blk_ptr<B>(hess, vr, vc);
             #pragma unroll
-            for (int q = 0; q < 9; ++q) atomicAdd(D + q, m[q]);
+            for (int q = 0; q < 9; ++q) atomicAdd(D + q, M[q]);
         }
     }
 }
@@ -515,34 +574,60 @@ __device__ __forceinline__ bool stage_tiles(S* tile, const S* src, int nb, int b
     return mbar_wait(bar, 0, err);
 }
 
-constexpr int kApplyThreads = 128;
+constexpr int kL0Banks = 4;         // level-0 banks per CTA of the level-0 kernel
+constexpr int kCoarseThreads = 256;  // threads per CTA of the coarse kernel
+constexpr int kCoarseSmem = 80 * 1024;
 
-// Level-0 kernel: (mode 1: x += alpha p, r -= alpha Ap first) r -> Acc,
-// level-0 Schwarz from the staged tile, component sums pushed up the chain
-// (BuildMultiLevelR :727-845 with the level-0 part of _schwarzLocalXSym6).
+template <int B>
+__host__ __device__ constexpr int coarse_bpc() { return kCoarseThreads / B; }
+
+// Sum `v` over the lanes of this bank that share `key` (lanes ascending, the
+// order the oracle restates); *lead = lowest lane of its group.
+template <int B, typename Acc>
+__device__ __forceinline__ void group_sum(int key, Acc v0, Acc v1, Acc v2, int lane, Acc& s0, Acc& s1, Acc& s2,
+                                          bool& lead) {
+    s0 = 0; s1 = 0; s2 = 0;
+    lead = key >= 0;
+    #pragma unroll 4
+    for (int j = 0; j < B; ++j) {
+        const int kj = __shfl_sync(0xffffffffu, key, j, B);
+        const Acc y0 = shfl_acc(v0, j, B), y1 = shfl_acc(v1, j, B), y2 = shfl_acc(v2, j, B);
+        if (key >= 0 && kj == key) {
+            s0 += y0; s1 += y1; s2 += y2;
+            if (j < lane) lead = false;
+        }
+    }
+}
+
+// Level-0 kernel (BuildMultiLevelR :727-845 + the level-0 part of
+// _schwarzLocalXSym6 :954-1024): mode 1 first applies the PCG update
+// x += alpha p, r -= alpha Ap for the bank's vertices; then r -> Acc, the
+// level-0 Schwarz product from the staged tile, and each level-0 component's
+// residual sum stored into its level-1 node (a level-1 node has exactly one
+// level-0 component, so plain stores suffice -- no atomics).
 template <int B, typename S, typename Acc>
-__global__ void __launch_bounds__(kApplyThreads) k_apply_l0(int Mm, int L, const int* __restrict__ part_map,
-                                                            const unsigned* __restrict__ fine_mask,
-                                                            const int* __restrict__ going_next, const S* __restrict__ inv,
-                                                            double* r, Acc* R, Acc* Z, int mode, double* x,
-                                                            const double* __restrict__ p, const double* __restrict__ Ap,
-                                                            const PcgState* st, int* err) {
+__global__ void __launch_bounds__(kL0Banks * B) k_apply_l0(int Mm, int L, const int* __restrict__ part_map,
+                                                          const unsigned* __restrict__ fine_mask,
+                                                          const int* __restrict__ going_next, const S* __restrict__ inv,
+                                                          double* r, Acc* R, Acc* Z, int mode, double* x,
+                                                          const double* __restrict__ p, const double* __restrict__ Ap,
+                                                          const PcgState* st, int* err) {
     if (st && st->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t bar;
     constexpr int bs = bsym_of(B);
-    constexpr int BPC = kApplyThreads / B;
     S* tile = reinterpret_cast<S*>(smem_raw);
-    const int bank0 = blockIdx.x * BPC;
-    const int nbank = Mm / B;
-    const int nb = min(BPC, nbank - bank0);
+    const int bank0 = blockIdx.x * kL0Banks;
+    const int nb = min(kL0Banks, Mm / B - bank0);
     const bool ok = stage_tiles<S>(tile, inv + (size_t)bank0 * bs * 9, nb, bs, &bar, err);
 
-    const int tdx = blockIdx.x * kApplyThreads + threadIdx.x;
+    const int tdx = blockIdx.x * (kL0Banks * B) + threadIdx.x;
     const int lane = threadIdx.x % B;
     const int idx = tdx < Mm ? part_map[tdx] : -1;
     double rv0 = 0.0, rv1 = 0.0, rv2 = 0.0;
+    unsigned msk = 0u;
     if (idx >= 0) {
+        msk = fine_mask[idx];
         double* rp = r + 3 * (size_t)idx;
         rv0 = rp[0]; rv1 = rp[1]; rv2 = rp[2];
         if (mode == 1) {
@@ -556,72 +641,142 @@ __global__ void __launch_bounds__(kApplyThreads) k_apply_l0(int Mm, int L, const
         }
     }
     const Acc r0 = (Acc)rv0, r1 = (Acc)rv1, r2 = (Acc)rv2;
-    // component sums (members ascending) and the push up the chain
-    const unsigned msk = idx >= 0 ? fine_mask[idx] : 0u;
     Acc s0 = 0, s1 = 0, s2 = 0;
     #pragma unroll 4
     for (int j = 0; j < B; ++j) {
         const Acc y0 = shfl_acc(r0, j, B), y1 = shfl_acc(r1, j, B), y2 = shfl_acc(r2, j, B);
         if (msk & (1u << j)) { s0 += y0; s1 += y1; s2 += y2; }
     }
-    if (idx >= 0 && __popc(msk & lanemask_lt(lane)) == 0) {
-        int nx = idx;
-        for (int level = 1; level < L; ++level) {
-            nx = going_next[nx];
-            atomicAdd(R + 3 * (size_t)nx, s0);
-            atomicAdd(R + 3 * (size_t)nx + 1, s1);
-            atomicAdd(R + 3 * (size_t)nx + 2, s2);
-        }
+    if (idx >= 0 && L > 1 && __popc(msk & lanemask_lt(lane)) == 0) {
+        const int nx = going_next[idx];
+        R[3 * (size_t)nx] = s0; R[3 * (size_t)nx + 1] = s1; R[3 * (size_t)nx + 2] = s2;
     }
     if (!ok) return;
     Acc z0, z1, z2;
-    const int lb = threadIdx.x / B;
-    schwarz_rows<B, S, Acc>(tile + (size_t)lb * bs * 9, lane, r0, r1, r2, z0, z1, z2);
+    schwarz_rows<B, S, Acc>(tile + (size_t)(threadIdx.x / B) * bs * 9, lane, r0, r1, r2, z0, z1, z2);
     if (tdx < Mm) {
         Z[3 * (size_t)tdx] = z0; Z[3 * (size_t)tdx + 1] = z1; Z[3 * (size_t)tdx + 2] = z2;
     }
 }
 
-// Coarse banks: z = P r for every bank of levels >= 1 (_schwarzLocalXSym6).
+// Schwarz products for `nbk` consecutive banks starting at `bank0`, staged in
+// chunks of at most `chunk` tiles.  With PUSH, each bank's residuals are
+// also summed per parent node (the children of a node of the next level
+// all lie in one bank) and stored into the parent.
+template <int B, typename S, typename Acc, bool PUSH>
+__device__ __forceinline__ bool schwarz_banks(const S* __restrict__ inv, Acc* R, Acc* Z,
+                                              const int* __restrict__ going_next, int node_end, int bank0, int nbk,
+                                              int chunk, S* tile, uint64_t* bar, unsigned& phase, int* err) {
+    constexpr int bs = bsym_of(B);
+    const int per_pass = blockDim.x / B;
+    const int lane = threadIdx.x % B;
+    for (int c0 = 0; c0 < nbk; c0 += chunk) {
+        const int nc = min(chunk, nbk - c0);
+        __syncthreads();  // the previous chunk's tiles are no longer read
+        if (threadIdx.x == 0) {
+            const unsigned bytes = (unsigned)(nc * bs * 9 * sizeof(S));
+            mbar_expect_tx(bar, bytes);
+            bulk_g2s(tile, inv + (size_t)(bank0 + c0) * bs * 9, bytes, bar);
+        }
+        if (!mbar_wait(bar, phase, err)) return false;
+        phase ^= 1u;
+        for (int q = threadIdx.x / B; q < ((nc + per_pass - 1) / per_pass) * per_pass; q += per_pass) {
+            const bool valid = q < nc;
+            const int node = (bank0 + c0 + q) * B + lane;
+            const Acc v0 = valid ? __ldcg(R + 3 * (size_t)node) : (Acc)0;
+            const Acc v1 = valid ? __ldcg(R + 3 * (size_t)node + 1) : (Acc)0;
+            const Acc v2 = valid ? __ldcg(R + 3 * (size_t)node + 2) : (Acc)0;
+            if (PUSH) {
+                const int par = (valid && node < node_end) ? going_next[node] : -1;
+                Acc s0, s1, s2;
+                bool lead;
+                group_sum<B, Acc>(par, v0, v1, v2, lane, s0, s1, s2, lead);
+                if (lead) { R[3 * (size_t)par] = s0; R[3 * (size_t)par + 1] = s1; R[3 * (size_t)par + 2] = s2; }
+            }
+            Acc z0, z1, z2;
+            schwarz_rows<B, S, Acc>(tile + (size_t)(valid ? q : 0) * bs * 9, lane, v0, v1, v2, z0, z1, z2);
+            if (valid) { Z[3 * (size_t)node] = z0; Z[3 * (size_t)node + 1] = z1; Z[3 * (size_t)node + 2] = z2; }
+        }
+    }
+    return true;
+}
+
+// Coarse levels (_schwarzLocalXSym6 for levels >= 1).  Each CTA applies a
+// run of level-1 banks and sums their residuals into the level-2 nodes; the
+// CTA that finishes last (a ticket, nothing waits) then builds levels >= 3
+// the same way, bank by bank, and applies the banks of levels >= 2.
 template <int B, typename S, typename Acc>
-__global__ void __launch_bounds__(kApplyThreads) k_apply_coarse(int Mm, int L, const int* __restrict__ level_size,
-                                                                const S* __restrict__ inv, const Acc* __restrict__ R,
-                                                                Acc* Z, const PcgState* st, int* err) {
+__global__ void __launch_bounds__(kCoarseThreads) k_apply_coarse(int L, const int* __restrict__ level_size,
+                                                                 const int* __restrict__ going_next,
+                                                                 const S* __restrict__ inv, Acc* R, Acc* Z,
+                                                                 const PcgState* st, unsigned* ticket, int* err) {
     if (st && st->done) return;
+    if (L < 2) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t bar;
+    __shared__ bool am_last;
     constexpr int bs = bsym_of(B);
-    constexpr int BPC = kApplyThreads / B;
-    const int total = level_size[2 * L + 1];
-    const int first = round_up(Mm, B) / B;
-    const int nbank = total / B;
-    const int bank0 = first + blockIdx.x * BPC;
-    if (bank0 >= nbank) return;
-    const int nb = min(BPC, nbank - bank0);
+    constexpr int BPC = coarse_bpc<B>();
     S* tile = reinterpret_cast<S*>(smem_raw);
-    const bool ok = stage_tiles<S>(tile, inv + (size_t)bank0 * bs * 9, nb, bs, &bar, err);
-    const int lb = threadIdx.x / B, lane = threadIdx.x % B;
-    const int node = (bank0 + lb) * B + lane;
-    const bool valid = bank0 + lb < nbank;
-    const Acc r0 = valid ? R[3 * (size_t)node] : (Acc)0;
-    const Acc r1 = valid ? R[3 * (size_t)node + 1] : (Acc)0;
-    const Acc r2 = valid ? R[3 * (size_t)node + 2] : (Acc)0;
-    if (!ok) return;
-    Acc z0, z1, z2;
-    schwarz_rows<B, S, Acc>(tile + (size_t)(valid ? lb : 0) * bs * 9, lane, r0, r1, r2, z0, z1, z2);
-    if (valid) {
-        Z[3 * (size_t)node] = z0; Z[3 * (size_t)node + 1] = z1; Z[3 * (size_t)node + 2] = z2;
+    const int chunk = max(1, min(BPC, (int)(kCoarseSmem / (bs * 9 * sizeof(S)))));
+    const int total = level_size[2 * L + 1];
+    const int beg1 = level_size[3], cnt1 = level_size[2];
+    const int b1 = beg1 / B;                                    // first level-1 bank
+    const int b2 = (L > 2 ? level_size[5] : total) / B;         // first level-2 bank
+    const int active = (b2 - b1 + BPC - 1) / BPC;               // CTAs with level-1 work
+    if ((int)blockIdx.x >= active) return;
+    const int bank0 = b1 + blockIdx.x * BPC;
+    unsigned phase = 0u;
+    if (threadIdx.x == 0) { mbar_init(&bar, 1); fence_mbar_init(); }
+    bool ok;
+    if (L > 2)
+        ok = schwarz_banks<B, S, Acc, true>(inv, R, Z, going_next, beg1 + cnt1, bank0, min(BPC, b2 - bank0), chunk,
+                                            tile, &bar, phase, err);
+    else
+        ok = schwarz_banks<B, S, Acc, false>(inv, R, Z, going_next, 0, bank0, min(BPC, b2 - bank0), chunk, tile,
+                                             &bar, phase, err);
+    if (!ok || L <= 2) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        am_last = atomicAdd(ticket, 1u) == (unsigned)(active - 1);
     }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    // levels >= 3 from level 2, bank by bank (uniform trip counts per warp)
+    const int lane = threadIdx.x % B;
+    const int warp = threadIdx.x / 32, nwarp = blockDim.x / 32;
+    constexpr int HPW = 32 / B;
+    for (int lvl = 3; lvl < L; ++lvl) {
+        const int beg = level_size[2 * (lvl - 1) + 1], cnt = level_size[2 * (lvl - 1)];
+        const int nbk = (cnt + B - 1) / B;
+        for (int kk = warp * HPW; kk < nbk; kk += nwarp * HPW) {
+            const int k = kk + (threadIdx.x % 32) / B;
+            const bool valid = k < nbk && k * B + lane < cnt;
+            const int node = beg + k * B + lane;
+            const Acc v0 = valid ? __ldcg(R + 3 * (size_t)node) : (Acc)0;
+            const Acc v1 = valid ? __ldcg(R + 3 * (size_t)node + 1) : (Acc)0;
+            const Acc v2 = valid ? __ldcg(R + 3 * (size_t)node + 2) : (Acc)0;
+            const int par = valid ? going_next[node] : -1;
+            Acc s0, s1, s2;
+            bool lead;
+            group_sum<B, Acc>(par, v0, v1, v2, lane, s0, s1, s2, lead);
+            if (lead) { R[3 * (size_t)par] = s0; R[3 * (size_t)par + 1] = s1; R[3 * (size_t)par + 2] = s2; }
+        }
+        __syncthreads();
+    }
+    schwarz_banks<B, S, Acc, false>(inv, R, Z, going_next, 0, b2, total / B - b2, chunk, tile, &bar, phase, err);
+    if (threadIdx.x == 0) *ticket = 0u;
 }
 
 }  // namespace
 
 namespace {
 
-// CollectFinalZ (:848-877) + r.z and r.r (kind >= 1) + clearing the coarse
-// accumulators for the next apply.
+// CollectFinalZ (:848-877) + r.z and r.r (kind >= 1).
 template <typename Acc>
-__global__ void __launch_bounds__(kThreads) k_collect(int N, int L, int Mm, const int* __restrict__ level_size,
+__global__ void __launch_bounds__(kCollectThreads) k_collect(int N, int L, int Mm, const int* __restrict__ level_size,
                                                       const int* __restrict__ real_map,
                                                       const int* __restrict__ coarse_table, const Acc* __restrict__ Z,
                                                       Acc* R, const double* __restrict__ r, double* z, int kind,
@@ -651,17 +806,9 @@ __global__ void __launch_bounds__(kThreads) k_collect(int N, int L, int Mm, cons
             rr = r0 * r0 + r1 * r1 + r2 * r2;
         }
     }
-    // clear the coarse accumulators (levels >= 1) for the next apply
-    const int total = level_size[2 * L + 1];
-    {
-        const size_t beg = 3 * (size_t)level_size[3];  // begin of level 1
-        const size_t end = 3 * (size_t)total;
-        for (size_t i = beg + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += (size_t)gridDim.x * blockDim.x)
-            R[i] = (Acc)0;
-    }
     if (kind < 1) return;
-    const double brz = block_sum<kThreads>(rz, sh);
-    const double brr = block_sum<kThreads>(rr, sh);
+    const double brz = block_sum<kCollectThreads>(rz, sh);
+    const double brr = block_sum<kCollectThreads>(rr, sh);
     __shared__ bool am_last;
     if (threadIdx.x == 0) {
         partials[blockIdx.x] = brz;
@@ -673,12 +820,12 @@ __global__ void __launch_bounds__(kThreads) k_collect(int N, int L, int Mm, cons
     if (!am_last) return;
     __threadfence();
     double s1 = 0.0, s2 = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += kThreads) {
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += kCollectThreads) {
         s1 += ((volatile double*)partials)[i];
         s2 += ((volatile double*)partials)[gridDim.x + i];
     }
-    s1 = block_sum<kThreads>(s1, sh);
-    s2 = block_sum<kThreads>(s2, sh);
+    s1 = block_sum<kCollectThreads>(s1, sh);
+    s2 = block_sum<kCollectThreads>(s2, sh);
     if (threadIdx.x == 0) {
         *ticket = 0u;
         pcg_end_iteration(st, s1, s2, kind, set_cond, cond);
@@ -736,11 +883,15 @@ int scatter_invert_t(sgmas_context* c, const double* vals, const int* rows, cons
     const size_t bs = bsym_of(B);
     SG_CUDA(c, cudaMemsetAsync(c->d_hess, 0, sizeof(double) * nblk * bs * 9, s));
     if (n > 0)
-        k_scatter1<B><<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+        k_scatter1<B><<<(n + 255) / 256, 256, 0, s>>>(
             n, vals, rows, cols, indices, offset, c->N, c->L, c->d_real_map, c->d_going_next, c->d_hess,
             c->d_level_size, c->d_err);
-    k_scatter2<B><<<c->Mm / B, B * B, 0, s>>>(c->Mm / B, c->L, c->d_part_map, c->d_prefix_orig, c->d_going_next,
-                                             c->d_hess);
+    {
+        const size_t smem2 = (size_t)B * B * 9 * sizeof(double);
+        SG_CUDA(c, cudaFuncSetAttribute(k_scatter2<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+        k_scatter2<B><<<c->Mm / B, B * B, smem2, s>>>(c->Mm / B, c->L, c->d_part_map, c->d_fine_mask, c->d_going_next,
+                                                     c->d_hess);
+    }
     constexpr int W = inv_warps<B>();
     const size_t smem = (size_t)W * (9 * B * B + 3 * B) * sizeof(double);
     auto kern = k_invert<B, S>;
@@ -755,26 +906,28 @@ int apply_t(sgmas_context* c, const double* r, double* z, int mode, const PcgSta
             const double* Ap, double* partials, unsigned* ticket, int kind, unsigned long long cond, int* launches) {
     cudaStream_t s = c->stream;
     constexpr int bs = bsym_of(B);
-    constexpr int BPC = kApplyThreads / B;
-    const size_t smem = (size_t)BPC * bs * 9 * sizeof(S);
+    const size_t smem0 = (size_t)kL0Banks * bs * 9 * sizeof(S);
+    const int chunk = std::max(1, std::min(coarse_bpc<B>(), (int)(kCoarseSmem / (bs * 9 * sizeof(S)))));
+    const size_t smem1 = (size_t)chunk * bs * 9 * sizeof(S);
     auto k0 = k_apply_l0<B, S, Acc>;
     auto k1 = k_apply_coarse<B, S, Acc>;
-    SG_CUDA(c, cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    SG_CUDA(c, cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SG_CUDA(c, cudaFuncSetAttribute(k0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
+    SG_CUDA(c, cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
     const int nbank0 = c->Mm / B;
     const int parts = c->apply_parts;
     if (parts & 1)
-    k0<<<(nbank0 + BPC - 1) / BPC, kApplyThreads, smem, s>>>(c->Mm, c->L, c->d_part_map, c->d_fine_mask,
-                                                             c->d_going_next, (const S*)c->d_inv, (double*)r,
-                                                             (Acc*)c->d_R, (Acc*)c->d_Z, mode, x, p, Ap, st, c->d_err);
-    const int coarse_cap = c->cap_total / B - round_up(c->Mm, B) / B;
+        k0<<<(nbank0 + kL0Banks - 1) / kL0Banks, kL0Banks * B, smem0, s>>>(
+            c->Mm, c->L, c->d_part_map, c->d_fine_mask, c->d_going_next, (const S*)c->d_inv, (double*)r,
+            (Acc*)c->d_R, (Acc*)c->d_Z, mode, x, p, Ap, st, c->d_err);
+    // level-1 banks are bounded by the vertex count (extra CTAs return at once)
+    const int l1_cap = (c->N + B - 1) / B + 1;
     if (parts & 2)
-    k1<<<max(1, (coarse_cap + BPC - 1) / BPC), kApplyThreads, smem, s>>>(c->Mm, c->L, c->d_level_size,
-                                                                         (const S*)c->d_inv, (const Acc*)c->d_R,
-                                                                         (Acc*)c->d_Z, st, c->d_err);
-    const int gN = (c->N + kThreads - 1) / kThreads;
+        k1<<<(l1_cap + coarse_bpc<B>() - 1) / coarse_bpc<B>(), kCoarseThreads, smem1, s>>>(
+            c->L, c->d_level_size, c->d_going_next, (const S*)c->d_inv, (Acc*)c->d_R, (Acc*)c->d_Z, st,
+            c->d_coarse_ticket, c->d_err);
+    const int gN = (c->N + kCollectThreads - 1) / kCollectThreads;
     if (parts & 4)
-    k_collect<Acc><<<gN, kThreads, 0, s>>>(c->N, c->L, c->Mm, c->d_level_size, c->d_real_map, c->d_coarse_table,
+    k_collect<Acc><<<gN, kCollectThreads, 0, s>>>(c->N, c->L, c->Mm, c->d_level_size, c->d_real_map, c->d_coarse_table,
                                           (const Acc*)c->d_Z, (Acc*)c->d_R, r, z, kind, (PcgState*)st, partials,
                                           ticket, cond != 0ull, cond);
     SG_CUDA(c, cudaGetLastError());

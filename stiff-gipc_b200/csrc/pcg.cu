@@ -69,7 +69,7 @@ __global__ void k_row_scan(int n, const int* __restrict__ cnt, int* row_ptr) {
 __global__ void k_bsr_fill(int nb, int nrows, const int* __restrict__ rows, const int* __restrict__ cols,
                            const int* __restrict__ row_ptr, const int* __restrict__ cnt,
                            const int* __restrict__ cnt_lower, const int* __restrict__ first, int* fill, int* bcols,
-                           uint32_t* src, int* err) {
+                           uint32_t* src, int* tcols, uint32_t* tsrc, int* err) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nb) return;
     const int i = rows[k], j = cols[k];
@@ -79,36 +79,70 @@ __global__ void k_bsr_fill(int nb, int nrows, const int* __restrict__ rows, cons
     const int pu = row_ptr[i] + cnt_lower[i] + u;
     bcols[pu] = j;
     src[pu] = (uint32_t)k;
-    if (i != j) {
+    if (i != j) {  // lower entries land in claim order in the scratch copy; sorted next
         const int pl = row_ptr[j] + atomicAdd(fill + j, 1);
-        bcols[pl] = i;
-        src[pl] = (uint32_t)k | 0x80000000u;
+        tcols[pl] = i;
+        tsrc[pl] = (uint32_t)k | 0x80000000u;
     }
 }
 
-// sort each row's lower entries by column (their slots were claimed
-// atomically) and write the even-length padding entry
+// one warp per row: each lower entry's rank among the row's lower entries
+// (columns are distinct) places it in column order; then the even-length
+// padding entry
 __global__ void k_bsr_sort_lower(int nrows, const int* __restrict__ row_ptr, const int* __restrict__ cnt,
-                                 const int* __restrict__ cnt_lower, int* bcols, uint32_t* src) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+                                 const int* __restrict__ cnt_lower, const int* __restrict__ tcols,
+                                 const uint32_t* __restrict__ tsrc, int* bcols, uint32_t* src) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (i >= nrows) return;
     const int b = row_ptr[i], nl = cnt_lower[i];
-    for (int a = 1; a < nl; ++a) {
-        const int kc = bcols[b + a];
-        const uint32_t ks = src[b + a];
-        int q = a - 1;
-        while (q >= 0 && bcols[b + q] > kc) {
-            bcols[b + q + 1] = bcols[b + q];
-            src[b + q + 1] = src[b + q];
-            --q;
-        }
-        bcols[b + q + 1] = kc;
-        src[b + q + 1] = ks;
+    for (int e = lane; e < nl; e += 32) {
+        const int key = tcols[b + e];
+        int rank = 0;
+        for (int f = 0; f < nl; ++f) rank += tcols[b + f] < key;
+        bcols[b + rank] = key;
+        src[b + rank] = tsrc[b + e];
     }
-    if (cnt[i] & 1) {
+    if (lane == 0 && (cnt[i] & 1)) {
         bcols[b + cnt[i]] = i;
         src[b + cnt[i]] = 0xffffffffu;
     }
+}
+
+// Split rows into long (more than kLongRow entries: one warp each) and short
+// (8 lanes each), both lists in row order; one CTA.
+constexpr int kLongRow = 32;
+__global__ void k_row_split(int n, const int* __restrict__ row_ptr, int* row_list, int* n_long) {
+    __shared__ int sh[1024];
+    __shared__ int carry, total_long;
+    if (threadIdx.x == 0) { carry = 0; total_long = 0; }
+    __syncthreads();
+    // pass 1: count long rows
+    int cnt = 0;
+    for (int i = threadIdx.x; i < n; i += 1024) cnt += (row_ptr[i + 1] - row_ptr[i]) > kLongRow;
+    atomicAdd(&total_long, cnt);
+    __syncthreads();
+    const int nl = total_long;
+    for (int base = 0; base < n; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int v = i < n ? ((row_ptr[i + 1] - row_ptr[i]) > kLongRow) : 0;
+        sh[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            const int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+            __syncthreads();
+            sh[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (i < n) {
+            const int before = carry + sh[threadIdx.x] - v;  // long rows before i
+            row_list[v ? before : nl + (i - before)] = i;
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += sh[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *n_long = nl;
 }
 
 __global__ void k_bsr_values(long long cap, const int* __restrict__ row_ptr, int nrows, const uint32_t* __restrict__ src,
@@ -206,22 +240,39 @@ __global__ void k_abd_inverse(int bodies, int nb, const int* __restrict__ rows, 
 //   MODE 1: p_new = z + beta p_old (fused), Ap = A p_new, p.Ap -> alpha
 //   MODE 2: r = rhs - A x
 // ---------------------------------------------------------------------------
+// Work split: warps [0, n_long) take one long row each (all 32 lanes), the
+// remaining warps take four short rows (8 lanes each); row_list holds the
+// long rows first, both parts in row order.
 template <int MODE>
-__global__ void __launch_bounds__(kT) k_bsr_spmv(int nrows, const int* __restrict__ row_ptr, const int* __restrict__ bcols,
-                                                 const double* __restrict__ bvals, long long cap,
-                                                 const double* __restrict__ xin, const double* __restrict__ pold,
+__global__ void __launch_bounds__(kT) k_bsr_spmv(BsrView A, const double* __restrict__ xin, const double* __restrict__ pold,
                                                  double* pnew, double* y, const double* __restrict__ rhs, double a,
                                                  double b, PcgState* st, double* partials, unsigned* ticket) {
     if (MODE != 0 && st->done) return;
     __shared__ double sh[32];
     const double beta = MODE == 1 ? st->beta : 0.0;
-    const int row = (blockIdx.x * kT + threadIdx.x) >> 3;
-    const int l = threadIdx.x & 7;
+    const int* __restrict__ row_ptr = A.row_ptr;
+    const int* __restrict__ bcols = A.cols;
+    const double* __restrict__ bvals = A.vals;
+    const long long cap = A.cap;
+    const int gw = blockIdx.x * (kT / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const bool longw = gw < A.n_long;
+    int row = -1, l, G;
+    if (longw) {
+        row = A.row_list[gw];
+        l = lane;
+        G = 32;
+    } else {
+        const int g = (gw - A.n_long) * 4 + (lane >> 3);
+        if (g < A.nrows - A.n_long) row = A.row_list[A.n_long + g];
+        l = lane & 7;
+        G = 8;
+    }
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     double dot = 0.0;
-    if (row < nrows) {
-        const int beg = row_ptr[row], end = row_ptr[row + 1];
-        for (int p = beg + 2 * l; p < end; p += 16) {
+    {
+        const int beg = row >= 0 ? row_ptr[row] : 0, end = row >= 0 ? row_ptr[row + 1] : 0;
+        for (int p = beg + 2 * l; p < end; p += 2 * G) {
             const int2 cc = *reinterpret_cast<const int2*>(bcols + p);
             double2 v[9];
             #pragma unroll
@@ -241,13 +292,22 @@ __global__ void __launch_bounds__(kT) k_bsr_spmv(int nrows, const int* __restric
             a1 += v[3].x * x0[0] + v[4].x * x0[1] + v[5].x * x0[2] + v[3].y * x1[0] + v[4].y * x1[1] + v[5].y * x1[2];
             a2 += v[6].x * x0[0] + v[7].x * x0[1] + v[8].x * x0[2] + v[6].y * x1[0] + v[7].y * x1[1] + v[8].y * x1[2];
         }
-        #pragma unroll
-        for (int o = 4; o > 0; o >>= 1) {
-            a0 += __shfl_xor_sync(0xffffffffu, a0, o, 8);
-            a1 += __shfl_xor_sync(0xffffffffu, a1, o, 8);
-            a2 += __shfl_xor_sync(0xffffffffu, a2, o, 8);
+        if (longw) {  // warp-uniform branch
+            #pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+            }
+        } else {
+            #pragma unroll
+            for (int o = 4; o > 0; o >>= 1) {
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o, 8);
+                a1 += __shfl_xor_sync(0xffffffffu, a1, o, 8);
+                a2 += __shfl_xor_sync(0xffffffffu, a2, o, 8);
+            }
         }
-        if (l == 0) {
+        if (l == 0 && row >= 0) {
             double* yr = y + 3 * (size_t)row;
             if (MODE == 0) {
                 if (b != 0.0) { yr[0] = a * a0 + b * yr[0]; yr[1] = a * a1 + b * yr[1]; yr[2] = a * a2 + b * yr[2]; }
@@ -417,14 +477,16 @@ int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* 
     cudaStream_t s = c->stream;
     if (nrows > B.rows_cap) {
         if (ctx_alloc(c, &B.row_ptr, (size_t)nrows + 1) || ctx_alloc(c, &B.cnt, nrows) ||
-            ctx_alloc(c, &B.cnt_lower, nrows) || ctx_alloc(c, &B.fill, nrows) || ctx_alloc(c, &B.first, nrows))
+            ctx_alloc(c, &B.cnt_lower, nrows) || ctx_alloc(c, &B.fill, nrows) || ctx_alloc(c, &B.first, nrows) ||
+            ctx_alloc(c, &B.row_list, nrows) || ctx_alloc(c, &B.d_nlong, 1))
             return SGMAS_ERR_CUDA;
         B.rows_cap = nrows;
     }
     const long long need = 2LL * nb + nrows + 2;  // both triangles + one padding entry per row at most
     if (need > B.cap) {
         const long long cap = (need + 1) & ~1LL;
-        if (ctx_alloc(c, &B.cols, cap) || ctx_alloc(c, &B.src, cap) || ctx_alloc(c, &B.vals, 9 * cap))
+        if (ctx_alloc(c, &B.cols, cap) || ctx_alloc(c, &B.src, cap) || ctx_alloc(c, &B.vals, 9 * cap) ||
+            ctx_alloc(c, &B.tcols, cap) || ctx_alloc(c, &B.tsrc, cap))
             return SGMAS_ERR_CUDA;
         B.cap = cap;
     }
@@ -434,23 +496,35 @@ int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* 
     SG_CUDA(c, cudaMemsetAsync(B.cnt_lower, 0, sizeof(int) * nrows, s));
     SG_CUDA(c, cudaMemsetAsync(B.fill, 0, sizeof(int) * nrows, s));
     SG_CUDA(c, cudaMemsetAsync(B.first, 0, sizeof(int) * nrows, s));
-    const int gb = (nb + kT - 1) / kT, gr = (nrows + kT - 1) / kT;
+    const int gb = (nb + kT - 1) / kT;
     if (nb > 0) k_bsr_count<<<gb, kT, 0, s>>>(nb, nrows, rows, cols, B.cnt, B.cnt_lower, B.first, c->d_err);
     k_row_scan<<<1, 1024, 0, s>>>(nrows, B.cnt, B.row_ptr);
     if (nb > 0)
         k_bsr_fill<<<gb, kT, 0, s>>>(nb, nrows, rows, cols, B.row_ptr, B.cnt, B.cnt_lower, B.first, B.fill, B.cols,
-                                     B.src, c->d_err);
-    k_bsr_sort_lower<<<gr, kT, 0, s>>>(nrows, B.row_ptr, B.cnt, B.cnt_lower, B.cols, B.src);
+                                     B.src, B.tcols, B.tsrc, c->d_err);
+    k_bsr_sort_lower<<<(nrows * 32 + kT - 1) / kT, kT, 0, s>>>(nrows, B.row_ptr, B.cnt, B.cnt_lower, B.tcols, B.tsrc,
+                                                             B.cols, B.src);
     k_bsr_values<<<(int)((B.cap + kT - 1) / kT), kT, 0, s>>>(B.cap, B.row_ptr, nrows, B.src, vals, B.vals);
+    k_row_split<<<1, 1024, 0, s>>>(nrows, B.row_ptr, B.row_list, B.d_nlong);
     SG_CUDA(c, cudaGetLastError());
+    // the long-row count sizes the SpMV grid (one 4-byte read per build)
+    SG_CUDA(c, cudaMemcpyAsync(&B.n_long, B.d_nlong, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SG_CUDA(c, cudaStreamSynchronize(s));
     return 0;
+}
+
+static BsrView bsr_view(const BsrMatrix& B) {
+    return BsrView{B.row_ptr, B.cols, B.vals, B.cap, B.row_list, B.nrows, B.n_long};
+}
+static int spmv_grid(const BsrMatrix& B) {
+    const int warps = B.n_long + (B.nrows - B.n_long + 3) / 4;
+    return (warps + kT / 32 - 1) / (kT / 32);
 }
 
 int bsr_spmv_plain(sgmas_context* c, double a, const double* x, double b, double* y) {
     const BsrMatrix& B = c->bsr;
-    const int grid = (B.nrows * 8 + kT - 1) / kT;
-    k_bsr_spmv<0><<<grid, kT, 0, c->stream>>>(B.nrows, B.row_ptr, B.cols, B.vals, B.cap, x, nullptr, nullptr, y,
-                                              nullptr, a, b, nullptr, nullptr, nullptr);
+    k_bsr_spmv<0><<<spmv_grid(B), kT, 0, c->stream>>>(bsr_view(B), x, nullptr, nullptr, y, nullptr, a, b, nullptr,
+                                                      nullptr, nullptr);
     SG_CUDA(c, cudaGetLastError());
     return 0;
 }
@@ -513,7 +587,7 @@ static int record_body(sgmas_context* c, cudaStream_t s, const double* b, double
                        unsigned long long cond, int* nk) {
     const int nrows = c->bsr.nrows, n = 3 * nrows;
     const BsrMatrix& B = c->bsr;
-    const int gs = (nrows * 8 + kT - 1) / kT;
+    const int gs = spmv_grid(B);
     const int gj = (nrows + kT - 1) / kT;
     cudaStream_t saved = c->stream;
     c->stream = s;
@@ -524,13 +598,13 @@ static int record_body(sgmas_context* c, cudaStream_t s, const double* b, double
         double* pnew = (t % 2 == 0) ? c->d_p1 : c->d_p0;
         const bool check = (t == 9);
         const unsigned long long cnd = check ? cond : 0ull;
-        k_bsr_spmv<1><<<gs, kT, 0, s>>>(nrows, B.row_ptr, B.cols, B.vals, B.cap, c->d_z, pold, pnew, c->d_Ap,
-                                        nullptr, 1.0, 0.0, c->d_state, c->d_partials, c->d_ticket);
+        k_bsr_spmv<1><<<gs, kT, 0, s>>>(bsr_view(B), c->d_z, pold, pnew, c->d_Ap, nullptr, 1.0, 0.0, c->d_state,
+                                        c->d_partials, c->d_ticket);
         *nk += 1;
         if (check) {
             k_update_x<<<(n + kT - 1) / kT, kT, 0, s>>>(n, x, pnew, c->d_state);
-            k_bsr_spmv<2><<<gs, kT, 0, s>>>(nrows, B.row_ptr, B.cols, B.vals, B.cap, x, nullptr, nullptr, c->d_r, b,
-                                            1.0, 0.0, c->d_state, nullptr, nullptr);
+            k_bsr_spmv<2><<<gs, kT, 0, s>>>(bsr_view(B), x, nullptr, nullptr, c->d_r, b, 1.0, 0.0, c->d_state, nullptr,
+                                            nullptr);
             *nk += 2;
         }
         if (cfg.precond == 1) {
@@ -557,7 +631,7 @@ static int record_body(sgmas_context* c, cudaStream_t s, const double* b, double
 int pcg_run(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, float* solve_ms, int* launches) {
     const int nrows = c->bsr.nrows;
     if (ensure_vec(c, nrows)) return SGMAS_ERR_CUDA;
-    const int gmax = (nrows * 8 + kT - 1) / kT + 8;
+    const int gmax = nrows / 8 + 16;  // >= every grid of the loop (SpMV: at most one warp per row)
     if (ensure_partials(c, gmax)) return SGMAS_ERR_CUDA;
     if (!c->d_state) {
         if (ctx_alloc(c, &c->d_state, 1) || ctx_alloc(c, &c->d_ticket, 1)) return SGMAS_ERR_CUDA;
@@ -567,7 +641,8 @@ int pcg_run(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, 
     // graph cache key: everything the recorded launches capture
     unsigned long long key[8] = {(unsigned long long)(uintptr_t)b,
                                  (unsigned long long)(uintptr_t)x,
-                                 (unsigned long long)nrows | ((unsigned long long)c->bsr.cap << 24),
+                                 (unsigned long long)nrows | ((unsigned long long)c->bsr.cap << 24) ^
+                                     ((unsigned long long)c->bsr.n_long << 44),
                                  (unsigned long long)cfg.precond | ((unsigned long long)cfg.abd_bodies << 8) |
                                      ((unsigned long long)c->precision << 40),
                                  (unsigned long long)(uintptr_t)c->bsr.vals,
@@ -672,15 +747,15 @@ int pcg_profile(sgmas_context* c, int reps, float* ms, int n_ms) {
     if (!(h.rz == h.rz) || h.rz == 0.0) h.rz = 1.0;
     SG_CUDA(c, cudaMemcpyAsync(c->d_state, &h, sizeof(PcgState), cudaMemcpyHostToDevice, s));
     for (int i = 0; i < n_ms; ++i) ms[i] = 0.f;
-    const int gs = (nrows * 8 + kT - 1) / kT, gj = (nrows + kT - 1) / kT;
+    const int gs = spmv_grid(B), gj = (nrows + kT - 1) / kT;
     int rc = 0;
     for (int part = 0; part < 4 && part < n_ms && rc == 0; ++part) {
         if (c->last_cfg.precond == 0 && part >= 2) break;
         SG_CUDA(c, cudaEventRecord(c->ev0, s));
         for (int r = 0; r < reps && rc == 0; ++r) {
             if (part == 0) {
-                k_bsr_spmv<1><<<gs, kT, 0, s>>>(nrows, B.row_ptr, B.cols, B.vals, B.cap, c->d_z, c->d_p0, c->d_p1,
-                                                c->d_Ap, nullptr, 1.0, 0.0, c->d_state, c->d_partials, c->d_ticket);
+                k_bsr_spmv<1><<<gs, kT, 0, s>>>(bsr_view(B), c->d_z, c->d_p0, c->d_p1, c->d_Ap, nullptr, 1.0, 0.0,
+                                                c->d_state, c->d_partials, c->d_ticket);
             } else if (c->last_cfg.precond == 0) {
                 k_jacobi_iter<1><<<gj, kT, 0, s>>>(nrows, 4 * c->last_cfg.abd_bodies, c->last_x, c->d_r, c->d_p1,
                                                    c->d_Ap, c->d_z, c->d_diag_inv, c->d_abd_inv, 3, c->d_state,
