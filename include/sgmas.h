@@ -171,6 +171,21 @@ int sgmas_write_upper_blocks(sgmas_context* ctx, const double* d_H, int n_elem, 
  * vertices' own bounding box */
 int sgmas_morton_codes(sgmas_context* ctx, const double* d_pos, int n, const double* aabb,
                        uint64_t* d_codes);
+/* Morton codes exactly as sgmas_morton_codes, for callers that cannot
+ * allocate device memory: code running during CUDA graph capture, or hosts
+ * whose device memory comes from their own pool.  No reference counterpart:
+ * this entry point exists only in this library.  It needs no context and
+ * calls no allocating routine; the bounding-box reduction uses a fixed
+ * 49,216-byte static device array that every GPU loading the library holds
+ * until exit.  n must not exceed SGMAS_MORTON_NOALLOC_MAX_VERTS
+ * (SGMAS_ERR_CAPACITY otherwise, before any work is queued).  Runs on the
+ * current device and `stream` (NULL = legacy default stream).  The first
+ * call on a device looks the array up (cudaGetSymbolAddress): make that first
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race, so order them (same stream or synchronised). */
+#define SGMAS_MORTON_NOALLOC_MAX_VERTS 2097152
+int sgmas_morton_codes_noalloc(const double* d_pos, int n, const double* aabb, uint64_t* d_codes,
+                               void* stream);
 /* Morton order cut into bank-size subdomains: slot maps in the layout of
  * setMAS_partition (part_map[part_map_size], real_map[n]; host arrays) */
 int sgmas_morton_partition(sgmas_context* ctx, const double* d_pos, int n, int* part_map,

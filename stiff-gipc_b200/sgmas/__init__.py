@@ -54,8 +54,10 @@ EXPORTS = [
     "sgmas_mas_download_tables", "sgmas_mas_download_matrices", "sgmas_mas_invert_host",
     "sgmas_pcg_solve", "sgmas_pcg_solve_host", "sgmas_spmv", "sgmas_convert", "sgmas_write_upper_blocks",
     "sgmas_morton_codes", "sgmas_morton_partition", "sgmas_pcg_profile", "sgmas_vert_neighbors",
-    "sgmas_part_maps",
+    "sgmas_part_maps", "sgmas_morton_codes_noalloc",
 ]
+
+MORTON_NOALLOC_MAX_VERTS = 2097152  # SGMAS_MORTON_NOALLOC_MAX_VERTS in include/sgmas.h
 
 
 def lib(build_if_missing: bool = False):
@@ -94,8 +96,20 @@ def lib(build_if_missing: bool = False):
     L.sgmas_pcg_profile.argtypes = [vp, i, vp, i]
     L.sgmas_vert_neighbors.argtypes = [vp, i, vp, i, i, i, vp, vp, vp, i]
     L.sgmas_part_maps.argtypes = [vp, i, i, vp, i, C.POINTER(i), vp]
+    L.sgmas_morton_codes_noalloc.argtypes = [vp, i, vp, vp, vp]
     _lib = L
     return L
+
+
+def morton_codes_noalloc(pos, codes, aabb=None, stream=None, n=None):
+    """Morton codes without any device allocation (sgmas_morton_codes_noalloc).
+
+    For callers that may not allocate device memory (e.g. during CUDA graph
+    capture).  Runs on the current device; returns the C status code (0 = ok,
+    SGMAS_ERR_CAPACITY = -4 when n exceeds MORTON_NOALLOC_MAX_VERTS)."""
+    box = None if aabb is None else _h(aabb, np.float64)
+    count = int(pos.shape[0]) if n is None else n
+    return lib().sgmas_morton_codes_noalloc(_ptr(pos), count, _ptr(box), _ptr(codes), stream)
 
 
 def vert_neighbors(tets, n_verts, tris=None, abd_vert_offset=0):
