@@ -49,7 +49,9 @@ def parse():
     ap.add_argument("--impl", default="sgmas", choices=["sgmas", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = benchmark size)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--variants", default="bf16,fp32,fp64,jacobi")
+    ap.add_argument("--variants", default="bf16,fp32,fp64,jacobi,fp32-graph",
+                    help="MAS storage precision (or jacobi); suffix -graph = kernel-per-phase CUDA graph "
+                         "instead of the persistent cooperative kernel")
     ap.add_argument("--profile-reps", type=int, default=50,
                     help="replays per kernel for the per-kernel times (1 = one launch each, for ncu)")
     return ap.parse_args()
@@ -196,9 +198,11 @@ def run_sgmas(args):
     clocks = Clocks(local)
     gpu_launches = None
     for v in variants:
-        precision = v if v in ("fp32", "bf16", "fp64") else "fp32"
-        precond = "jacobi" if v == "jacobi" else "mas"
+        base, mode = (v[:-6], "graph") if v.endswith("-graph") else (v, "persistent")
+        precision = base if base in ("fp32", "bf16", "fp64") else "fp32"
+        precond = "jacobi" if base == "jacobi" else "mas"
         ctx, pms = make(precision)
+        ctx.set_pcg_mode(mode)
         ctxs[v] = (ctx, pms)
         x = torch.zeros_like(b)
         try:
@@ -240,7 +244,7 @@ def run_sgmas(args):
             ms = float(t.item())
         results[v] = {"ms": ms, "ms_min": min(times), "ms_max": max(times), "iterations": int(statistics.median(iters)),
                       "rel_residual": res, "converged": bool(rep["converged"]),
-                      "precond_build_ms": rep["precond_ms"], "pcg_graph_ms": rep["solve_ms"],
+                      "precond_build_ms": rep["precond_ms"], "pcg_loop_ms": rep["solve_ms"], "mode": mode,
                       "kernel_launches": int(statistics.median(launches))}
         if first:
             gpu_launches = int(sum(launches))
@@ -249,40 +253,63 @@ def run_sgmas(args):
     head = ok[0] if ok else next(v for v in variants if "ms" in results.get(v, {}))
     # ---- per-kernel times and roofline of the headline variant ----
     ctx, pms = ctxs[head]
-    precision = head if head in ("fp32", "bf16", "fp64") else "fp32"
+    hbase = head[:-6] if head.endswith("-graph") else head
+    precision = hbase if hbase in ("fp32", "bf16", "fp64") else "fp32"
     print(json.dumps({"progress": results}), file=sys.stderr, flush=True)
     # ---- e2e through the public API with host buffers ----
     try:
-        e2e = run_e2e(args, ctx, s, dev, stream, head)
+        e2e = run_e2e(args, ctx, s, dev, stream, hbase)
     except Exception as e:  # reported, not hidden
         e2e = {"error": str(e)}
     x = torch.zeros_like(b)
     ctx.pcg_solve(vals, rows, cols, s.n_verts, b, x, rel_tol=REL_TOL, max_iter=MAX_ITER,
-                  preconditioner="mas" if head != "jacobi" else "jacobi")
+                  preconditioner="mas" if hbase != "jacobi" else "jacobi")
     kms = ctx.pcg_profile(reps=args.profile_reps)
+    gkms = None  # per-kernel times of the graph form, for comparison
+    gvar = next((v for v in variants if v.endswith("-graph") and "ms" in results.get(v, {})), None)
+    if gvar and gvar != head:
+        gctx = ctxs[gvar][0]
+        gctx.pcg_solve(vals, rows, cols, s.n_verts, b, x, rel_tol=REL_TOL, max_iter=MAX_ITER,
+                       preconditioner="mas" if not gvar.startswith("jacobi") else "jacobi")
+        gkms = gctx.pcg_profile(reps=args.profile_reps)
     info = ctx.mas_info()
     info["part_map_size"] = pms
     abytes = algorithmic_bytes(s, info, precision)
-    dom = max(kms, key=lambda k: kms[k])
     hbm, peak_kind = peaks()
-    achieved = abytes[dom] / (kms[dom] * 1e-3) / 1e9
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            traffic = json.load(f).get(f"{dom}_{precision}")
+            tj = json.load(f)
     except Exception:
-        pass
+        tj = {}
+    if results[head]["mode"] == "persistent":
+        # the whole loop is one launch: bytes of all its iterations over the loop time
+        its = results[head]["iterations"]
+        per_it = sum(abytes[k] for k in ("spmv", "update_l0", "coarse", "collect"))
+        n3 = 3 * s.n_verts
+        refresh = abytes["spmv"] + 8 * 3 * n3 + 8 * n3  # every 10th: x += alpha p, r = b - A x
+        dom = "k_pcg_persistent"
+        dom_bytes = its * per_it + (its // 10) * refresh
+        dom_ms = results[head]["pcg_loop_ms"]
+        traffic = tj.get(f"persistent_{precision}_per_iteration")
+        traffic = None if traffic is None else traffic * its
+    else:
+        dom = max(kms, key=lambda k: kms[k])
+        dom_bytes, dom_ms = abytes[dom], kms[dom]
+        traffic = tj.get(f"{dom}_{precision}")
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": f"{peak_kind} HBM copy",
-                "algorithmic_bytes": abytes[dom], "kernel_ms": kms[dom], "kernel_ms_all": kms,
+                "algorithmic_bytes": int(dom_bytes), "kernel_ms": dom_ms, "phase_ms": kms,
+                "phase_bytes": abytes, "graph_kernel_ms": gkms,
                 "note": "per-iteration working set < 126 MB L2: achieved can exceed the HBM copy peak"}
     out = {"metric": METRIC, "value": round(results[head]["ms"], 4), "unit": "ms", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(results[head]["ms"], 4),
            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-           "dtype": {"bf16": "f64+bf16", "fp32": "f64+f32", "fp64": "f64", "jacobi": "f64"}[head],
+           "dtype": {"bf16": "f64+bf16", "fp32": "f64+f32", "fp64": "f64", "jacobi": "f64"}[hbase],
            "data": "synthetic",
            "config": {"workload": WORKLOAD, "scale": args.scale, "rel_tol": REL_TOL,
-                      "headline": f"{head} MAS-PCG", "partition": "Morton order, 16-vertex subdomains",
+                      "headline": f"{head} MAS-PCG ({results[head]['mode']})", "partition": "Morton order, 16-vertex subdomains",
                       "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{world}",
                       "n_blocks": int(len(s.rows)), "n_pairs": int(len(s.pairs)), "gen_s": round(gen_s, 1)},
            "variants": results,

@@ -128,15 +128,37 @@ int sgmas_mas_invert_host(sgmas_context* ctx, const double* hess64, int nblocks,
  * assembles the MAS itself) when cfg->preconditioner == 1. */
 int sgmas_pcg_solve(sgmas_context* ctx, const sgmas_bcoo* A, const double* d_b, double* d_x,
                     const sgmas_pcg_config* cfg, sgmas_pcg_report* report);
+/* How sgmas_pcg_solve runs the loop: SGMAS_PCG_PERSISTENT (default) = one
+ * cooperative kernel, one CTA per SM, grid barriers between phases (falls
+ * back to the graph form when the system's subdomain tiles do not fit in
+ * shared memory); SGMAS_PCG_GRAPH = one kernel per phase in a CUDA graph with
+ * a conditional WHILE node. */
+/* Copy the residual r and the preconditioned residual z = M^-1 r of the last
+ * iteration of the last sgmas_pcg_solve (PCGSolver's members r and z,
+ * SG/linear_system/solver/pcg_solver.h:29-30) into d_r / d_z (3 * n_block_rows
+ * doubles each; either may be NULL).  After a solve stopped by max_iter = 1, z
+ * is M^-1 b.  sgmas_pcg_profile overwrites both. */
+int sgmas_pcg_last_vectors(sgmas_context* ctx, double* d_r, double* d_z);
+#define SGMAS_PCG_GRAPH 0
+#define SGMAS_PCG_PERSISTENT 1
+int sgmas_set_pcg_mode(sgmas_context* ctx, int mode);
 /* the same with host arrays: uploads A and b, solves, downloads x */
 int sgmas_pcg_solve_host(sgmas_context* ctx, const double* values, const int* rows,
                          const int* cols, int n_blocks, int n_block_rows, const double* b,
                          double* x, const sgmas_pcg_config* cfg, sgmas_pcg_report* report);
 
-/* Device time of each kernel of one PCG iteration, replayed `reps` times on
- * the buffers of the last sgmas_pcg_solve (which it overwrites): ms[0] SpMV
- * with the fused p update and p.Ap, ms[1] update + level-0 MAS (or the
- * block-Jacobi tail), ms[2] coarse Schwarz, ms[3] CollectFinalZ + r.z. */
+/* Device time of each phase of one PCG iteration on the buffers of the last
+ * sgmas_pcg_solve (which it overwrites): ms[0] SpMV with the fused p update
+ * and p.Ap, ms[1] update + level-0 MAS (or the block-Jacobi tail), ms[2]
+ * coarse Schwarz, ms[3] CollectFinalZ + r.z.  After a graph-form solve each
+ * kernel is replayed `reps` times between events.  After a persistent solve
+ * the solve is run once more with clock stamps at every grid barrier: ms[0]
+ * SpMV phase, ms[1] update + levels 0-1 (+ collect when the hierarchy has at
+ * most two levels), ms[2] levels >= 2 + collect, ms[3] 0, ms[4] that solve's
+ * loop time, ms[5] iterations averaged, and for each barrier slot (0 SpMV,
+ * 1 x refresh, 2 r refresh, 3 levels 0-1, 4 unused, 5 end of iteration)
+ * ms[6 + 3 * slot + 0..2] = the CTAs' mean and maximum work before it and
+ * their mean wait in it, per occurrence (`reps` unused). */
 int sgmas_pcg_profile(sgmas_context* ctx, int reps, float* ms, int n_ms);
 
 /* ---- MAS set-up data on the host (no GPU needed) ----------------------- */

@@ -78,7 +78,8 @@ void free_all(sgmas_context* c) {
                     c->bsr.src, c->bsr.vals, c->bsr.cnt, c->bsr.cnt_lower, c->bsr.fill, c->bsr.first, c->d_r,
                     c->d_z, c->d_p0, c->d_p1, c->d_Ap, c->d_diag_inv, c->d_abd_inv, c->d_partials, c->d_ticket,
                     c->d_state, c->d_hvals, c->d_hb, c->d_hx, c->d_hrows, c->d_hcols, c->d_sort_scratch,
-                    c->d_coarse_ticket, c->bsr.row_list, c->bsr.d_nlong, c->bsr.tcols, c->bsr.tsrc};
+                    c->d_coarse_ticket, c->bsr.row_list, c->bsr.d_nlong, c->bsr.tcols, c->bsr.tsrc,
+                    c->d_psync, c->d_stamps, c->d_l1_bank};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -359,7 +360,8 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
     int launches = 0;
     SG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     float prep_ms = 0.f;
-    rc = pcg_run(c, d_b, d_x, rc_cfg, &solve_ms, &launches);
+    rc = c->persistent ? pcg_run_persistent(c, d_b, d_x, rc_cfg, &solve_ms, &launches) : 1;
+    if (rc == 1) rc = pcg_run(c, d_b, d_x, rc_cfg, &solve_ms, &launches);  // graph path
     if (rc) return rc;
     cudaEventElapsedTime(&prep_ms, c->ev2, c->ev0);
     rc = check_device_error(c, "sgmas_pcg_solve");
@@ -465,6 +467,22 @@ int sgmas_morton_partition(sgmas_context* c, const double* d_pos, int n, int* pa
     for (int s = 0; s < size; ++s) part_map[s] = s < n ? (int)order[s] : -1;
     for (int s = 0; s < n; ++s) real_map[order[s]] = s;
     *part_map_size = size;
+    return SGMAS_OK;
+}
+
+int sgmas_pcg_last_vectors(sgmas_context* c, double* d_r, double* d_z) {
+    if (!c) return SGMAS_ERR_ARG;
+    if (!c->last_cfg.valid) return ctx_fail(c, SGMAS_ERR_STATE, "sgmas_pcg_last_vectors needs a completed solve");
+    SG_CUDA(c, cudaSetDevice(c->device));
+    const size_t bytes = sizeof(double) * 3 * (size_t)c->bsr.nrows;
+    if (d_r) SG_CUDA(c, cudaMemcpyAsync(d_r, c->d_r, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    if (d_z) SG_CUDA(c, cudaMemcpyAsync(d_z, c->d_z, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    return SGMAS_OK;
+}
+
+int sgmas_set_pcg_mode(sgmas_context* c, int mode) {
+    if (!c || (mode != SGMAS_PCG_GRAPH && mode != SGMAS_PCG_PERSISTENT)) return SGMAS_ERR_ARG;
+    c->persistent = mode == SGMAS_PCG_PERSISTENT;
     return SGMAS_OK;
 }
 

@@ -19,6 +19,16 @@ struct PcgRunCfgLite {
     int precond, abd_bodies, valid;
 };
 
+struct PcgRunCfg {
+    int max_iter;
+    double rel_tol, abs_tol;
+    int use_prec_norm;
+    int precond;       // 0 Jacobi, 1 MAS
+    int abd_bodies;
+    int fem_offset;
+    int check_every;
+};
+
 struct BsrMatrix {
     int nrows = 0, nblocks = 0;       // upper blocks in
     long long nnz_pad = 0, cap = 0;   // full (both triangles), rows padded to even length
@@ -92,6 +102,14 @@ struct sgmas_context {
     double* d_partials = nullptr;     // reduction partials
     unsigned* d_ticket = nullptr;
     unsigned* d_coarse_ticket = nullptr;  // last-CTA ticket of the coarse MAS kernel
+    unsigned* d_psync = nullptr;          // grid barrier + ticket of the persistent PCG kernel
+    bool persistent = true;               // solve with the persistent kernel when the system fits
+    bool last_persistent = false;         // the last solve ran the persistent kernel
+    PcgRunCfg last_run = {};
+    unsigned long long* d_stamps = nullptr;  // phase clock stamps of a profiled persistent solve
+    size_t stamps_cap = 0;
+    int* d_l1_bank = nullptr;             // level-0 bank of each level-1 node (persistent ownership)
+    int l1_bank_cap = 0;
     int partial_cap = 0;
     PcgState* d_state = nullptr;
     // uploaded host systems (sgmas_pcg_solve_host)
@@ -101,7 +119,7 @@ struct sgmas_context {
     // graph cache
     cudaGraphExec_t graph_exec = nullptr;
     cudaGraph_t graph = nullptr;
-    unsigned long long graph_key[8] = {0};
+    unsigned long long graph_key[10] = {0};
     int graph_kernels_prologue = 0, graph_kernels_body = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     PcgRunCfgLite last_cfg = {0, 0, 0};
@@ -133,15 +151,14 @@ int ctx_alloc(sgmas_context* c, T** p, size_t count) {
     return 0;
 }
 
-struct PcgRunCfg {
-    int max_iter;
-    double rel_tol, abs_tol;
-    int use_prec_norm;
-    int precond;       // 0 Jacobi, 1 MAS
-    int abd_bodies;
-    int fem_offset;
-    int check_every;
-};
+// (re)allocate only when `count` exceeds the capacity `*cap`
+template <typename T>
+int ctx_alloc_grow(sgmas_context* c, T** p, int* cap, int count) {
+    if (*p && count <= *cap) return 0;
+    if (ctx_alloc(c, p, (size_t)count)) return -2;
+    *cap = count;
+    return 0;
+}
 
 // internal entry points across translation units
 int mas_build_hierarchy(sgmas_context* c);   // ReorderRealtime on the device
@@ -165,4 +182,6 @@ int morton_codes(sgmas_context* c, const double* pos, int n, const double* aabb,
 int sort_u64_pairs(sgmas_context* c, uint64_t* keys, uint32_t* vals, int n, int key_bits);
 int mas_invert_blocks_dev(sgmas_context* c, const double* hess, int nblk, double* out64);
 int pcg_profile(sgmas_context* c, int reps, float* ms, int n_ms);
+int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, float* solve_ms,
+                       int* launches, unsigned long long* stamps = nullptr, int stamp_iters = 0);
 

@@ -17,6 +17,7 @@
 #include "../../include/sgmas.h"
 #include "ctx.hpp"
 #include "pcg_state.cuh"
+#include "mas_dev.cuh"
 
 using namespace sgmas;
 
@@ -25,9 +26,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kCollectThreads = 128;
 
-__host__ __device__ constexpr int bsym_of(int B) { return B * (B + 1) / 2; }
-__host__ __device__ __forceinline__ int sym_index(int B, int r, int c) { return B * r - r * (r + 1) / 2 + c; }
-__host__ __device__ __forceinline__ int round_up(int v, int b) { return (v + b - 1) / b * b; }
 
 template <int B>
 __device__ __forceinline__ unsigned seg_ballot(bool pred) {
@@ -530,33 +528,7 @@ __global__ void __launch_bounds__(32 * inv_warps<B>()) k_invert(int nblk, const 
 // ---------------------------------------------------------------------------
 // Apply (preconditioning, :2210-2251)
 // ---------------------------------------------------------------------------
-template <typename Acc>
-__device__ __forceinline__ Acc shfl_acc(Acc v, int src, int width) { return __shfl_sync(0xffffffffu, v, src, width); }
 
-// z_lane = sum_c P(lane, c) r_c over one bank; columns ascending, each 3x3
-// row an fma chain (the order the oracle restates).
-template <int B, typename S, typename Acc>
-__device__ __forceinline__ void schwarz_rows(const S* tile, int lane, Acc r0, Acc r1, Acc r2, Acc& z0, Acc& z1,
-                                             Acc& z2) {
-    Acc a0 = 0, a1 = 0, a2 = 0;
-    #pragma unroll 4
-    for (int c = 0; c < B; ++c) {
-        const Acc x0 = shfl_acc(r0, c, B), x1 = shfl_acc(r1, c, B), x2 = shfl_acc(r2, c, B);
-        const bool tr = c < lane;
-        const S* P = tile + (tr ? sym_index(B, c, lane) : sym_index(B, lane, c)) * 9;
-        const int s1 = tr ? 1 : 3, s2 = tr ? 3 : 1;  // element (a, k) at a*s2 + k*s1
-        a0 = fma_acc(Store<S>::to_acc(P[0]), x0, a0);
-        a0 = fma_acc(Store<S>::to_acc(P[s1]), x1, a0);
-        a0 = fma_acc(Store<S>::to_acc(P[2 * s1]), x2, a0);
-        a1 = fma_acc(Store<S>::to_acc(P[s2]), x0, a1);
-        a1 = fma_acc(Store<S>::to_acc(P[s2 + s1]), x1, a1);
-        a1 = fma_acc(Store<S>::to_acc(P[s2 + 2 * s1]), x2, a1);
-        a2 = fma_acc(Store<S>::to_acc(P[2 * s2]), x0, a2);
-        a2 = fma_acc(Store<S>::to_acc(P[2 * s2 + s1]), x1, a2);
-        a2 = fma_acc(Store<S>::to_acc(P[2 * s2 + 2 * s1]), x2, a2);
-    }
-    z0 = a0; z1 = a1; z2 = a2;
-}
 
 // Stage `nb` consecutive bank tiles into shared memory with one bulk copy.
 template <typename S>
@@ -581,23 +553,6 @@ constexpr int kCoarseSmem = 80 * 1024;
 template <int B>
 __host__ __device__ constexpr int coarse_bpc() { return kCoarseThreads / B; }
 
-// Sum `v` over the lanes of this bank that share `key` (lanes ascending, the
-// order the oracle restates); *lead = lowest lane of its group.
-template <int B, typename Acc>
-__device__ __forceinline__ void group_sum(int key, Acc v0, Acc v1, Acc v2, int lane, Acc& s0, Acc& s1, Acc& s2,
-                                          bool& lead) {
-    s0 = 0; s1 = 0; s2 = 0;
-    lead = key >= 0;
-    #pragma unroll 4
-    for (int j = 0; j < B; ++j) {
-        const int kj = __shfl_sync(0xffffffffu, key, j, B);
-        const Acc y0 = shfl_acc(v0, j, B), y1 = shfl_acc(v1, j, B), y2 = shfl_acc(v2, j, B);
-        if (key >= 0 && kj == key) {
-            s0 += y0; s1 += y1; s2 += y2;
-            if (j < lane) lead = false;
-        }
-    }
-}
 
 // Level-0 kernel (BuildMultiLevelR :727-845 + the level-0 part of
 // _schwarzLocalXSym6 :954-1024): mode 1 first applies the PCG update

@@ -14,9 +14,13 @@
 //    read of the iteration count.
 #include <stdio.h>
 
+#include <algorithm>
+#include <cmath>
+
 #include "../../include/sgmas.h"
 #include "ctx.hpp"
 #include "pcg_state.cuh"
+#include "spmv_dev.cuh"
 
 using namespace sgmas;
 
@@ -240,9 +244,6 @@ __global__ void k_abd_inverse(int bodies, int nb, const int* __restrict__ rows, 
 //   MODE 1: p_new = z + beta p_old (fused), Ap = A p_new, p.Ap -> alpha
 //   MODE 2: r = rhs - A x
 // ---------------------------------------------------------------------------
-// Work split: warps [0, n_long) take one long row each (all 32 lanes), the
-// remaining warps take four short rows (8 lanes each); row_list holds the
-// long rows first, both parts in row order.
 template <int MODE>
 __global__ void __launch_bounds__(kT) k_bsr_spmv(BsrView A, const double* __restrict__ xin, const double* __restrict__ pold,
                                                  double* pnew, double* y, const double* __restrict__ rhs, double a,
@@ -250,81 +251,8 @@ __global__ void __launch_bounds__(kT) k_bsr_spmv(BsrView A, const double* __rest
     if (MODE != 0 && st->done) return;
     __shared__ double sh[32];
     const double beta = MODE == 1 ? st->beta : 0.0;
-    const int* __restrict__ row_ptr = A.row_ptr;
-    const int* __restrict__ bcols = A.cols;
-    const double* __restrict__ bvals = A.vals;
-    const long long cap = A.cap;
     const int gw = blockIdx.x * (kT / 32) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    const bool longw = gw < A.n_long;
-    int row = -1, l, G;
-    if (longw) {
-        row = A.row_list[gw];
-        l = lane;
-        G = 32;
-    } else {
-        const int g = (gw - A.n_long) * 4 + (lane >> 3);
-        if (g < A.nrows - A.n_long) row = A.row_list[A.n_long + g];
-        l = lane & 7;
-        G = 8;
-    }
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    double dot = 0.0;
-    {
-        const int beg = row >= 0 ? row_ptr[row] : 0, end = row >= 0 ? row_ptr[row + 1] : 0;
-        for (int p = beg + 2 * l; p < end; p += 2 * G) {
-            const int2 cc = *reinterpret_cast<const int2*>(bcols + p);
-            double2 v[9];
-            #pragma unroll
-            for (int q = 0; q < 9; ++q) v[q] = __ldg(reinterpret_cast<const double2*>(bvals + q * cap + p));
-            double x0[3], x1[3];
-            #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                if (MODE == 1) {
-                    x0[d] = __fma_rn(beta, pold[3 * (size_t)cc.x + d], xin[3 * (size_t)cc.x + d]);
-                    x1[d] = __fma_rn(beta, pold[3 * (size_t)cc.y + d], xin[3 * (size_t)cc.y + d]);
-                } else {
-                    x0[d] = xin[3 * (size_t)cc.x + d];
-                    x1[d] = xin[3 * (size_t)cc.y + d];
-                }
-            }
-            a0 += v[0].x * x0[0] + v[1].x * x0[1] + v[2].x * x0[2] + v[0].y * x1[0] + v[1].y * x1[1] + v[2].y * x1[2];
-            a1 += v[3].x * x0[0] + v[4].x * x0[1] + v[5].x * x0[2] + v[3].y * x1[0] + v[4].y * x1[1] + v[5].y * x1[2];
-            a2 += v[6].x * x0[0] + v[7].x * x0[1] + v[8].x * x0[2] + v[6].y * x1[0] + v[7].y * x1[1] + v[8].y * x1[2];
-        }
-        if (longw) {  // warp-uniform branch
-            #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
-            }
-        } else {
-            #pragma unroll
-            for (int o = 4; o > 0; o >>= 1) {
-                a0 += __shfl_xor_sync(0xffffffffu, a0, o, 8);
-                a1 += __shfl_xor_sync(0xffffffffu, a1, o, 8);
-                a2 += __shfl_xor_sync(0xffffffffu, a2, o, 8);
-            }
-        }
-        if (l == 0 && row >= 0) {
-            double* yr = y + 3 * (size_t)row;
-            if (MODE == 0) {
-                if (b != 0.0) { yr[0] = a * a0 + b * yr[0]; yr[1] = a * a1 + b * yr[1]; yr[2] = a * a2 + b * yr[2]; }
-                else { yr[0] = a * a0; yr[1] = a * a1; yr[2] = a * a2; }
-            } else if (MODE == 1) {
-                const double p0 = __fma_rn(beta, pold[3 * (size_t)row], xin[3 * (size_t)row]);
-                const double p1 = __fma_rn(beta, pold[3 * (size_t)row + 1], xin[3 * (size_t)row + 1]);
-                const double p2 = __fma_rn(beta, pold[3 * (size_t)row + 2], xin[3 * (size_t)row + 2]);
-                pnew[3 * (size_t)row] = p0; pnew[3 * (size_t)row + 1] = p1; pnew[3 * (size_t)row + 2] = p2;
-                yr[0] = a0; yr[1] = a1; yr[2] = a2;
-                dot = p0 * a0 + p1 * a1 + p2 * a2;
-            } else {
-                const double* br = rhs + 3 * (size_t)row;
-                yr[0] = br[0] - a0; yr[1] = br[1] - a1; yr[2] = br[2] - a2;
-            }
-        }
-    }
+    const double dot = spmv_unit<MODE>(A, gw, threadIdx.x & 31, xin, pold, pnew, y, rhs, a, b, beta);
     if (MODE != 1) return;
     double total;
     if (grid_sum_last<kT>(block_sum<kT>(dot, sh), partials, ticket, sh, &total)) {
@@ -633,13 +561,14 @@ int pcg_run(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, 
     if (ensure_vec(c, nrows)) return SGMAS_ERR_CUDA;
     const int gmax = nrows / 8 + 16;  // >= every grid of the loop (SpMV: at most one warp per row)
     if (ensure_partials(c, gmax)) return SGMAS_ERR_CUDA;
-    if (!c->d_state) {
-        if (ctx_alloc(c, &c->d_state, 1) || ctx_alloc(c, &c->d_ticket, 1)) return SGMAS_ERR_CUDA;
+    if (!c->d_state && ctx_alloc(c, &c->d_state, 1)) return SGMAS_ERR_CUDA;
+    if (!c->d_ticket) {
+        if (ctx_alloc(c, &c->d_ticket, 1)) return SGMAS_ERR_CUDA;
         SG_CUDA(c, cudaMemset(c->d_ticket, 0, sizeof(unsigned)));
     }
     int rc = 0;
     // graph cache key: everything the recorded launches capture
-    unsigned long long key[8] = {(unsigned long long)(uintptr_t)b,
+    unsigned long long key[10] = {(unsigned long long)(uintptr_t)b,
                                  (unsigned long long)(uintptr_t)x,
                                  (unsigned long long)nrows | ((unsigned long long)c->bsr.cap << 24) ^
                                      ((unsigned long long)c->bsr.n_long << 44),
@@ -650,9 +579,11 @@ int pcg_run(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, 
                                  (unsigned long long)(uintptr_t)c->d_r,
                                  (unsigned long long)cfg.max_iter ^ ((unsigned long long)cfg.check_every << 32) ^
                                      ((unsigned long long)cfg.use_prec_norm << 48) ^
-                                     (unsigned long long)(cfg.rel_tol * 1e18) ^ ((unsigned long long)(cfg.abs_tol * 1e30) << 7)};
+                                     (unsigned long long)(cfg.rel_tol * 1e18) ^ ((unsigned long long)(cfg.abs_tol * 1e30) << 7),
+                                 (unsigned long long)(uintptr_t)c->d_partials,
+                                 (unsigned long long)(uintptr_t)c->d_ticket};
     bool same = c->graph_exec != nullptr;
-    for (int i = 0; i < 8 && same; ++i) same = key[i] == c->graph_key[i];
+    for (int i = 0; i < 10 && same; ++i) same = key[i] == c->graph_key[i];
     if (!same) {
         if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
         if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
@@ -703,7 +634,7 @@ int pcg_run(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, 
         if (rc) return rc;
         if (e != cudaSuccess) return ctx_fail(c, SGMAS_ERR_CUDA, "capture body: %s", cudaGetErrorString(e));
         SG_CUDA(c, cudaGraphInstantiate(&c->graph_exec, g, 0));
-        for (int i = 0; i < 8; ++i) c->graph_key[i] = key[i];
+        for (int i = 0; i < 10; ++i) c->graph_key[i] = key[i];
         c->graph_kernels_prologue = nk_pro;
         c->graph_kernels_body = nk_body;
     }
@@ -723,6 +654,8 @@ int pcg_run(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, 
         const int bodies = (h.iters + 9) / 10;
         *launches = c->graph_kernels_prologue + c->graph_kernels_body * (bodies < 1 ? 1 : bodies);
     }
+    c->last_persistent = false;
+    c->last_run = cfg;
     c->last_cfg = {cfg.precond, cfg.abd_bodies, 1};
     c->last_b = b;
     c->last_x = x;
@@ -733,11 +666,80 @@ int pcg_run(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, 
 // Replay each kernel of one iteration `reps` times with events around each
 // group (the solve's own graph gives no per-kernel times).  The replay
 // overwrites x, r, z, p, Ap; the next solve re-initialises them.
+// Persistent solves: the same solve again with clock stamps at every phase
+// boundary of CTA 0; the phase times are averaged over iterations
+// 1..min(iters, kStampIters) that are not residual-refresh iterations.
+static int pcg_profile_persistent(sgmas_context* c, float* ms, int n_ms) {
+    constexpr int kStampIters = 1000;
+    int n_sm = 0;
+    SG_CUDA(c, cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, c->device));
+    const size_t n_it = 8 * (size_t)(kStampIters + 2);
+    const size_t n_st = n_it + 16 * (size_t)n_sm;
+    if (c->d_stamps && c->stamps_cap < n_st) { cudaFree(c->d_stamps); c->d_stamps = nullptr; }
+    c->stamps_cap = n_st;
+    if (!c->d_stamps && ctx_alloc(c, &c->d_stamps, n_st)) return SGMAS_ERR_CUDA;
+    SG_CUDA(c, cudaMemsetAsync(c->d_stamps, 0, n_st * sizeof(unsigned long long), c->stream));
+    float loop_ms = 0.f;
+    int rc = pcg_run_persistent(c, c->last_b, c->last_x, c->last_run, &loop_ms, nullptr, c->d_stamps, kStampIters);
+    if (rc) return rc < 0 ? rc : ctx_fail(c, SGMAS_ERR_STATE, "persistent solve no longer fits");
+    unsigned long long* h = new unsigned long long[n_st];
+    cudaError_t e = cudaMemcpy(h, c->d_stamps, n_st * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { delete[] h; return ctx_fail(c, SGMAS_ERR_CUDA, "stamps: %s", cudaGetErrorString(e)); }
+    PcgState st;
+    SG_CUDA(c, cudaMemcpy(&st, c->d_state, sizeof(PcgState), cudaMemcpyDeviceToHost));
+    const double cyc = (double)(h[1] - h[0]);
+    const double ms_per_cycle = cyc > 0 ? loop_ms / cyc : 0.0;
+    double sum[4] = {0, 0, 0, 0};
+    int n = 0;
+    const int last = std::min(st.iters - 1, kStampIters);  // the converged iteration may stop early
+    for (int k = 1; k <= last; ++k) {
+        const unsigned long long* t = h + 8 * (size_t)(k + 1);
+        if (k % 10 == 0 || t[5] == 0) continue;
+        const bool split = t[3] != 0;  // levels >= 2 after their own barrier
+        sum[0] += (double)(t[1] - t[0]);
+        sum[1] += (double)((split ? t[3] : t[5]) - t[1]);
+        sum[2] += split ? (double)(t[5] - t[3]) : 0.0;
+        ++n;
+    }
+    // per barrier slot: mean and max over CTAs of the work before it, mean wait in it
+    const double passes = (double)h[2];
+    double slot_stats[6][3] = {};
+    for (int sl = 0; sl < 6; ++sl) {
+        const double occ = (sl == 1 || sl == 2) ? std::floor(passes / 10.0) : passes;
+        double wsum = 0.0, wmax = 0.0, tsum = 0.0;
+        for (int b = 0; b < n_sm; ++b) {
+            const unsigned long long* acc = h + n_it + 16 * (size_t)b + 2 * sl;
+            wsum += (double)acc[0];
+            wmax = std::max(wmax, (double)acc[0]);
+            tsum += (double)acc[1];
+        }
+        if (occ > 0) {
+            slot_stats[sl][0] = wsum / n_sm / occ * ms_per_cycle;
+            slot_stats[sl][1] = wmax / occ * ms_per_cycle;
+            slot_stats[sl][2] = tsum / n_sm / occ * ms_per_cycle;
+        }
+    }
+    delete[] h;
+    for (int i = 0; i < n_ms; ++i) ms[i] = 0.f;
+    for (int i = 0; i < 4 && i < n_ms; ++i) ms[i] = n ? (float)(sum[i] / n * ms_per_cycle) : 0.f;
+    if (n_ms > 4) ms[4] = loop_ms;
+    if (n_ms > 5) ms[5] = (float)n;
+    for (int i = 6; i < n_ms && i < 24; ++i) ms[i] = (float)slot_stats[(i - 6) / 3][(i - 6) % 3];
+    c->solved = false;
+    return 0;
+}
+
 int pcg_profile(sgmas_context* c, int reps, float* ms, int n_ms) {
     if (!c->solved) return ctx_fail(c, SGMAS_ERR_STATE, "sgmas_pcg_profile needs a completed sgmas_pcg_solve");
+    if (c->last_persistent) return pcg_profile_persistent(c, ms, n_ms);
     cudaStream_t s = c->stream;
     const BsrMatrix& B = c->bsr;
     const int nrows = B.nrows;
+    if (ensure_partials(c, nrows / 8 + 16)) return SGMAS_ERR_CUDA;  // the persistent solve sizes them per CTA
+    if (!c->d_ticket) {
+        if (ctx_alloc(c, &c->d_ticket, 1)) return SGMAS_ERR_CUDA;
+        SG_CUDA(c, cudaMemset(c->d_ticket, 0, sizeof(unsigned)));
+    }
     PcgState h;
     SG_CUDA(c, cudaMemcpyAsync(&h, c->d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
     SG_CUDA(c, cudaStreamSynchronize(s));

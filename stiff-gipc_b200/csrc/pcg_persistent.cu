@@ -1,0 +1,688 @@
+// pcg_persistent.cu -- the whole PCG solve (PCGSolver::pcg,
+// SG/linear_system/solver/pcg_solver.cu:171-304) with the MAS preconditioner
+// (MASPreconditioner::preconditioning, SG/MASPreconditioner.cu:2173-2196) as
+// one cooperative, persistent kernel: one CTA per SM for the whole loop.
+//
+// Ownership.  Level-1 nodes of the MAS hierarchy are numbered in level-0 bank
+// order (component ids are an exclusive scan over the banks), so a range of
+// level-1 banks is fed by a range of level-0 banks.  CTA c owns level-1 banks
+// [c k1, (c+1) k1) and processes every level-0 bank whose components fall in
+// them (a bank split between two CTAs is processed by both; each vertex
+// belongs to the CTA that owns its level-1 node).  Level 0, level 1 and the
+// push of level-1 residuals into level 2 then need no grid-wide step; the few
+// nodes of levels >= 2 are processed redundantly by every CTA in shared
+// memory.  An iteration is three phases with a grid barrier after each:
+//   A  p = z + beta p_old, Ap = A p, p.Ap partials            (SpMV)
+//   B  x += alpha p, r -= alpha Ap, level-0 and level-1 Schwarz, R2 push
+//   C  levels >= 2 (redundant per CTA) + CollectFinalZ, r.z / r.r partials
+// (B and C fuse when the hierarchy has at most two levels.)  Every 10th
+// iteration adds x += alpha p | r = b - A x (the reference's true residual).
+//
+//  * Each thread keeps its level-0 slot's x, r and level-0 Schwarz result in
+//    registers across the phases; x and r reach global memory only for the
+//    residual refresh and at the end.
+//  * The CTA partials of p.Ap, r.z, r.r go to a small array; every CTA sums
+//    all partials in CTA order itself (same values everywhere, deterministic).
+//  * Subdomain inverse tiles (levels 0, 1 and, when they fit, >= 2) are
+//    copied into shared memory once per solve (one bulk copy) and stay there.
+//  * Data written by other CTAs in an earlier phase is read with plain weak
+//    loads: the grid barrier is a release (red.release) / acquire
+//    (ld.acquire) pair, after which weak loads see every write before it.
+//  * Sums keep the order of the graph-form kernels (component sums and group
+//    sums in lane order, Schwarz columns ascending, collect in level order),
+//    so z is bit-identical to sgmas_mas_apply.
+#include <algorithm>
+
+#include "../../include/sgmas.h"
+#include "ctx.hpp"
+#include "mas_dev.cuh"
+#include "spmv_dev.cuh"
+
+using namespace sgmas;
+
+namespace {
+
+constexpr int kPT = 512;  // threads per CTA
+
+struct PArgs {
+    BsrView A;
+    const double* b;
+    double *x, *r, *z, *p0, *p1, *Ap;
+    int nrows, units;  // SpMV warp units
+    // MAS
+    int N, Mm, L, total;
+    int lvl_count[kMaxLevels + 2], lvl_begin[kMaxLevels + 2];
+    const int *part_map, *going_next, *coarse_table;
+    const unsigned* fine_mask;
+    const int* l1_bank;  // level-0 bank of each level-1 node
+    const void* inv;
+    void* R;             // level-2 residual pushes (Acc, global node ids)
+    int k0, k1, nb0, nb1;  // level-0 banks per CTA (max), level-1 banks per CTA, bank counts
+    int nc;                // nodes of levels >= 2 (a multiple of B)
+    int cache_c, kd;       // levels >= 2 tiles cached in shared memory, else staged kd at a time
+    // block-Jacobi
+    const double* dinv;
+    int abd_rows, precond;
+    // control
+    int max_iter, check_every, use_prec_norm;
+    double rel2, abs2;
+    double* partials;  // [3][grid]
+    unsigned* sync;    // [0] barrier arrivals (monotonic)
+    PcgState* st;
+    int* err;
+    // optional phase stamps (clock64 of CTA 0): [0] start, [1] end, [2] loop
+    // passes, then 8 per iteration k = 1..stamp_iters at 8 * (k + 1): loop
+    // top, after the SpMV barrier, after the refresh, after the level 0-1
+    // barrier (0 when fused), -, after the last barrier.  From
+    // 8 * (stamp_iters + 2) on, 16 per CTA: per barrier slot (0 SpMV, 1 x
+    // refresh, 2 r refresh, 3 levels 0-1, 5 end of iteration) the cycles of
+    // work before it and of waiting in it, summed over the loop.
+    unsigned long long* stamps;
+    int stamp_iters;
+};
+
+__device__ __forceinline__ void stamp(const PArgs& a, int k, int slot) {
+    if (a.stamps && blockIdx.x == 0 && threadIdx.x == 0 && k <= a.stamp_iters)
+        a.stamps[8 * (size_t)(k + 1) + slot] = clock64();
+}
+
+// ---- grid barrier: monotonic arrival counter, release add / acquire poll ---
+// Barrier number `epoch` (1, 2, ...) completes when the counter reaches
+// epoch * gridDim.x.  Bounded spin; a timeout sets the error flag.
+// acc (thread 0 of each CTA, profiling only): += work and wait cycles of this
+// barrier slot; t_rel carries the previous release time.
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned& epoch, int* err,
+                                             unsigned long long* acc = nullptr, long long* t_rel = nullptr) {
+    __shared__ int ok_sh;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const long long t_arrive = acc ? clock64() : 0;
+        epoch += 1u;
+        const unsigned target = epoch * gridDim.x;
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
+        int ok = 0;
+        for (int it = 0; it < kSpinLimit; ++it) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+            if ((int)(v - target) >= 0) { ok = 1; break; }
+        }
+        if (!ok) set_error(err, kDevWaitTimeout);
+        ok_sh = ok;
+        if (acc) {
+            const long long t = clock64();
+            acc[0] += (unsigned long long)(t_arrive - *t_rel);
+            acc[1] += (unsigned long long)(t - t_arrive);
+            *t_rel = t;
+        }
+    }
+    __syncthreads();
+    return ok_sh != 0;
+}
+
+// sum of the grid's partials in CTA order (every CTA gets the same value)
+__device__ __forceinline__ double sum_partials(const double* part, double* sh) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += kPT) s += part[i];
+    s = block_sum<kPT>(s, sh);
+    __shared__ double out;
+    if (threadIdx.x == 0) out = s;
+    __syncthreads();
+    const double v = out;
+    __syncthreads();
+    return v;
+}
+
+// ---- block-Jacobi tail (z = D^-1 r with 3x3 inverses) ----------------------
+__device__ void phase_jacobi(const PArgs& a, int mode, double alpha, const double* pcur, double* part_rz,
+                             double* part_rr, double* sh) {
+    double rz = 0.0, rr = 0.0;
+    for (int i = blockIdx.x * kPT + threadIdx.x; i < a.nrows; i += gridDim.x * kPT) {
+        double rv[3], xv[3], pv[3], qv[3], D[9];
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) rv[d] = a.r[3 * (size_t)i + d];
+        #pragma unroll
+        for (int q = 0; q < 9; ++q) D[q] = a.dinv[9 * (size_t)i + q];
+        if (mode == 1) {  // every load before the first store (the pointers may alias)
+            #pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                xv[d] = a.x[3 * (size_t)i + d];
+                pv[d] = pcur[3 * (size_t)i + d];
+                qv[d] = a.Ap[3 * (size_t)i + d];
+            }
+            #pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                rv[d] = rv[d] - alpha * qv[d];
+                a.x[3 * (size_t)i + d] = xv[d] + alpha * pv[d];
+                a.r[3 * (size_t)i + d] = rv[d];
+            }
+        }
+        rr += rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
+        double zv[3];
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) zv[d] = D[3 * d] * rv[0] + D[3 * d + 1] * rv[1] + D[3 * d + 2] * rv[2];
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) a.z[3 * (size_t)i + d] = zv[d];
+        rz += rv[0] * zv[0] + rv[1] * zv[1] + rv[2] * zv[2];
+    }
+    rz = block_sum<kPT>(rz, sh);
+    rr = block_sum<kPT>(rr, sh);
+    if (threadIdx.x == 0) { part_rz[blockIdx.x] = rz; part_rr[blockIdx.x] = rr; }
+}
+
+// per-CTA ranges of the MAS ownership
+struct Own {
+    int lo, nbk0;  // level-0 banks [lo, lo + nbk0)
+    int j0, nbk1;  // level-1 banks [j0, j0 + nbk1) (bank index within level 1)
+};
+
+template <int B>
+__device__ __forceinline__ Own own_ranges(const PArgs& a) {
+    Own o;
+    if (a.L >= 2) {
+        const int cnt1 = a.lvl_count[1];
+        o.j0 = blockIdx.x * a.k1;
+        const int j1 = min(o.j0 + a.k1, a.nb1);
+        o.nbk1 = max(0, j1 - o.j0);
+        const int n_lo = o.j0 * B, n_hi = min(j1 * B, cnt1) - 1;
+        if (n_lo <= n_hi) {
+            o.lo = a.l1_bank[n_lo];
+            o.nbk0 = a.l1_bank[n_hi] - o.lo + 1;
+        } else {
+            o.lo = 0;
+            o.nbk0 = 0;
+        }
+    } else {
+        o.j0 = 0;
+        o.nbk1 = 0;
+        o.lo = blockIdx.x * a.k0;
+        o.nbk0 = max(0, min(a.k0, a.nb0 - o.lo));
+    }
+    return o;
+}
+
+// Schwarz of `nbk` banks whose residuals are in shared memory (rs, node-local
+// index) with tiles at `tiles`; results to zs.  Warps whose half-warps are all
+// idle skip (the shuffles need whole warps).
+template <int B, typename S, typename Acc>
+__device__ __forceinline__ void smem_banks(const S* tiles, const Acc* rs, Acc* zs, int nbk) {
+    constexpr int bs = bsym_of(B);
+    constexpr int HPW = 32 / B;
+    const int lane = threadIdx.x % B;
+    for (int q0 = 0; q0 < nbk; q0 += kPT / B) {
+        const int hw = q0 + threadIdx.x / B;
+        if ((hw / HPW) * HPW >= nbk) continue;  // whole warp idle
+        const bool valid = hw < nbk;
+        const int i = hw * B + lane;
+        const Acc v0 = valid ? rs[3 * i] : (Acc)0, v1 = valid ? rs[3 * i + 1] : (Acc)0,
+                  v2 = valid ? rs[3 * i + 2] : (Acc)0;
+        Acc z0, z1, z2;
+        schwarz_rows<B, S, Acc>(tiles + (size_t)(valid ? hw : 0) * bs * 9, lane, v0, v1, v2, z0, z1, z2);
+        if (valid) { zs[3 * i] = z0; zs[3 * i + 1] = z1; zs[3 * i + 2] = z2; }
+    }
+}
+
+// levels >= 2, redundantly in every CTA: level-2 residuals from global memory,
+// levels >= 3 by group sums in shared memory, then the Schwarz products.
+template <int B, typename S, typename Acc>
+__device__ __forceinline__ bool levels_c(const PArgs& a, S* tilesC, Acc* Rc, Acc* Zc, const int* parc,
+                                         uint64_t* mbar, unsigned& mphase) {
+    constexpr int bs = bsym_of(B);
+    constexpr int HPW = 32 / B;
+    const int base = a.lvl_begin[2];
+    const Acc* Rg = (const Acc*)a.R;
+    for (int i = threadIdx.x; i < a.lvl_count[2]; i += kPT) {
+        Rc[3 * i] = Rg[3 * (size_t)(base + i)];
+        Rc[3 * i + 1] = Rg[3 * (size_t)(base + i) + 1];
+        Rc[3 * i + 2] = Rg[3 * (size_t)(base + i) + 2];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x % B;
+    for (int lvl = 3; lvl < a.L; ++lvl) {
+        const int off = a.lvl_begin[lvl - 1] - base, cnt = a.lvl_count[lvl - 1];
+        const int nb = (cnt + B - 1) / B;
+        for (int q0 = 0; q0 < nb; q0 += kPT / B) {
+            const int k = q0 + threadIdx.x / B;
+            if ((k / HPW) * HPW >= nb) continue;
+            const bool valid = k < nb && k * B + lane < cnt;
+            const int i = off + k * B + lane;
+            const Acc v0 = valid ? Rc[3 * i] : (Acc)0, v1 = valid ? Rc[3 * i + 1] : (Acc)0,
+                      v2 = valid ? Rc[3 * i + 2] : (Acc)0;
+            const int par = valid ? parc[i] : -1;
+            Acc s0, s1, s2;
+            bool lead;
+            group_sum<B, Acc>(par, v0, v1, v2, lane, s0, s1, s2, lead);
+            if (lead) { Rc[3 * par] = s0; Rc[3 * par + 1] = s1; Rc[3 * par + 2] = s2; }
+        }
+        __syncthreads();
+    }
+    const int nbc = a.nc / B;
+    if (a.cache_c) {
+        smem_banks<B, S, Acc>(tilesC, Rc, Zc, nbc);
+    } else {
+        const S* inv = (const S*)a.inv + (size_t)(base / B) * bs * 9;
+        for (int c0 = 0; c0 < nbc; c0 += a.kd) {
+            const int ncb = min(a.kd, nbc - c0);
+            __syncthreads();  // the previous chunk's tiles are no longer read
+            if (threadIdx.x == 0) {
+                const unsigned bytes = (unsigned)(ncb * bs * 9 * sizeof(S));
+                mbar_expect_tx(mbar, bytes);
+                bulk_g2s(tilesC, inv + (size_t)c0 * bs * 9, bytes, mbar);
+            }
+            if (!mbar_wait(mbar, mphase, a.err)) return false;
+            mphase ^= 1u;
+            smem_banks<B, S, Acc>(tilesC, Rc + 3 * (size_t)c0 * B, Zc + 3 * (size_t)c0 * B, ncb);
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
+template <int B, typename S, typename Acc>
+__global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ uint64_t mbar;
+    __shared__ double sh[32];
+    constexpr int bs = bsym_of(B);
+    constexpr int HPW = 32 / B;
+    const size_t tb = (size_t)bs * 9;  // elements per tile
+    const bool mas = a.precond == 1;
+    // shared memory: tiles0 [k0] | tiles1 [k1] | tilesC [nc/B or kd] | R1s, Z1s [k1 B 3] | Rc, Zc [nc 3] | parc [nc]
+    S* tiles0 = reinterpret_cast<S*>(smem_raw);
+    S* tiles1 = tiles0 + (size_t)a.k0 * tb;
+    S* tilesC = tiles1 + (size_t)a.k1 * tb;
+    Acc* R1s = reinterpret_cast<Acc*>(tilesC + (size_t)(a.cache_c ? a.nc / B : a.kd) * tb);
+    Acc* Z1s = R1s + 3 * (size_t)a.k1 * B;
+    Acc* Rc = Z1s + 3 * (size_t)a.k1 * B;
+    Acc* Zc = Rc + 3 * (size_t)a.nc;
+    int* parc = reinterpret_cast<int*>(Zc + 3 * (size_t)a.nc);
+    if (a.stamps && blockIdx.x == 0 && threadIdx.x == 0) a.stamps[0] = clock64();
+    unsigned epoch = 0u, mphase = 0u;
+    double* part_pap = a.partials;
+    double* part_rz = a.partials + gridDim.x;
+    double* part_rr = a.partials + 2 * gridDim.x;
+    const int lane = threadIdx.x % B, hw = threadIdx.x / B;
+    bool ok = true;
+
+    // ---- ownership, per-thread constants, cached tiles ----------------------
+    Own o = {0, 0, 0, 0};
+    int v = -1, n1loc = -1, par1 = -1;
+    unsigned msk = 0u;
+    bool own = false;
+    if (mas) {
+        o = own_ranges<B>(a);
+        const int b1 = a.lvl_begin[1] / B;
+        if (threadIdx.x == 0) { mbar_init(&mbar, 1); fence_mbar_init(); }
+        for (int i = threadIdx.x; i < 3 * a.k1 * B; i += kPT) { R1s[i] = (Acc)0; Z1s[i] = (Acc)0; }
+        for (int i = threadIdx.x; i < 3 * a.nc; i += kPT) { Rc[i] = (Acc)0; Zc[i] = (Acc)0; }
+        for (int i = threadIdx.x; i < a.nc; i += kPT) {  // parents of the nodes of levels 2 .. L-2
+            const int node = a.lvl_begin[2] + i;
+            int par = -1;
+            for (int l = 2; l + 1 < a.L; ++l)
+                if (node >= a.lvl_begin[l] && node < a.lvl_begin[l] + a.lvl_count[l])
+                    par = a.going_next[node] - a.lvl_begin[2];
+            parc[i] = par;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned by0 = (unsigned)(o.nbk0 * tb * sizeof(S)), by1 = (unsigned)(o.nbk1 * tb * sizeof(S));
+            const unsigned byc = a.cache_c ? (unsigned)((a.nc / B) * tb * sizeof(S)) : 0u;
+            mbar_expect_tx(&mbar, by0 + by1 + byc);
+            if (by0) bulk_g2s(tiles0, (const S*)a.inv + (size_t)o.lo * tb, by0, &mbar);
+            if (by1) bulk_g2s(tiles1, (const S*)a.inv + (size_t)(b1 + o.j0) * tb, by1, &mbar);
+            if (byc) bulk_g2s(tilesC, (const S*)a.inv + (size_t)(a.lvl_begin[2] / B) * tb, byc, &mbar);
+        }
+        if (hw < o.nbk0) v = a.part_map[(o.lo + hw) * B + lane];
+        if (v >= 0) {
+            msk = a.fine_mask[v];
+            if (a.L >= 2) {
+                const int n1 = a.going_next[v] - a.lvl_begin[1];
+                n1loc = n1 - o.j0 * B;
+                own = n1loc >= 0 && n1loc < o.nbk1 * B;
+            } else {
+                own = true;
+            }
+        }
+        if (a.L > 2 && hw < o.nbk1) {
+            const int i1 = (o.j0 + hw) * B + lane;
+            if (i1 < a.lvl_count[1]) par1 = a.going_next[a.lvl_begin[1] + i1] - a.lvl_begin[2];
+        }
+        ok = mbar_wait(&mbar, mphase, a.err);
+        mphase ^= 1u;
+    }
+    const bool act0 = (hw / HPW) * HPW < o.nbk0;  // this warp has level-0 work
+    const bool act1 = (hw / HPW) * HPW < o.nbk1;  // this warp has level-1 work
+
+    // ---- MAS pieces on the registers of this thread's slot ----------------
+    double x0 = 0.0, x1 = 0.0, x2 = 0.0, r0 = 0.0, r1 = 0.0, r2 = 0.0;
+    Acc zl0 = 0, zl1 = 0, zl2 = 0;  // level-0 Schwarz of the slot
+    // level-0 (+ level-1) part of the apply on r (registers)
+    auto apply_b = [&]() {
+        if (act0) {
+            const Acc ra = (Acc)r0, rb = (Acc)r1, rc = (Acc)r2;
+            Acc s0 = 0, s1 = 0, s2 = 0;
+            #pragma unroll 4
+            for (int j = 0; j < B; ++j) {
+                const Acc y0 = shfl_acc(ra, j, B), y1 = shfl_acc(rb, j, B), y2 = shfl_acc(rc, j, B);
+                if (msk & (1u << j)) { s0 += y0; s1 += y1; s2 += y2; }
+            }
+            if (own && a.L >= 2 && __popc(msk & lanemask_lt(lane)) == 0) {
+                R1s[3 * n1loc] = s0; R1s[3 * n1loc + 1] = s1; R1s[3 * n1loc + 2] = s2;
+            }
+            schwarz_rows<B, S, Acc>(tiles0 + (size_t)(hw < o.nbk0 ? hw : 0) * tb, lane, ra, rb, rc, zl0, zl1, zl2);
+        }
+        if (a.L < 2) return;
+        __syncthreads();
+        if (act1) {  // level-1 banks of this CTA: push to level 2, Schwarz
+            const bool valid = hw < o.nbk1;
+            const int i = hw * B + lane;
+            const Acc v0 = valid ? R1s[3 * i] : (Acc)0, v1 = valid ? R1s[3 * i + 1] : (Acc)0,
+                      v2 = valid ? R1s[3 * i + 2] : (Acc)0;
+            if (a.L > 2) {
+                Acc s0, s1, s2;
+                bool lead;
+                group_sum<B, Acc>(par1, v0, v1, v2, lane, s0, s1, s2, lead);
+                if (lead) {
+                    Acc* Rg = (Acc*)a.R + 3 * (size_t)(a.lvl_begin[2] + par1);
+                    Rg[0] = s0; Rg[1] = s1; Rg[2] = s2;
+                }
+            }
+            Acc z0, z1, z2;
+            schwarz_rows<B, S, Acc>(tiles1 + (size_t)(valid ? hw : 0) * tb, lane, v0, v1, v2, z0, z1, z2);
+            if (valid) { Z1s[3 * i] = z0; Z1s[3 * i + 1] = z1; Z1s[3 * i + 2] = z2; }
+        }
+        __syncthreads();
+    };
+    // CollectFinalZ for the owned slot + r.z, r.r partials
+    auto collect = [&]() {
+        double rz = 0.0, rr = 0.0;
+        if (own) {
+            Acc c0 = zl0, c1 = zl1, c2 = zl2;
+            if (a.L >= 2) { c0 += Z1s[3 * n1loc]; c1 += Z1s[3 * n1loc + 1]; c2 += Z1s[3 * n1loc + 2]; }
+            for (int l = 2; l < a.L; ++l) {
+                const int n = a.coarse_table[(size_t)kMaxLevels * v + l - 1] - a.lvl_begin[2];
+                c0 += Zc[3 * n]; c1 += Zc[3 * n + 1]; c2 += Zc[3 * n + 2];
+            }
+            const double z0 = (double)c0, z1 = (double)c1, z2 = (double)c2;
+            a.z[3 * (size_t)v] = z0; a.z[3 * (size_t)v + 1] = z1; a.z[3 * (size_t)v + 2] = z2;
+            rz = r0 * z0 + r1 * z1 + r2 * z2;
+            rr = r0 * r0 + r1 * r1 + r2 * r2;
+        }
+        rz = block_sum<kPT>(rz, sh);
+        rr = block_sum<kPT>(rr, sh);
+        if (threadIdx.x == 0) { part_rz[blockIdx.x] = rz; part_rr[blockIdx.x] = rr; }
+    };
+
+    // ---- prologue: x = 0, r = b, p_old = 0, z = M^-1 r, r.z, r.r
+    for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT) {
+        a.p0[i] = 0.0;
+        if (!mas) { a.x[i] = 0.0; a.r[i] = a.b[i]; }
+    }
+    if (mas) {
+        if (v >= 0) { r0 = a.b[3 * (size_t)v]; r1 = a.b[3 * (size_t)v + 1]; r2 = a.b[3 * (size_t)v + 2]; }
+        if (ok) apply_b();
+        if (a.L > 2) {
+            ok = ok && grid_barrier(a.sync, epoch, a.err);
+            if (ok) ok = levels_c<B, S, Acc>(a, tilesC, Rc, Zc, parc, &mbar, mphase);
+        }
+        if (ok) collect();
+    } else {
+        ok = ok && grid_barrier(a.sync, epoch, a.err);
+        if (ok) phase_jacobi(a, 0, 0.0, a.p1, part_rz, part_rr, sh);
+    }
+    ok = ok && grid_barrier(a.sync, epoch, a.err);
+    double rz = ok ? sum_partials(part_rz, sh) : 0.0;
+    const double rz0 = rz;
+    const double rr0 = ok ? sum_partials(part_rr, sh) : 0.0;
+    double rr_last = rr0, beta = 0.0;
+    int k = 1, iters = 1, converged = 0;
+    bool done = !ok || a.max_iter <= 1;
+    double* pold = a.p0;
+    double* pnew = a.p1;
+    unsigned long long* acc = a.stamps ? a.stamps + 8 * (size_t)(a.stamp_iters + 2) + 16 * (size_t)blockIdx.x : nullptr;
+    long long t_rel = clock64();
+#define SLOT(i) (acc ? acc + 2 * (i) : nullptr), &t_rel
+    const int warps = kPT / 32, gw0 = blockIdx.x * warps + threadIdx.x / 32;
+    int passes = 0;
+    while (!done) {
+        ++passes;
+        // A: p_new = z + beta p_old, Ap = A p_new, p.Ap
+        stamp(a, k, 0);
+        double dot = 0.0;
+        for (int u = gw0; u < a.units; u += gridDim.x * warps)
+            dot += spmv_unit<1, true>(a.A, u, threadIdx.x & 31, a.z, pold, pnew, a.Ap, nullptr, 1.0, 0.0, beta);
+        dot = block_sum<kPT>(dot, sh);
+        if (threadIdx.x == 0) part_pap[blockIdx.x] = dot;
+        if (!grid_barrier(a.sync, epoch, a.err, SLOT(0))) { ok = false; break; }
+        stamp(a, k, 1);
+        const bool refresh = k % 10 == 0;  // true residual (pcg_solver.cu:240-244)
+        // B: the slot's p and Ap are loaded before the partials are summed
+        double p0v = 0.0, p1v = 0.0, p2v = 0.0, q0 = 0.0, q1 = 0.0, q2 = 0.0;
+        if (mas && v >= 0) {
+            if (own) { p0v = pnew[3 * (size_t)v]; p1v = pnew[3 * (size_t)v + 1]; p2v = pnew[3 * (size_t)v + 2]; }
+            if (!refresh) { q0 = a.Ap[3 * (size_t)v]; q1 = a.Ap[3 * (size_t)v + 1]; q2 = a.Ap[3 * (size_t)v + 2]; }
+        }
+        const double alpha = rz / sum_partials(part_pap, sh);
+        if (refresh) {
+            if (mas) {
+                if (own) {
+                    x0 += alpha * p0v; x1 += alpha * p1v; x2 += alpha * p2v;
+                    a.x[3 * (size_t)v] = x0; a.x[3 * (size_t)v + 1] = x1; a.x[3 * (size_t)v + 2] = x2;
+                }
+            } else {
+                for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT)
+                    a.x[i] = a.x[i] + alpha * pnew[i];
+            }
+            if (!grid_barrier(a.sync, epoch, a.err, SLOT(1))) { ok = false; break; }
+            for (int u = gw0; u < a.units; u += gridDim.x * warps)
+                spmv_unit<2, true>(a.A, u, threadIdx.x & 31, a.x, nullptr, nullptr, a.r, a.b, 1.0, 0.0, 0.0);
+            if (!grid_barrier(a.sync, epoch, a.err, SLOT(2))) { ok = false; break; }
+            if (mas && v >= 0) { r0 = a.r[3 * (size_t)v]; r1 = a.r[3 * (size_t)v + 1]; r2 = a.r[3 * (size_t)v + 2]; }
+        } else if (mas && v >= 0) {
+            r0 = r0 - alpha * q0; r1 = r1 - alpha * q1; r2 = r2 - alpha * q2;
+            if (own) { x0 += alpha * p0v; x1 += alpha * p1v; x2 += alpha * p2v; }
+        }
+        stamp(a, k, 2);
+        if (mas) {
+            apply_b();
+            if (a.L > 2) {
+                if (!grid_barrier(a.sync, epoch, a.err, SLOT(3))) { ok = false; break; }
+                stamp(a, k, 3);
+                if (!levels_c<B, S, Acc>(a, tilesC, Rc, Zc, parc, &mbar, mphase)) ok = false;
+            }
+            collect();
+        } else {
+            phase_jacobi(a, refresh ? 0 : 1, alpha, pnew, part_rz, part_rr, sh);
+        }
+        if (!grid_barrier(a.sync, epoch, a.err, SLOT(5)) || !ok) { ok = false; break; }
+        stamp(a, k, 5);
+        const double rz_new = sum_partials(part_rz, sh);
+        const double rr = sum_partials(part_rr, sh);
+        bool conv = false;
+        if (k % a.check_every == 0) {
+            rr_last = rr;
+            conv = a.use_prec_norm ? (rz_new <= a.rel2 * rz0 || rz_new <= a.abs2)
+                                   : (rr <= a.rel2 * rr0 || rr <= a.abs2);
+            if (!(rz_new == rz_new) || !(rr == rr)) { conv = true; ok = false; }
+        }
+        if (conv) {
+            iters = k;
+            converged = ok ? 1 : 0;
+            done = true;
+        } else {
+            beta = rz_new / rz;
+            rz = rz_new;
+            ++k;
+            iters = k;
+            if (k >= a.max_iter) done = true;
+            double* t = pold; pold = pnew; pnew = t;
+        }
+    }
+#undef SLOT
+    if (mas && own) {
+        a.x[3 * (size_t)v] = x0; a.x[3 * (size_t)v + 1] = x1; a.x[3 * (size_t)v + 2] = x2;
+        a.r[3 * (size_t)v] = r0; a.r[3 * (size_t)v + 1] = r1; a.r[3 * (size_t)v + 2] = r2;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        PcgState s = {};
+        s.rz = rz; s.rz0 = rz0; s.rr0 = rr0; s.rr = rr_last; s.k = k; s.iters = iters; s.done = 1;
+        s.converged = converged;
+        s.max_iter = a.max_iter;
+        s.check_every = a.check_every;
+        *a.st = s;
+        if (a.stamps) {
+            a.stamps[1] = clock64();
+            a.stamps[2] = (unsigned long long)passes;
+        }
+    }
+}
+
+// level-0 bank of every level-1 node (all slots of a component agree)
+template <int B>
+__global__ void k_l1_bank(int Mm, int l1_begin, const int* __restrict__ part_map, const int* __restrict__ going_next,
+                          int* l1_bank) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= Mm) return;
+    const int v = part_map[s];
+    if (v >= 0) l1_bank[going_next[v] - l1_begin] = s / B;
+}
+
+// largest number of level-0 banks any CTA processes
+template <int B>
+__global__ void k_cta_span(int G, int k1, int nb1, int cnt1, const int* __restrict__ l1_bank, unsigned* out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= G) return;
+    const int j0 = c * k1, j1 = min(j0 + k1, nb1);
+    const int n_lo = j0 * B, n_hi = min(j1 * B, cnt1) - 1;
+    if (n_lo <= n_hi) atomicMax(out, (unsigned)(l1_bank[n_hi] - l1_bank[n_lo] + 1));
+}
+
+template <int B, typename S, typename Acc>
+int launch_t(sgmas_context* c, PArgs& a, float* ms) {
+    int dev_sms = 0;
+    SG_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device));
+    constexpr int bs = bsym_of(B);
+    const size_t tb = (size_t)bs * 9 * sizeof(S);
+    int max_smem = 0;
+    SG_CUDA(c, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    const size_t budget = (size_t)max_smem - 2048;  // static shared memory of the kernel
+    const int G = dev_sms;
+    size_t smem = 0;
+    if (a.precond == 1) {
+        a.nb0 = a.Mm / B;
+        if (a.L >= 2) {
+            a.nb1 = (a.lvl_count[1] + B - 1) / B;
+            a.k1 = (a.nb1 + G - 1) / G;
+            // level-0 banks per CTA follow the level-1 ranges
+            if (ctx_alloc_grow(c, &c->d_l1_bank, &c->l1_bank_cap, a.lvl_count[1])) return SGMAS_ERR_CUDA;
+            a.l1_bank = c->d_l1_bank;
+            k_l1_bank<B><<<(a.Mm + 255) / 256, 256, 0, c->stream>>>(a.Mm, a.lvl_begin[1], a.part_map, a.going_next,
+                                                                 c->d_l1_bank);
+            SG_CUDA(c, cudaMemsetAsync(c->d_psync + 4, 0, sizeof(unsigned), c->stream));
+            k_cta_span<B><<<(G + 127) / 128, 128, 0, c->stream>>>(G, a.k1, a.nb1, a.lvl_count[1], c->d_l1_bank,
+                                                                c->d_psync + 4);
+            unsigned span = 0;
+            SG_CUDA(c, cudaMemcpyAsync(&span, c->d_psync + 4, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+            SG_CUDA(c, cudaStreamSynchronize(c->stream));
+            a.k0 = (int)span;
+        } else {
+            a.nb1 = 0;
+            a.k1 = 0;
+            a.k0 = (a.nb0 + G - 1) / G;
+        }
+        a.nc = a.L > 2 ? a.total - a.lvl_begin[2] : 0;
+        if (a.k0 > kPT / B || a.k1 > kPT / B) return 1;  // one slot per thread: use the graph form
+        const size_t fixed = (size_t)(a.k0 + a.k1) * tb + 2 * 3 * (size_t)a.k1 * B * sizeof(Acc) +
+                             2 * 3 * (size_t)a.nc * sizeof(Acc) + (size_t)a.nc * sizeof(int);
+        const int nbc = a.nc / B;
+        if (fixed + (size_t)nbc * tb <= budget) {
+            a.cache_c = 1;
+            a.kd = 0;
+            smem = fixed + (size_t)nbc * tb;
+        } else {
+            if (fixed + tb > budget) return 1;
+            a.cache_c = 0;
+            a.kd = (int)std::min<size_t>((size_t)std::max(nbc, 1), (budget - fixed) / tb);
+            smem = fixed + (size_t)a.kd * tb;
+        }
+    } else {
+        a.k0 = a.k1 = a.nb0 = a.nb1 = a.nc = a.kd = a.cache_c = 0;
+    }
+    auto kern = k_pcg_persistent<B, S, Acc>;
+    SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
+    int per_sm = 0;
+    SG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPT, smem));
+    if (per_sm < 1) return 1;
+    SG_CUDA(c, cudaMemsetAsync(a.sync, 0, sizeof(unsigned), c->stream));
+    void* params[] = {&a};
+    SG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    SG_CUDA(c, cudaLaunchCooperativeKernel((const void*)kern, dim3(G), dim3(kPT), params, smem, c->stream));
+    SG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    SG_CUDA(c, cudaEventSynchronize(c->ev1));
+    SG_CUDA(c, cudaEventElapsedTime(ms, c->ev0, c->ev1));
+    return 0;
+}
+
+}  // namespace
+
+// Returns 0 when solved, 1 when the system does not fit this kernel (the
+// caller then uses the graph path), negative on error.
+int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, float* solve_ms,
+                       int* launches, unsigned long long* stamps, int stamp_iters) {
+    const BsrMatrix& M = c->bsr;
+    if (cfg.precond == 0 && cfg.abd_bodies > 0) return 1;  // 12x12 body blocks: graph form
+    PArgs a = {};
+    a.A = BsrView{M.row_ptr, M.cols, M.vals, M.cap, M.row_list, M.nrows, M.n_long};
+    a.b = b; a.x = x; a.r = c->d_r; a.z = c->d_z; a.p0 = c->d_p0; a.p1 = c->d_p1; a.Ap = c->d_Ap;
+    a.nrows = M.nrows;
+    a.units = M.n_long + (M.nrows - M.n_long + 3) / 4;
+    a.precond = cfg.precond;
+    a.dinv = c->d_diag_inv; a.abd_rows = 0;
+    a.max_iter = cfg.max_iter == 0 ? 3 * M.nrows : cfg.max_iter;
+    a.check_every = cfg.check_every;
+    a.use_prec_norm = cfg.use_prec_norm;
+    a.rel2 = cfg.rel_tol * cfg.rel_tol;
+    a.abs2 = cfg.abs_tol * cfg.abs_tol;
+    a.err = c->d_err;
+    a.stamps = stamps;
+    a.stamp_iters = stamp_iters;
+    if (!c->d_psync) {
+        if (ctx_alloc(c, &c->d_psync, 8)) return SGMAS_ERR_CUDA;
+    }
+    a.sync = c->d_psync;
+    int dev_sms = 0;
+    SG_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device));
+    if (2 * c->partial_cap < 3 * dev_sms) {  // partials of p.Ap, r.z, r.r per CTA (2 * partial_cap doubles)
+        const int cap = (3 * dev_sms + 1) / 2;
+        if (ctx_alloc(c, &c->d_partials, 2 * (size_t)cap)) return SGMAS_ERR_CUDA;
+        c->partial_cap = cap;
+    }
+    if (!c->d_state && ctx_alloc(c, &c->d_state, 1)) return SGMAS_ERR_CUDA;
+    a.st = c->d_state;
+    a.partials = c->d_partials;
+    if (cfg.precond == 1) {
+        a.N = c->N; a.Mm = c->Mm; a.L = c->L; a.total = c->total;
+        for (int l = 0; l <= c->L; ++l) { a.lvl_count[l] = c->h_level_size[2 * l]; a.lvl_begin[l] = c->h_level_size[2 * l + 1]; }
+        a.part_map = c->d_part_map; a.going_next = c->d_going_next;
+        a.coarse_table = c->d_coarse_table; a.fine_mask = c->d_fine_mask;
+        a.inv = c->d_inv; a.R = c->d_R;
+    }
+    int rc;
+    if (c->bank == 16) {
+        rc = c->precision == SGMAS_MAS_FP32   ? launch_t<16, float, float>(c, a, solve_ms)
+             : c->precision == SGMAS_MAS_BF16 ? launch_t<16, __nv_bfloat16, float>(c, a, solve_ms)
+                                              : launch_t<16, double, double>(c, a, solve_ms);
+    } else {
+        rc = c->precision == SGMAS_MAS_FP32   ? launch_t<32, float, float>(c, a, solve_ms)
+             : c->precision == SGMAS_MAS_BF16 ? launch_t<32, __nv_bfloat16, float>(c, a, solve_ms)
+                                              : launch_t<32, double, double>(c, a, solve_ms);
+    }
+    if (rc) return rc;
+    if (launches) *launches = 1;
+    c->last_persistent = true;
+    c->last_run = cfg;
+    c->last_cfg = {cfg.precond, cfg.abd_bodies, 1};
+    c->last_b = b;
+    c->last_x = x;
+    c->solved = true;
+    return 0;
+}

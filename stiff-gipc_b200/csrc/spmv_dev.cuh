@@ -1,0 +1,109 @@
+// spmv_dev.cuh -- one SpMV work unit over the row-owned block CSR, shared by
+// the per-iteration kernel (pcg.cu) and the persistent PCG kernel.
+//   MODE 0: y = a A x + b y
+//   MODE 1: p_new = z + beta p_old (fused), Ap = A p_new; returns p_new.Ap of
+//           the rows this lane wrote (0 elsewhere)
+//   MODE 2: r = rhs - A x
+#pragma once
+#include "ctx.hpp"
+
+namespace sgmas {
+
+// Work split: warps [0, n_long) take one long row each (all 32 lanes), the
+// remaining warps take four short rows (8 lanes each); row_list holds the
+// long rows first, both parts in row order.
+// LIVE = the vector is written by other CTAs earlier in the same launch (the
+// persistent kernel): it is read with an explicit weak ld.global, never the
+// read-only (.nc) path that const __restrict__ would allow; the grid
+// barrier's fences between the phases make those loads current.
+template <bool LIVE>
+__device__ __forceinline__ double ldv(const double* p) {
+    if (LIVE) {
+        double v;
+        asm volatile("ld.global.f64 %0, [%1];" : "=d"(v) : "l"(p));
+        return v;
+    }
+    return *p;
+}
+
+template <int MODE, bool LIVE = false>
+__device__ __forceinline__ double spmv_unit(const BsrView& A, int gw, int lane, const double* __restrict__ xin,
+                                            const double* __restrict__ pold, double* pnew, double* y,
+                                            const double* __restrict__ rhs, double a, double b, double beta) {
+    const int* __restrict__ row_ptr = A.row_ptr;
+    const int* __restrict__ bcols = A.cols;
+    const double* __restrict__ bvals = A.vals;
+    const long long cap = A.cap;
+    const bool longw = gw < A.n_long;
+    int row = -1, l, G;
+    if (longw) {
+        row = A.row_list[gw];
+        l = lane;
+        G = 32;
+    } else {
+        const int g = (gw - A.n_long) * 4 + (lane >> 3);
+        if (g < A.nrows - A.n_long) row = A.row_list[A.n_long + g];
+        l = lane & 7;
+        G = 8;
+    }
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    double dot = 0.0;
+    {
+        const int beg = row >= 0 ? row_ptr[row] : 0, end = row >= 0 ? row_ptr[row + 1] : 0;
+        for (int p = beg + 2 * l; p < end; p += 2 * G) {
+            const int2 cc = *reinterpret_cast<const int2*>(bcols + p);
+            double2 v[9];
+            #pragma unroll
+            for (int q = 0; q < 9; ++q) v[q] = __ldg(reinterpret_cast<const double2*>(bvals + q * cap + p));
+            double x0[3], x1[3];
+            #pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (MODE == 1) {
+                    x0[d] = __fma_rn(beta, ldv<LIVE>(pold + 3 * (size_t)cc.x + d), ldv<LIVE>(xin + 3 * (size_t)cc.x + d));
+                    x1[d] = __fma_rn(beta, ldv<LIVE>(pold + 3 * (size_t)cc.y + d), ldv<LIVE>(xin + 3 * (size_t)cc.y + d));
+                } else {
+                    x0[d] = ldv<LIVE>(xin + 3 * (size_t)cc.x + d);
+                    x1[d] = ldv<LIVE>(xin + 3 * (size_t)cc.y + d);
+                }
+            }
+            a0 += v[0].x * x0[0] + v[1].x * x0[1] + v[2].x * x0[2] + v[0].y * x1[0] + v[1].y * x1[1] + v[2].y * x1[2];
+            a1 += v[3].x * x0[0] + v[4].x * x0[1] + v[5].x * x0[2] + v[3].y * x1[0] + v[4].y * x1[1] + v[5].y * x1[2];
+            a2 += v[6].x * x0[0] + v[7].x * x0[1] + v[8].x * x0[2] + v[6].y * x1[0] + v[7].y * x1[1] + v[8].y * x1[2];
+        }
+        if (longw) {  // warp-uniform branch
+            #pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+            }
+        } else {
+            #pragma unroll
+            for (int o = 4; o > 0; o >>= 1) {
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o, 8);
+                a1 += __shfl_xor_sync(0xffffffffu, a1, o, 8);
+                a2 += __shfl_xor_sync(0xffffffffu, a2, o, 8);
+            }
+        }
+        if (l == 0 && row >= 0) {
+            double* yr = y + 3 * (size_t)row;
+            if (MODE == 0) {
+                if (b != 0.0) { yr[0] = a * a0 + b * ldv<LIVE>(yr); yr[1] = a * a1 + b * ldv<LIVE>(yr + 1); yr[2] = a * a2 + b * ldv<LIVE>(yr + 2); }
+                else { yr[0] = a * a0; yr[1] = a * a1; yr[2] = a * a2; }
+            } else if (MODE == 1) {
+                const double p0 = __fma_rn(beta, ldv<LIVE>(pold + 3 * (size_t)row), ldv<LIVE>(xin + 3 * (size_t)row));
+                const double p1 = __fma_rn(beta, ldv<LIVE>(pold + 3 * (size_t)row + 1), ldv<LIVE>(xin + 3 * (size_t)row + 1));
+                const double p2 = __fma_rn(beta, ldv<LIVE>(pold + 3 * (size_t)row + 2), ldv<LIVE>(xin + 3 * (size_t)row + 2));
+                pnew[3 * (size_t)row] = p0; pnew[3 * (size_t)row + 1] = p1; pnew[3 * (size_t)row + 2] = p2;
+                yr[0] = a0; yr[1] = a1; yr[2] = a2;
+                dot = p0 * a0 + p1 * a1 + p2 * a2;
+            } else {
+                const double* br = rhs + 3 * (size_t)row;
+                yr[0] = br[0] - a0; yr[1] = br[1] - a1; yr[2] = br[2] - a2;
+            }
+        }
+    }
+    return dot;
+}
+
+}  // namespace sgmas

@@ -54,7 +54,7 @@ EXPORTS = [
     "sgmas_mas_download_tables", "sgmas_mas_download_matrices", "sgmas_mas_invert_host",
     "sgmas_pcg_solve", "sgmas_pcg_solve_host", "sgmas_spmv", "sgmas_convert", "sgmas_write_upper_blocks",
     "sgmas_morton_codes", "sgmas_morton_partition", "sgmas_pcg_profile", "sgmas_vert_neighbors",
-    "sgmas_part_maps", "sgmas_morton_codes_noalloc",
+    "sgmas_part_maps", "sgmas_morton_codes_noalloc", "sgmas_set_pcg_mode", "sgmas_pcg_last_vectors",
 ]
 
 MORTON_NOALLOC_MAX_VERTS = 2097152  # SGMAS_MORTON_NOALLOC_MAX_VERTS in include/sgmas.h
@@ -97,6 +97,8 @@ def lib(build_if_missing: bool = False):
     L.sgmas_vert_neighbors.argtypes = [vp, i, vp, i, i, i, vp, vp, vp, i]
     L.sgmas_part_maps.argtypes = [vp, i, i, vp, i, C.POINTER(i), vp]
     L.sgmas_morton_codes_noalloc.argtypes = [vp, i, vp, vp, vp]
+    L.sgmas_set_pcg_mode.argtypes = [vp, i]
+    L.sgmas_pcg_last_vectors.argtypes = [vp, vp, vp]
     _lib = L
     return L
 
@@ -194,6 +196,14 @@ class Context:
     def set_stream(self, stream_ptr):
         self._check(self.L.sgmas_set_stream(self.h, stream_ptr))
 
+    def pcg_last_vectors(self, r=None, z=None):
+        """Copy the last solve's residual r and z = M^-1 r into device arrays."""
+        self._check(self.L.sgmas_pcg_last_vectors(self.h, _ptr(r), _ptr(z)))
+
+    def set_pcg_mode(self, mode):
+        """'persistent' (one cooperative kernel, default) or 'graph' (a kernel per phase)."""
+        self._check(self.L.sgmas_set_pcg_mode(self.h, {"graph": 0, "persistent": 1}[mode]))
+
     def synchronize(self):
         self._check(self.L.sgmas_synchronize(self.h))
 
@@ -277,9 +287,17 @@ class Context:
         return x, {k: getattr(rep, k) for k, _ in PcgReport._fields_}
 
     def pcg_profile(self, reps=20):
-        ms = np.zeros(4, np.float32)
-        self._check(self.L.sgmas_pcg_profile(self.h, reps, _ptr(ms), 4))
-        return dict(spmv=float(ms[0]), update_l0=float(ms[1]), coarse=float(ms[2]), collect=float(ms[3]))
+        """Per-phase device ms of one iteration of the last solve (sgmas_pcg_profile)."""
+        ms = np.zeros(24, np.float32)
+        self._check(self.L.sgmas_pcg_profile(self.h, reps, _ptr(ms), 24))
+        if ms[5] == 0:  # graph form: kernel replays
+            return dict(spmv=float(ms[0]), update_l0=float(ms[1]), coarse=float(ms[2]), collect=float(ms[3]))
+        out = dict(spmv=float(ms[0]), update_levels01=float(ms[1]), levels2_collect=float(ms[2]),
+                   loop_ms=float(ms[4]), stamped_iterations=int(ms[5]))
+        names = ("spmv", "x_refresh", "r_refresh", "levels01", "unused", "end")
+        out["barriers"] = {nm: dict(work_mean=float(ms[6 + 3 * i]), work_max=float(ms[7 + 3 * i]),
+                                    wait_mean=float(ms[8 + 3 * i])) for i, nm in enumerate(names)}
+        return out
 
     # ---- path kernels ----
     def spmv(self, a, vals, rows, cols, n_block_rows, x, b, y):
