@@ -74,19 +74,55 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region: NVML
+    polled every 5 ms from a thread (nvidia-smi -lms 200 as the fallback)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
     def __init__(self, gpu_index):
-        self.path = tempfile.mktemp(suffix=".csv")
         self.idx = gpu_index
         self.p = None
+        self.thread = None
+        self.h = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(gpu_index)
+            try:
+                bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+                self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+            self.nv = pynvml
+        except Exception:
+            self.h = None
+
+    def _poll(self):
+        nv = self.nv
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop_flag:
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                self.bits |= int(get_reasons(self.h))
+            except Exception:
+                pass
+            time.sleep(0.005)
 
     def start(self):
+        if self.h is not None:
+            import threading
+            self.sm, self.bits, self.stop_flag = [], 0, False
+            self.mx = float(self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
         try:
+            self.path = tempfile.mktemp(suffix=".csv")
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
@@ -95,6 +131,15 @@ class Clocks:
             self.p = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag = True
+            self.thread.join()
+            if not self.sm:
+                return None
+            reasons = sorted(nm for nm, b in self.REASONS.items() if self.bits & b)
+            busy = [v for v in self.sm if v > 0.5 * self.mx] or self.sm
+            return {"sm_mhz": statistics.median(busy), "sm_max_mhz": self.mx, "reasons": reasons,
+                    "samples": len(self.sm), "source": "nvml, 5 ms"}
         if self.p is None:
             return None
         self.p.terminate()
@@ -122,7 +167,7 @@ class Clocks:
             return None
         busy = [v for v in sm if v > 0.5 * mx] or sm
         return {"sm_mhz": statistics.median(busy), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def build_problem(scale, seed=0):
@@ -216,9 +261,7 @@ def run_sgmas(args):
         if world > 1:
             torch.distributed.barrier()
         times, iters, launches = [], [], []
-        first = not any("ms" in r for r in results.values())
-        if first:
-            clocks.start()
+        clocks.start()
         for _ in range(args.steps):
             flush.zero_()                      # L2 flushed between timed steps
             e0 = torch.cuda.Event(enable_timing=True)
@@ -229,9 +272,8 @@ def run_sgmas(args):
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
             iters.append(rep["iterations"])
-            launches.append(rep["kernel_launches"])
-        if first:
-            ck = clocks.stop()
+            launches.append(rep["kernel_launches"] + rep["build_launches"])
+        ck = clocks.stop()
         torch.cuda.synchronize()
         # verify: true relative residual of the last solution
         y = torch.zeros_like(b)
@@ -245,12 +287,12 @@ def run_sgmas(args):
         results[v] = {"ms": ms, "ms_min": min(times), "ms_max": max(times), "iterations": int(statistics.median(iters)),
                       "rel_residual": res, "converged": bool(rep["converged"]),
                       "precond_build_ms": rep["precond_ms"], "pcg_loop_ms": rep["solve_ms"], "mode": mode,
-                      "kernel_launches": int(statistics.median(launches))}
-        if first:
-            gpu_launches = int(sum(launches))
-            clocks_rec = ck
+                      "kernel_launches": int(statistics.median(launches)), "launches_timed": int(sum(launches)),
+                      "clocks": ck}
     ok = [v for v in variants if "ms" in results.get(v, {}) and results[v]["converged"]]
     head = ok[0] if ok else next(v for v in variants if "ms" in results.get(v, {}))
+    gpu_launches = results[head]["launches_timed"]   # library kernels in the headline's timed steps
+    clocks_rec = results[head]["clocks"]
     # ---- per-kernel times and roofline of the headline variant ----
     ctx, pms = ctxs[head]
     hbase = head[:-6] if head.endswith("-graph") else head

@@ -65,7 +65,8 @@ typedef struct {
     double rr_last;      /* r.r at the last convergence test */
     float solve_ms;      /* device time of the PCG loop (CUDA events) */
     float precond_ms;    /* device time of the preconditioner build */
-    int kernel_launches; /* kernels this solve launched (graph nodes executed) */
+    int kernel_launches; /* kernels of the PCG loop (1 for the persistent form, graph nodes executed otherwise) */
+    int build_launches;  /* kernels of the solve's set-up: block CSR, MAS hierarchy, scatter, inverses */
 } sgmas_pcg_report;
 
 /* One BCOO matrix on the device (borrowed). */

@@ -350,6 +350,7 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
         SG_CUDA(c, cudaEventCreate(&c->ev2));
     }
     SG_CUDA(c, cudaEventRecord(c->ev2, c->stream));
+    c->build_launches = 0;
     int rc = pcg_prepare(c, A, rc_cfg);
     if (rc) return rc;
     if (rc_cfg.precond == 1) {
@@ -378,6 +379,7 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
         report->solve_ms = solve_ms;
         report->precond_ms = prep_ms;
         report->kernel_launches = launches;
+        report->build_launches = c->build_launches;
     }
     if (!(h.rz == h.rz) || !(h.rr == h.rr)) return ctx_fail(c, SGMAS_ERR_NUMERIC, "non-finite residual in PCG");
     return SGMAS_OK;

@@ -91,6 +91,7 @@ struct sgmas_context {
     const int* d_pairs = nullptr;
     int cp_num = 0;
     int mas_launches = 0;             // kernels per apply
+    int build_launches = 0;           // kernels launched by the set-up of the current solve
     int apply_parts = 7;              // which apply kernels to launch (profiling)
 
     // ---- PCG ----

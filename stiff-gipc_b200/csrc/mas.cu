@@ -819,6 +819,8 @@ int build_hierarchy_t(sgmas_context* c) {
         k_next_table<<<gN, kThreads, 0, s>>>(N, level, c->d_coarse_space, c->d_next_mask);
     }
     k_aggregate<<<gN, kThreads, 0, s>>>(N, L, c->d_going_next, c->gn_cap, c->d_coarse_table, c->d_err);
+    // kernels launched above: 4 at level 0 (+ contacts), 5 per coarser level (+ contacts), aggregate
+    c->build_launches += 5 + (L - 1) * 5 + L * (c->cp_num > 0 ? 1 : 0);
     SG_CUDA(c, cudaGetLastError());
     SG_CUDA(c, cudaMemcpyAsync(c->h_level_size, c->d_level_size, sizeof(int) * 2 * (kMaxLevels + 2),
                                cudaMemcpyDeviceToHost, s));
@@ -852,6 +854,7 @@ int scatter_invert_t(sgmas_context* c, const double* vals, const int* rows, cons
     auto kern = k_invert<B, S>;
     SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<(nblk + W - 1) / W, 32 * W, smem, s>>>(nblk, c->d_hess, (S*)c->d_inv, nullptr, c->d_level_size, c->L);
+    c->build_launches += (n > 0 ? 1 : 0) + 2;  // scatter1, scatter2, invert
     SG_CUDA(c, cudaGetLastError());
     return 0;
 }

@@ -434,6 +434,7 @@ int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* 
                                                              B.cols, B.src);
     k_bsr_values<<<(int)((B.cap + kT - 1) / kT), kT, 0, s>>>(B.cap, B.row_ptr, nrows, B.src, vals, B.vals);
     k_row_split<<<1, 1024, 0, s>>>(nrows, B.row_ptr, B.row_list, B.d_nlong);
+    c->build_launches += 4 + (nb > 0 ? 2 : 0);
     SG_CUDA(c, cudaGetLastError());
     // the long-row count sizes the SpMV grid (one 4-byte read per build)
     SG_CUDA(c, cudaMemcpyAsync(&B.n_long, B.d_nlong, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -480,6 +481,7 @@ static int jacobi_setup(sgmas_context* c, const double* vals, const int* rows, c
         k_abd_inverse<<<(abd_bodies + 63) / 64, 64, 0, s>>>(abd_bodies, nb, rows, cols, vals, c->bsr.first, c->bsr.cnt,
                                                             c->bsr.cnt_lower, c->d_abd_inv, c->d_err);
     }
+    c->build_launches += (nb > 0 ? 1 : 0) + (abd_bodies > 0 ? 1 : 0);
     SG_CUDA(c, cudaGetLastError());
     return 0;
 }

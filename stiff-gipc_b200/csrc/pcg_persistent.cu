@@ -59,7 +59,7 @@ struct PArgs {
     void* R;             // level-2 residual pushes (Acc, global node ids)
     int k0, k1, nb0, nb1;  // level-0 banks per CTA (max), level-1 banks per CTA, bank counts
     int nc;                // nodes of levels >= 2 (a multiple of B)
-    int cache_c, kd;       // levels >= 2 tiles cached in shared memory, else staged kd at a time
+    int capc;              // tiles of levels >= 2 a CTA holds in shared memory (<= kPT / B)
     // block-Jacobi
     const double* dinv;
     int abd_rows, precond;
@@ -221,11 +221,22 @@ __device__ __forceinline__ void smem_banks(const S* tiles, const Acc* rs, Acc* z
     }
 }
 
+// Ancestor banks of this CTA's vertices at levels >= 2: node ids of every
+// level are assigned in bank order, so each level's ancestors form one
+// contiguous range of banks.  anc_lo[l] = first global bank, anc_nb[l] =
+// banks at level l; the tiles of all of them, level after level, fill the
+// first anc_total tiles of tilesC when anc_total <= capc.
+struct Anc {
+    int lo[kMaxLevels + 2], nb[kMaxLevels + 2];
+    int total;
+};
+
 // levels >= 2, redundantly in every CTA: level-2 residuals from global memory,
-// levels >= 3 by group sums in shared memory, then the Schwarz products.
+// levels >= 3 by group sums in shared memory, then the Schwarz products of
+// this CTA's ancestor banks (cached tiles, or staged per level).
 template <int B, typename S, typename Acc>
-__device__ __forceinline__ bool levels_c(const PArgs& a, S* tilesC, Acc* Rc, Acc* Zc, const int* parc,
-                                         uint64_t* mbar, unsigned& mphase) {
+__device__ __forceinline__ bool levels_c(const PArgs& a, const Anc& anc, S* tilesC, Acc* Rc, Acc* Zc,
+                                         const int* parc, uint64_t* mbar, unsigned& mphase) {
     constexpr int bs = bsym_of(B);
     constexpr int HPW = 32 / B;
     const int base = a.lvl_begin[2];
@@ -255,22 +266,35 @@ __device__ __forceinline__ bool levels_c(const PArgs& a, S* tilesC, Acc* Rc, Acc
         }
         __syncthreads();
     }
-    const int nbc = a.nc / B;
-    if (a.cache_c) {
-        smem_banks<B, S, Acc>(tilesC, Rc, Zc, nbc);
-    } else {
-        const S* inv = (const S*)a.inv + (size_t)(base / B) * bs * 9;
-        for (int c0 = 0; c0 < nbc; c0 += a.kd) {
-            const int ncb = min(a.kd, nbc - c0);
-            __syncthreads();  // the previous chunk's tiles are no longer read
-            if (threadIdx.x == 0) {
-                const unsigned bytes = (unsigned)(ncb * bs * 9 * sizeof(S));
-                mbar_expect_tx(mbar, bytes);
-                bulk_g2s(tilesC, inv + (size_t)c0 * bs * 9, bytes, mbar);
+    const int bbase = base / B;  // global bank index of the first level-2 bank
+    if (anc.total <= a.capc) {   // one pass over all ancestor banks, tiles resident
+        const int hw = threadIdx.x / B;
+        if ((hw / HPW) * HPW < anc.total) {
+            const bool valid = hw < anc.total;
+            int l = 2, first = 0;  // level of entry hw
+            while (l + 1 < a.L && hw >= first + anc.nb[l]) { first += anc.nb[l]; ++l; }
+            const int i = valid ? (anc.lo[l] + hw - first - bbase) * B + lane : 0;
+            const Acc v0 = valid ? Rc[3 * i] : (Acc)0, v1 = valid ? Rc[3 * i + 1] : (Acc)0,
+                      v2 = valid ? Rc[3 * i + 2] : (Acc)0;
+            Acc z0, z1, z2;
+            schwarz_rows<B, S, Acc>(tilesC + (size_t)(valid ? hw : 0) * bs * 9, lane, v0, v1, v2, z0, z1, z2);
+            if (valid) { Zc[3 * i] = z0; Zc[3 * i + 1] = z1; Zc[3 * i + 2] = z2; }
+        }
+    } else {  // staged: each level's range in chunks of capc tiles
+        for (int l = 2; l < a.L; ++l) {
+            for (int c0 = 0; c0 < anc.nb[l]; c0 += a.capc) {
+                const int ncb = min(a.capc, anc.nb[l] - c0);
+                __syncthreads();  // the previous chunk's tiles are no longer read
+                if (threadIdx.x == 0) {
+                    const unsigned bytes = (unsigned)(ncb * bs * 9 * sizeof(S));
+                    mbar_expect_tx(mbar, bytes);
+                    bulk_g2s(tilesC, (const S*)a.inv + (size_t)(anc.lo[l] + c0) * bs * 9, bytes, mbar);
+                }
+                if (!mbar_wait(mbar, mphase, a.err)) return false;
+                mphase ^= 1u;
+                const int off = (anc.lo[l] + c0 - bbase) * B;
+                smem_banks<B, S, Acc>(tilesC, Rc + 3 * (size_t)off, Zc + 3 * (size_t)off, ncb);
             }
-            if (!mbar_wait(mbar, mphase, a.err)) return false;
-            mphase ^= 1u;
-            smem_banks<B, S, Acc>(tilesC, Rc + 3 * (size_t)c0 * B, Zc + 3 * (size_t)c0 * B, ncb);
         }
     }
     __syncthreads();
@@ -286,11 +310,13 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     constexpr int HPW = 32 / B;
     const size_t tb = (size_t)bs * 9;  // elements per tile
     const bool mas = a.precond == 1;
-    // shared memory: tiles0 [k0] | tiles1 [k1] | tilesC [nc/B or kd] | R1s, Z1s [k1 B 3] | Rc, Zc [nc 3] | parc [nc]
+    // shared memory: tiles0 [k0] | tiles1 [k1] | tilesC [capc] | R1s, Z1s [k1 B 3] | Rc, Zc [nc 3] | parc [nc]
     S* tiles0 = reinterpret_cast<S*>(smem_raw);
     S* tiles1 = tiles0 + (size_t)a.k0 * tb;
     S* tilesC = tiles1 + (size_t)a.k1 * tb;
-    Acc* R1s = reinterpret_cast<Acc*>(tilesC + (size_t)(a.cache_c ? a.nc / B : a.kd) * tb);
+    Acc* R1s = reinterpret_cast<Acc*>(tilesC + (size_t)a.capc * tb);
+    __shared__ Anc anc;
+    __shared__ int rng[2];
     Acc* Z1s = R1s + 3 * (size_t)a.k1 * B;
     Acc* Rc = Z1s + 3 * (size_t)a.k1 * B;
     Acc* Zc = Rc + 3 * (size_t)a.nc;
@@ -322,14 +348,50 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                     par = a.going_next[node] - a.lvl_begin[2];
             parc[i] = par;
         }
+        // ancestor bank ranges, level by level (parents of the previous range)
+        if (threadIdx.x == 0) {
+            anc.total = 0;
+            for (int l = 0; l < kMaxLevels + 2; ++l) { anc.lo[l] = 0; anc.nb[l] = 0; }
+        }
+        int lo_n = a.lvl_begin[1] + o.j0 * B, hi_n = min(a.lvl_begin[1] + (o.j0 + o.nbk1) * B,
+                                                         a.lvl_begin[1] + a.lvl_count[1]) - 1;
+        for (int l = 2; l < a.L && lo_n <= hi_n; ++l) {
+            if (threadIdx.x == 0) { rng[0] = 0x7fffffff; rng[1] = -1; }
+            __syncthreads();
+            int mn = 0x7fffffff, mx = -1;
+            for (int n = lo_n + (int)threadIdx.x; n <= hi_n; n += kPT) {
+                const int par = a.going_next[n];
+                mn = min(mn, par);
+                mx = max(mx, par);
+            }
+            if (mx >= 0) { atomicMin(&rng[0], mn); atomicMax(&rng[1], mx); }
+            __syncthreads();
+            lo_n = rng[0];
+            hi_n = rng[1];
+            if (threadIdx.x == 0 && lo_n <= hi_n) {
+                anc.lo[l] = lo_n / B;
+                anc.nb[l] = hi_n / B - lo_n / B + 1;
+                anc.total += anc.nb[l];
+            }
+            __syncthreads();
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
             const unsigned by0 = (unsigned)(o.nbk0 * tb * sizeof(S)), by1 = (unsigned)(o.nbk1 * tb * sizeof(S));
-            const unsigned byc = a.cache_c ? (unsigned)((a.nc / B) * tb * sizeof(S)) : 0u;
+            const bool cache_c = anc.total <= a.capc;
+            const unsigned byc = cache_c ? (unsigned)(anc.total * tb * sizeof(S)) : 0u;
             mbar_expect_tx(&mbar, by0 + by1 + byc);
             if (by0) bulk_g2s(tiles0, (const S*)a.inv + (size_t)o.lo * tb, by0, &mbar);
             if (by1) bulk_g2s(tiles1, (const S*)a.inv + (size_t)(b1 + o.j0) * tb, by1, &mbar);
-            if (byc) bulk_g2s(tilesC, (const S*)a.inv + (size_t)(a.lvl_begin[2] / B) * tb, byc, &mbar);
+            if (byc) {
+                int t = 0;
+                for (int l = 2; l < a.L; ++l) {
+                    if (anc.nb[l] == 0) continue;
+                    bulk_g2s(tilesC + (size_t)t * tb, (const S*)a.inv + (size_t)anc.lo[l] * tb,
+                             (unsigned)(anc.nb[l] * tb * sizeof(S)), &mbar);
+                    t += anc.nb[l];
+                }
+            }
         }
         if (hw < o.nbk0) v = a.part_map[(o.lo + hw) * B + lane];
         if (v >= 0) {
@@ -422,7 +484,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         if (ok) apply_b();
         if (a.L > 2) {
             ok = ok && grid_barrier(a.sync, epoch, a.err);
-            if (ok) ok = levels_c<B, S, Acc>(a, tilesC, Rc, Zc, parc, &mbar, mphase);
+            if (ok) ok = levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase);
         }
         if (ok) collect();
     } else {
@@ -441,7 +503,10 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     unsigned long long* acc = a.stamps ? a.stamps + 8 * (size_t)(a.stamp_iters + 2) + 16 * (size_t)blockIdx.x : nullptr;
     long long t_rel = clock64();
 #define SLOT(i) (acc ? acc + 2 * (i) : nullptr), &t_rel
-    const int warps = kPT / 32, gw0 = blockIdx.x * warps + threadIdx.x / 32;
+    // SpMV units round-robin over the grid's warps (a contiguous range per CTA
+    // measured no faster: long contact rows then pile up on a few CTAs)
+    constexpr int warps = kPT / 32;
+    const int gw0 = blockIdx.x * warps + threadIdx.x / 32;
     int passes = 0;
     while (!done) {
         ++passes;
@@ -487,7 +552,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             if (a.L > 2) {
                 if (!grid_barrier(a.sync, epoch, a.err, SLOT(3))) { ok = false; break; }
                 stamp(a, k, 3);
-                if (!levels_c<B, S, Acc>(a, tilesC, Rc, Zc, parc, &mbar, mphase)) ok = false;
+                if (!levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase)) ok = false;
             }
             collect();
         } else {
@@ -580,6 +645,7 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
             SG_CUDA(c, cudaMemsetAsync(c->d_psync + 4, 0, sizeof(unsigned), c->stream));
             k_cta_span<B><<<(G + 127) / 128, 128, 0, c->stream>>>(G, a.k1, a.nb1, a.lvl_count[1], c->d_l1_bank,
                                                                 c->d_psync + 4);
+            c->build_launches += 2;
             unsigned span = 0;
             SG_CUDA(c, cudaMemcpyAsync(&span, c->d_psync + 4, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
             SG_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -593,19 +659,16 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
         if (a.k0 > kPT / B || a.k1 > kPT / B) return 1;  // one slot per thread: use the graph form
         const size_t fixed = (size_t)(a.k0 + a.k1) * tb + 2 * 3 * (size_t)a.k1 * B * sizeof(Acc) +
                              2 * 3 * (size_t)a.nc * sizeof(Acc) + (size_t)a.nc * sizeof(int);
-        const int nbc = a.nc / B;
-        if (fixed + (size_t)nbc * tb <= budget) {
-            a.cache_c = 1;
-            a.kd = 0;
-            smem = fixed + (size_t)nbc * tb;
-        } else {
+        if (a.L > 2) {
             if (fixed + tb > budget) return 1;
-            a.cache_c = 0;
-            a.kd = (int)std::min<size_t>((size_t)std::max(nbc, 1), (budget - fixed) / tb);
-            smem = fixed + (size_t)a.kd * tb;
+            a.capc = (int)std::min<size_t>({(size_t)(a.nc / B), (size_t)(kPT / B), (budget - fixed) / tb});
+        } else {
+            if (fixed > budget) return 1;
+            a.capc = 0;
         }
+        smem = fixed + (size_t)a.capc * tb;
     } else {
-        a.k0 = a.k1 = a.nb0 = a.nb1 = a.nc = a.kd = a.cache_c = 0;
+        a.k0 = a.k1 = a.nb0 = a.nb1 = a.nc = a.capc = 0;
     }
     auto kern = k_pcg_persistent<B, S, Acc>;
     SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));

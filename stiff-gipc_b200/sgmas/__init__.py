@@ -40,7 +40,7 @@ class PcgConfig(C.Structure):
 class PcgReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("rz0", C.c_double), ("rr0", C.c_double),
                 ("rr_last", C.c_double), ("solve_ms", C.c_float), ("precond_ms", C.c_float),
-                ("kernel_launches", C.c_int)]
+                ("kernel_launches", C.c_int), ("build_launches", C.c_int)]
 
 
 class Bcoo(C.Structure):
