@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--impl", default="sgmas", choices=["sgmas", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = benchmark size)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--variants", default="bf16,fp32,fp64,jacobi,fp32-graph",
+    ap.add_argument("--variants", default="bf16,fp32,fp32f,fp64,jacobi,fp32-graph",
                     help="MAS storage precision (or jacobi); suffix -graph = kernel-per-phase CUDA graph "
                          "instead of the persistent cooperative kernel")
     ap.add_argument("--profile-reps", type=int, default=50,
@@ -185,7 +185,7 @@ def algorithmic_bytes(s, info, precision):
     collect: Z over L levels, slot + coarse tables, z written, r read."""
     n = 3 * s.n_verts
     nb = len(s.rows)
-    es = {"fp32": 4, "bf16": 2, "fp64": 8}[precision]
+    es = {"fp32": 4, "bf16": 2, "fp64": 8, "fp32f": 4}[precision]
     acc = 8 if precision == "fp64" else 4
     B = 16
     bs = B * (B + 1) // 2 * 9
@@ -244,7 +244,7 @@ def run_sgmas(args):
     gpu_launches = None
     for v in variants:
         base, mode = (v[:-6], "graph") if v.endswith("-graph") else (v, "persistent")
-        precision = base if base in ("fp32", "bf16", "fp64") else "fp32"
+        precision = base if base in ("fp32", "bf16", "fp64", "fp32f") else "fp32"
         precond = "jacobi" if base == "jacobi" else "mas"
         ctx, pms = make(precision)
         ctx.set_pcg_mode(mode)
@@ -296,7 +296,7 @@ def run_sgmas(args):
     # ---- per-kernel times and roofline of the headline variant ----
     ctx, pms = ctxs[head]
     hbase = head[:-6] if head.endswith("-graph") else head
-    precision = hbase if hbase in ("fp32", "bf16", "fp64") else "fp32"
+    precision = hbase if hbase in ("fp32", "bf16", "fp64", "fp32f") else "fp32"
     print(json.dumps({"progress": results}), file=sys.stderr, flush=True)
     # ---- e2e through the public API with host buffers ----
     try:
@@ -348,7 +348,7 @@ def run_sgmas(args):
     out = {"metric": METRIC, "value": round(results[head]["ms"], 4), "unit": "ms", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(results[head]["ms"], 4),
            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-           "dtype": {"bf16": "f64+bf16", "fp32": "f64+f32", "fp64": "f64", "jacobi": "f64"}[hbase],
+           "dtype": {"bf16": "f64+bf16", "fp32": "f64+f32", "fp32f": "f64+f32", "fp64": "f64", "jacobi": "f64"}[hbase],
            "data": "synthetic",
            "config": {"workload": WORKLOAD, "scale": args.scale, "rel_tol": REL_TOL,
                       "headline": f"{head} MAS-PCG ({results[head]['mode']})", "partition": "Morton order, 16-vertex subdomains",

@@ -36,8 +36,10 @@ typedef struct sgmas_context sgmas_context;
 
 /* precision of the stored subdomain inverses and of the MAS apply */
 #define SGMAS_MAS_FP32 0 /* reference parity: FP64 build, FP32 inverses and apply */
-#define SGMAS_MAS_BF16 1 /* BF16 inverses, FP32 accumulate */
+#define SGMAS_MAS_BF16 1 /* BF16 factored inverses (W = L^-1 of each subdomain's FP64 Cholesky
+                            factor, z = W^T W r), FP32 accumulate: SPD for any rounding of W */
 #define SGMAS_MAS_FP64 2 /* FP64 inverses and apply (plain FP64 MAS-PCG) */
+#define SGMAS_MAS_FP32_FACTORED 3 /* FP32 factored inverses, FP32 accumulate */
 
 typedef struct {
     int device;        /* CUDA device ordinal */

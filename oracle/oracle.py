@@ -69,6 +69,7 @@ def lib():
     L.or_mas_assemble.argtypes = [C.c_void_p, f64p, i32p, i32p, C.c_void_p, C.c_int, C.c_int, C.c_int]
     L.or_mas_get_matrices.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.or_mas_invert_blocks.argtypes = [f64p, C.c_int, C.c_int, f64p]
+    L.or_mas_factor_blocks.argtypes = [f64p, C.c_int, C.c_int, f64p]
     L.or_mas_set_hess.argtypes = [C.c_void_p, f64p, C.c_int]
     L.or_mas_apply.argtypes = [C.c_void_p, f64p, f64p]
     L.or_pcg.argtypes = [f64p, i32p, i32p, C.c_int, C.c_int, f64p, f64p, C.POINTER(PCGCfg),
@@ -245,6 +246,13 @@ class MAS:
 def invert_blocks(hess, nblocks, bank=16):
     out = np.zeros_like(cf64(hess))
     lib().or_mas_invert_blocks(cf64(hess), nblocks, bank, out)
+    return out
+
+
+def factor_blocks(hess, nblocks, bank=16):
+    """W = L^-1 per subdomain matrix, in the tile slots (the library's factored storage)."""
+    out = np.zeros_like(cf64(hess))
+    lib().or_mas_factor_blocks(cf64(hess), nblocks, bank, out)
     return out
 
 

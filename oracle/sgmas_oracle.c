@@ -824,11 +824,88 @@ static void gj_invert(const double* packed, int b, double* out_packed)
     free(col);
 }
 
+/* Factored inverse (the library's storage for its BF16 and FP32-factored
+ * MAS, not a reference kernel): lower Cholesky M = L L^T (right-looking, a
+ * pivot that is not positive becomes 1, zero diagonal -> 1 as the reference's
+ * inverse), then W = L^-1 column by column; slot (rb, cb), rb <= cb, of the
+ * output holds block (cb, rb) of W, column-major.  M^-1 = W^T W.  Operation
+ * order per element as the device kernel k_chol_inv. */
+static void chol_factor(const double* packed, int b, double* out_packed)
+{
+    const int n = 3 * b;
+    double* A  = (double*)calloc((size_t)n * n, sizeof(double));
+    double* dW = (double*)malloc(sizeof(double) * (size_t)n);
+    for(int i = 0; i < n; i++)
+        for(int j = 0; j <= i; j++)
+        {
+            int rb = j / 3, cb = i / 3;
+            double v = rb == cb ? packed[sym_index(b, rb, rb) * 9 + (i % 3) + 3 * (j % 3)]
+                                : packed[sym_index(b, rb, cb) * 9 + (j % 3) + 3 * (i % 3)];
+            if(i == j && v == 0)
+                v = 1;
+            A[(size_t)i * n + j] = v;
+        }
+    for(int k = 0; k < n; k++)
+    {
+        double d = A[(size_t)k * n + k];
+        if(!(d > 0.0))
+            d = 1.0;
+        const double lkk = sqrt(d);
+        for(int i = k + 1; i < n; i++)
+            A[(size_t)i * n + k] = A[(size_t)i * n + k] / lkk;
+        A[(size_t)k * n + k] = lkk;
+        for(int i = k + 1; i < n; i++)
+        {
+            const double lik = A[(size_t)i * n + k];
+            for(int j = k + 1; j <= i; j++)
+                A[(size_t)i * n + j] = fma(-lik, A[(size_t)j * n + k], A[(size_t)i * n + j]);
+        }
+    }
+    for(int j = 0; j < n; j++)
+        dW[j] = 1.0 / A[(size_t)j * n + j];
+    for(int j = 0; j < n; j++)
+        for(int i = j + 1; i < n; i++)
+        {
+            double sum = 0.0;
+            for(int k = j; k < i; k++)
+                sum = fma(A[(size_t)i * n + k], k == j ? dW[j] : A[(size_t)j * n + k], sum);
+            A[(size_t)j * n + i] = -sum / A[(size_t)i * n + i];
+        }
+    for(int rb = 0; rb < b; rb++)
+        for(int cb = rb; cb < b; cb++)
+            for(int q = 0; q < 9; q++)
+            {
+                int i = 3 * cb + q % 3, j = 3 * rb + q / 3;
+                double v = i > j ? A[(size_t)j * n + i] : (i == j ? dW[i] : 0.0);
+                out_packed[sym_index(b, rb, cb) * 9 + q] = v;
+            }
+    free(A);
+    free(dW);
+}
+
+static int is_factored(int precision) { return precision == 1 || precision == 3; }
+
+static void invert_one(const double* packed, int b, double* out_packed, int precision)
+{
+    if(is_factored(precision))
+        chol_factor(packed, b, out_packed);
+    else
+        gj_invert(packed, b, out_packed);
+}
+
 void or_mas_invert_blocks(const double* in, int nblocks, int bank, double* out64)
 {
     int bsym = bank * (bank + 1) / 2;
     for(int k = 0; k < nblocks; k++)
         gj_invert(in + (size_t)k * bsym * 9, bank, out64 + (size_t)k * bsym * 9);
+}
+
+int or_mas_factor_blocks(const double* in, int nblocks, int bank, double* out64)
+{
+    int bsym = bank * (bank + 1) / 2;
+    for(int k = 0; k < nblocks; k++)
+        chol_factor(in + (size_t)k * bsym * 9, bank, out64 + (size_t)k * bsym * 9);
+    return 0;
 }
 
 static float bf16_round_f(float f)
@@ -973,7 +1050,7 @@ int or_mas_assemble(or_mas* m, const double* vals, const int* rows, const int* c
     /* inverse, then storage precision */
 #pragma omp parallel for schedule(dynamic, 4)
     for(int k = 0; k < m->nblk; k++)
-        gj_invert(m->hess + (size_t)k * m->bsym * 9, b, m->inv64 + (size_t)k * m->bsym * 9);
+        invert_one(m->hess + (size_t)k * m->bsym * 9, b, m->inv64 + (size_t)k * m->bsym * 9, precision);
     for(size_t i = 0; i < nval; i++)
     {
         float f     = (float)m->inv64[i];
@@ -992,8 +1069,9 @@ int or_mas_set_hess(or_mas* m, const double* hess, int precision)
     size_t nval  = (size_t)m->nblk * m->bsym * 9;
     m->precision = precision;
     memcpy(m->hess, hess, nval * sizeof(double));
+#pragma omp parallel for schedule(dynamic, 4)
     for(int k = 0; k < m->nblk; k++)
-        gj_invert(m->hess + (size_t)k * m->bsym * 9, m->bank, m->inv64 + (size_t)k * m->bsym * 9);
+        invert_one(m->hess + (size_t)k * m->bsym * 9, m->bank, m->inv64 + (size_t)k * m->bsym * 9, precision);
     for(size_t i = 0; i < nval; i++)
     {
         float f     = (float)m->inv64[i];
@@ -1099,6 +1177,43 @@ int or_mas_apply(or_mas* m, const double* r, double* z)
     }
     /* Schwarz: per bank z = P r, columns ascending, fma chains */
     const size_t bsym = (size_t)m->bsym;
+    if(is_factored(m->precision))
+    {
+        /* factored tiles: y = W r (J <= I), z = W^T y (J >= I), J ascending */
+#pragma omp parallel for schedule(static)
+        for(int B = 0; B < T / b; B++)
+        {
+            float y[32][3];
+            for(int rl = 0; rl < b; rl++)
+            {
+                float a[3] = {0, 0, 0};
+                for(int cl = 0; cl <= rl; cl++)
+                {
+                    const float* P = m->inv32 + ((size_t)B * bsym + sym_index(b, cl, rl)) * 9;
+                    const float* x = R32 + 3 * (size_t)(B * b + cl);
+                    for(int d = 0; d < 3; d++)
+                        for(int k = 0; k < 3; k++)
+                            a[d] = fmaf(P[d + 3 * k], x[k], a[d]);
+                }
+                for(int d = 0; d < 3; d++)
+                    y[rl][d] = a[d];
+            }
+            for(int rl = 0; rl < b; rl++)
+            {
+                float a[3] = {0, 0, 0};
+                for(int cl = rl; cl < b; cl++)
+                {
+                    const float* P = m->inv32 + ((size_t)B * bsym + sym_index(b, rl, cl)) * 9;
+                    for(int d = 0; d < 3; d++)
+                        for(int k = 0; k < 3; k++)
+                            a[d] = fmaf(P[k + 3 * d], y[cl][k], a[d]);
+                }
+                for(int d = 0; d < 3; d++)
+                    Z32[3 * ((size_t)B * b + rl) + d] = a[d];
+            }
+        }
+    }
+    else
 #pragma omp parallel for schedule(static)
     for(int B = 0; B < T / b; B++)
         for(int rl = 0; rl < b; rl++)

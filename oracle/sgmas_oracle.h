@@ -68,6 +68,8 @@ int or_mas_get_matrices(const or_mas* m, double* hess64, double* inv64,
                         float* inv32);
 int or_mas_set_hess(or_mas* m, const double* hess, int precision);
 void or_mas_invert_blocks(const double* in, int nblocks, int bank, double* out64);
+/* factored inverse W = L^-1 per subdomain (the library's BF16 / FP32-factored storage) */
+int or_mas_factor_blocks(const double* in, int nblocks, int bank, double* out64);
 int or_mas_apply(or_mas* m, const double* r, double* z);
 
 /* ---- PCG: SG/linear_system/solver/pcg_solver.cu:155-304 ---- */

@@ -38,7 +38,9 @@ int num_levels(int max_nodes, int bank) {
     return n > kMaxLevels ? kMaxLevels : n;
 }
 
-size_t store_size(int precision) { return precision == SGMAS_MAS_FP32 ? 4 : precision == SGMAS_MAS_BF16 ? 2 : 8; }
+size_t store_size(int precision) {
+    return precision == SGMAS_MAS_BF16 ? 2 : precision == SGMAS_MAS_FP64 ? 8 : 4;
+}
 size_t acc_size(int precision) { return precision == SGMAS_MAS_FP64 ? 8 : 4; }
 
 int check_device_error(sgmas_context* c, const char* where) {
@@ -97,7 +99,7 @@ int sgmas_create(const sgmas_config* cfg, sgmas_context** out) {
     sgmas_config def = {0, 16, SGMAS_MAS_FP32};
     if (!cfg) cfg = &def;
     if (cfg->bank_size != 16 && cfg->bank_size != 32) return SGMAS_ERR_ARG;
-    if (cfg->mas_precision < 0 || cfg->mas_precision > 2) return SGMAS_ERR_ARG;
+    if (cfg->mas_precision < 0 || cfg->mas_precision > 3) return SGMAS_ERR_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return SGMAS_ERR_CUDA;
     if (cfg->device < 0 || cfg->device >= ndev) return SGMAS_ERR_ARG;

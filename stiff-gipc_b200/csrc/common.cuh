@@ -83,6 +83,19 @@ template <> struct Store<double> {
     __device__ __forceinline__ static double from_double(double v) { return v; }
 };
 
+// Storage tag of the factored subdomain inverse: the tile holds W = L^-1 of
+// the subdomain's Cholesky factor (M^-1 = W^T W, SPD for any rounding of W)
+// in T; same tile size and slots as the explicit symmetric inverse.
+template <typename T> struct Fact {
+    T v;
+};
+template <typename T> struct Store<Fact<T>> {
+    __device__ __forceinline__ static float to_acc(Fact<T> x) { return Store<T>::to_acc(x.v); }
+    __device__ __forceinline__ static Fact<T> from_double(double v) { return Fact<T>{Store<T>::from_double(v)}; }
+};
+template <typename S> struct is_fact { static constexpr bool value = false; };
+template <typename T> struct is_fact<Fact<T>> { static constexpr bool value = true; };
+
 __device__ __forceinline__ float fma_acc(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_acc(double a, double b, double c) { return __fma_rn(a, b, c); }
 

@@ -525,6 +525,73 @@ __global__ void __launch_bounds__(32 * inv_warps<B>()) k_invert(int nblk, const 
     }
 }
 
+// Factored inverse of one subdomain matrix per warp (storage Fact<T>): lower
+// Cholesky M = L L^T in FP64 (right-looking; a pivot that is not positive
+// becomes 1), then W = L^-1 column by column (one lane per column); the tile
+// slot (rb, cb), rb <= cb, receives block (cb, rb) of W.  Every element's
+// operations run in one fixed order (fma for each update), restated by the
+// oracle.  The padding rows of a bank (zero diagonal) become identity, as
+// the reference's inverse does (:628-724).
+template <int B, typename S>
+__global__ void __launch_bounds__(32 * inv_warps<B>()) k_chol_inv(int nblk, const double* __restrict__ hess, S* inv,
+                                                                 double* inv64, const int* __restrict__ level_size,
+                                                                 int L) {
+    constexpr int n = 3 * B;
+    constexpr int bs = bsym_of(B);
+    extern __shared__ double smem_inv[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mat = blockIdx.x * inv_warps<B>() + w;
+    const int limit = level_size ? level_size[2 * L + 1] / B : nblk;
+    if (mat >= nblk || mat >= limit) return;
+    double* A = smem_inv + (size_t)w * (n * n + n);  // row-major; L in the lower triangle, W^T in the upper
+    double* dW = A + n * n;                         // diagonal of W
+    const double* P = hess + (size_t)mat * bs * 9;
+    for (int e = lane; e < n * n; e += 32) {  // lower triangle of M
+        const int i = e / n, j = e % n;
+        if (j > i) continue;
+        const int rb = j / 3, cb = i / 3;
+        double v = rb == cb ? P[sym_index(B, rb, rb) * 9 + (i % 3) + 3 * (j % 3)]
+                            : P[sym_index(B, rb, cb) * 9 + (j % 3) + 3 * (i % 3)];
+        if (i == j && v == 0.0) v = 1.0;
+        A[e] = v;
+    }
+    __syncwarp();
+    for (int k = 0; k < n; ++k) {
+        double d = A[k * n + k];
+        if (!(d > 0.0)) d = 1.0;
+        const double lkk = sqrt(d);
+        for (int i = k + 1 + lane; i < n; i += 32) A[i * n + k] = A[i * n + k] / lkk;
+        __syncwarp();
+        if (lane == 0) A[k * n + k] = lkk;
+        for (int i = k + 1 + lane; i < n; i += 32) {
+            const double lik = A[i * n + k];
+            for (int j = k + 1; j <= i; ++j) A[i * n + j] = __fma_rn(-lik, A[j * n + k], A[i * n + j]);
+        }
+        __syncwarp();
+    }
+    for (int j = lane; j < n; j += 32) dW[j] = 1.0 / A[j * n + j];
+    __syncwarp();
+    for (int j = lane; j < n; j += 32) {
+        for (int i = j + 1; i < n; ++i) {
+            double sum = 0.0;
+            for (int k = j; k < i; ++k) sum = __fma_rn(A[i * n + k], k == j ? dW[j] : A[j * n + k], sum);
+            A[j * n + i] = -sum / A[i * n + i];
+        }
+    }
+    __syncwarp();
+    S* out = inv + (size_t)mat * bs * 9;
+    for (int e = lane; e < bs * 9; e += 32) {
+        const int b = e / 9, q = e % 9;
+        int rb = 0, off = 0;
+        while (off + (B - rb) <= b) { off += B - rb; ++rb; }
+        const int cb = rb + (b - off);
+        const int i = 3 * cb + q % 3, j = 3 * rb + q / 3;  // element (i, j) of W
+        const double v = i > j ? A[j * n + i] : (i == j ? dW[i] : 0.0);
+        out[e] = Store<S>::from_double(v);
+        if (inv64) inv64[(size_t)mat * bs * 9 + e] = v;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Apply (preconditioning, :2210-2251)
 // ---------------------------------------------------------------------------
@@ -851,7 +918,7 @@ int scatter_invert_t(sgmas_context* c, const double* vals, const int* rows, cons
     }
     constexpr int W = inv_warps<B>();
     const size_t smem = (size_t)W * (9 * B * B + 3 * B) * sizeof(double);
-    auto kern = k_invert<B, S>;
+    auto kern = is_fact<S>::value ? k_chol_inv<B, S> : k_invert<B, S>;
     SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<(nblk + W - 1) / W, 32 * W, smem, s>>>(nblk, c->d_hess, (S*)c->d_inv, nullptr, c->d_level_size, c->L);
     c->build_launches += (n > 0 ? 1 : 0) + 2;  // scatter1, scatter2, invert
@@ -909,7 +976,9 @@ int mas_scatter_and_invert(sgmas_context* c, const double* vals, const int* rows
     switch (c->precision) {                                                                              \
         case SGMAS_MAS_FP32: return scatter_invert_t<B, float, float>(c, vals, rows, cols, indices, offset, n); \
         case SGMAS_MAS_BF16:                                                                             \
-            return scatter_invert_t<B, __nv_bfloat16, float>(c, vals, rows, cols, indices, offset, n);   \
+            return scatter_invert_t<B, Fact<__nv_bfloat16>, float>(c, vals, rows, cols, indices, offset, n); \
+        case SGMAS_MAS_FP32_FACTORED:                                                                    \
+            return scatter_invert_t<B, Fact<float>, float>(c, vals, rows, cols, indices, offset, n);     \
         default: return scatter_invert_t<B, double, double>(c, vals, rows, cols, indices, offset, n);   \
     }
     if (c->bank == 16) { SG_DISPATCH(16) }
@@ -926,8 +995,11 @@ int mas_launch_apply(sgmas_context* c, const double* r, double* z, int mode, con
             return apply_t<B, float, float>(c, r, z, mode, st, x, p, Ap, partials, ticket, iter_kind, cond_handle, \
                                             launches);                                                          \
         case SGMAS_MAS_BF16:                                                                                    \
-            return apply_t<B, __nv_bfloat16, float>(c, r, z, mode, st, x, p, Ap, partials, ticket, iter_kind,   \
-                                                    cond_handle, launches);                                     \
+            return apply_t<B, Fact<__nv_bfloat16>, float>(c, r, z, mode, st, x, p, Ap, partials, ticket,        \
+                                                          iter_kind, cond_handle, launches);                    \
+        case SGMAS_MAS_FP32_FACTORED:                                                                           \
+            return apply_t<B, Fact<float>, float>(c, r, z, mode, st, x, p, Ap, partials, ticket, iter_kind,     \
+                                                  cond_handle, launches);                                       \
         default:                                                                                                \
             return apply_t<B, double, double>(c, r, z, mode, st, x, p, Ap, partials, ticket, iter_kind,         \
                                               cond_handle, launches);                                           \
@@ -942,14 +1014,17 @@ int mas_invert_blocks_dev(sgmas_context* c, const double* hess, int nblk, double
     float* tmp = nullptr;
     const size_t bs = (size_t)c->bank * (c->bank + 1) / 2;
     SG_CUDA(c, cudaMallocAsync((void**)&tmp, sizeof(float) * nblk * bs * 9, s));
+    const bool fact = c->precision == SGMAS_MAS_BF16 || c->precision == SGMAS_MAS_FP32_FACTORED;
     if (c->bank == 16) {
         const size_t smem = (size_t)inv_warps<16>() * (9 * 16 * 16 + 48) * sizeof(double);
-        SG_CUDA(c, cudaFuncSetAttribute(k_invert<16, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_invert<16, float><<<(nblk + 3) / 4, 128, smem, s>>>(nblk, hess, tmp, out64, nullptr, 0);
+        auto kern = fact ? k_chol_inv<16, float> : k_invert<16, float>;
+        SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<(nblk + 3) / 4, 128, smem, s>>>(nblk, hess, tmp, out64, nullptr, 0);
     } else {
         const size_t smem = (size_t)(9 * 32 * 32 + 96) * sizeof(double);
-        SG_CUDA(c, cudaFuncSetAttribute(k_invert<32, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_invert<32, float><<<nblk, 32, smem, s>>>(nblk, hess, tmp, out64, nullptr, 0);
+        auto kern = fact ? k_chol_inv<32, float> : k_invert<32, float>;
+        SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<nblk, 32, smem, s>>>(nblk, hess, tmp, out64, nullptr, 0);
     }
     SG_CUDA(c, cudaGetLastError());
     SG_CUDA(c, cudaFreeAsync(tmp, s));

@@ -730,14 +730,15 @@ int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRu
         a.inv = c->d_inv; a.R = c->d_R;
     }
     int rc;
-    if (c->bank == 16) {
-        rc = c->precision == SGMAS_MAS_FP32   ? launch_t<16, float, float>(c, a, solve_ms)
-             : c->precision == SGMAS_MAS_BF16 ? launch_t<16, __nv_bfloat16, float>(c, a, solve_ms)
-                                              : launch_t<16, double, double>(c, a, solve_ms);
-    } else {
-        rc = c->precision == SGMAS_MAS_FP32   ? launch_t<32, float, float>(c, a, solve_ms)
-             : c->precision == SGMAS_MAS_BF16 ? launch_t<32, __nv_bfloat16, float>(c, a, solve_ms)
-                                              : launch_t<32, double, double>(c, a, solve_ms);
+    switch ((c->bank == 16 ? 0 : 4) + c->precision) {
+        case 0 + SGMAS_MAS_FP32: rc = launch_t<16, float, float>(c, a, solve_ms); break;
+        case 0 + SGMAS_MAS_BF16: rc = launch_t<16, Fact<__nv_bfloat16>, float>(c, a, solve_ms); break;
+        case 0 + SGMAS_MAS_FP64: rc = launch_t<16, double, double>(c, a, solve_ms); break;
+        case 0 + SGMAS_MAS_FP32_FACTORED: rc = launch_t<16, Fact<float>, float>(c, a, solve_ms); break;
+        case 4 + SGMAS_MAS_FP32: rc = launch_t<32, float, float>(c, a, solve_ms); break;
+        case 4 + SGMAS_MAS_BF16: rc = launch_t<32, Fact<__nv_bfloat16>, float>(c, a, solve_ms); break;
+        case 4 + SGMAS_MAS_FP64: rc = launch_t<32, double, double>(c, a, solve_ms); break;
+        default: rc = launch_t<32, Fact<float>, float>(c, a, solve_ms); break;
     }
     if (rc) return rc;
     if (launches) *launches = 1;

@@ -17,8 +17,9 @@ from . import build as _build
 LIB_PATH = _build.LIB_PATH
 _lib = None
 
-SGMAS_MAS_FP32, SGMAS_MAS_BF16, SGMAS_MAS_FP64 = 0, 1, 2
-PRECISION = {"fp32": 0, "bf16": 1, "fp64": 2}
+SGMAS_MAS_FP32, SGMAS_MAS_BF16, SGMAS_MAS_FP64, SGMAS_MAS_FP32_FACTORED = 0, 1, 2, 3
+# fp32: explicit inverses as the reference; bf16 / fp32f: factored inverses W = L^-1
+PRECISION = {"fp32": 0, "bf16": 1, "fp64": 2, "fp32f": 3}
 
 
 class SgmasError(RuntimeError):

@@ -104,10 +104,64 @@ def test_scatter_and_inverse(sgm, name):
     ctx.close()
 
 
-PREC = {"fp32": 0, "bf16": 1, "fp64": 2}
+@pytest.mark.parametrize("name", ["c1", "c2s"])
+@pytest.mark.parametrize("precision", ["bf16", "fp32f"])
+def test_factored_inverse(sgm, name, precision):
+    """Factored storage W = L^-1: the device's FP64 factor equals the
+    oracle's bit for bit on the same matrices, the stored tiles are its
+    rounding (BF16 via FP32, or FP32), and W^T W inverts each subdomain."""
+    case = cases.build(name)
+    ctx = make_ctx(sgm, case, precision)
+    d = upload(case)
+    ctx.mas_set_contacts(d["pairs"], len(case.s.pairs))
+    ctx.mas_assemble(d["vals"], d["rows"], d["cols"])
+    torch.cuda.synchronize()
+    hess_g, inv_g = ctx.mas_matrices()
+    nblk = ctx.mas_info()["n_mas_blocks"]
+    w64_g = ctx.mas_invert_host(hess_g, nblk)   # factored contexts return W in FP64
+    w64_o = O.factor_blocks(hess_g, nblk)
+    np.testing.assert_array_equal(w64_g.view(np.uint64), w64_o.view(np.uint64))
+    r32 = w64_o.astype(np.float32)
+    if precision == "bf16":
+        r32 = O.bf16_round(w64_o)
+    np.testing.assert_array_equal(inv_g.astype(np.float32).view(np.uint32), r32.astype(np.float32).view(np.uint32))
+    # W^T W M = I on a few well-conditioned level-0 subdomains
+    B = 16
+    for k in range(0, min(nblk, 40), 7):
+        M = O_dense(hess_g, k, B, lower_from_upper=True)
+        W = O_dense(w64_o, k, B, lower_from_upper=False)
+        pad = np.all(M == 0, axis=0)
+        M[pad, pad] = 1.0
+        E = W.T @ W @ M - np.eye(3 * B)
+        assert np.abs(E).max() <= max(1e-9, np.linalg.cond(M) * 1e-13), (k, np.abs(E).max())
+    ctx.close()
 
 
-@pytest.mark.parametrize("precision", ["fp32", "bf16", "fp64"])
+def O_dense(packed, k, B, lower_from_upper):
+    """Dense 3B x 3B matrix of tile k: the symmetric matrix (upper slots hold
+    M blocks) or the lower-triangular W (slot (rb, cb) holds W block (cb, rb))."""
+    bs = B * (B + 1) // 2
+    T = packed[k * bs * 9:(k + 1) * bs * 9].reshape(bs, 3, 3).transpose(0, 2, 1)  # column-major blocks
+    n = 3 * B
+    D = np.zeros((n, n))
+    s = 0
+    for rb in range(B):
+        for cb in range(rb, B):
+            blk = T[s]
+            s += 1
+            if lower_from_upper:
+                D[3 * rb:3 * rb + 3, 3 * cb:3 * cb + 3] = blk
+                if cb != rb:
+                    D[3 * cb:3 * cb + 3, 3 * rb:3 * rb + 3] = blk.T
+            else:
+                D[3 * cb:3 * cb + 3, 3 * rb:3 * rb + 3] = blk
+    return D
+
+
+PREC = {"fp32": 0, "bf16": 1, "fp64": 2, "fp32f": 3}
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16", "fp64", "fp32f"])
 @pytest.mark.parametrize("name", ["c1", "c2s", "bar", "bunny2"])
 def test_apply(sgm, name, precision):
     """MAS apply on identical subdomain matrices (the oracle takes the

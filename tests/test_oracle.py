@@ -177,6 +177,48 @@ def test_gauss_jordan_inverse_of_spd_blocks():
                 idx += 1
 
 
+def test_factored_inverse_of_spd_blocks_with_padding():
+    """W = L^-1 (the library's factored storage): W^T W = A^-1, W lower
+    triangular; padding rows (zero diagonal) become identity rows."""
+    rng = np.random.default_rng(6)
+    bs = 136
+    M = rng.normal(size=(48, 48))
+    A = M @ M.T + 48 * np.eye(48)
+    A[42:, :] = 0.0  # two padding slots (vertices 14, 15)
+    A[:, 42:] = 0.0
+    packed = np.zeros((bs, 9))
+    idx = 0
+    for r in range(16):
+        for c in range(r, 16):
+            packed[idx] = A[3 * r:3 * r + 3, 3 * c:3 * c + 3].T.reshape(-1)
+            idx += 1
+    w = O.factor_blocks(packed.reshape(-1), 1).reshape(bs, 9)
+    W = np.zeros((48, 48))
+    idx = 0
+    for r in range(16):
+        for c in range(r, 16):
+            W[3 * c:3 * c + 3, 3 * r:3 * r + 3] = w[idx].reshape(3, 3).T  # slot (r, c) = block (c, r) of W
+            idx += 1
+    Ap = A.copy()
+    Ap[np.arange(42, 48), np.arange(42, 48)] = 1.0
+    assert np.allclose(np.triu(W, 1), 0.0)
+    np.testing.assert_allclose(W.T @ W, np.linalg.inv(Ap), rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(W[42:, 42:], np.eye(6), atol=0)
+
+
+@pytest.mark.parametrize("precision", [1, 3])
+def test_factored_mas_apply_is_symmetric_positive(precision):
+    """With factored tiles the MAS is W^T W per subdomain: symmetric (to FP32
+    accumulation) and positive even in BF16."""
+    case = cases.build("c1")
+    m = case.oracle_mas(pairs=False, precision=precision)
+    rng = np.random.default_rng(8)
+    u, v = rng.normal(size=(2, 3 * case.n))
+    Mu, Mv = m.apply(u), m.apply(v)
+    assert abs(u @ Mv - v @ Mu) <= 1e-5 * np.sqrt((u @ Mu) * (v @ Mv))
+    assert u @ Mu > 0 and v @ Mv > 0
+
+
 # ---------------------------------------------------------------- MAS + PCG
 @pytest.mark.parametrize("name", ["c1", "bar"])
 def test_mas_hierarchy_invariants(name):
