@@ -637,6 +637,7 @@ __global__ void __launch_bounds__(kL0Banks * B) k_apply_l0(int Mm, int L, const 
     if (st && st->done) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t bar;
+    __shared__ __align__(16) Acc xch[(kL0Banks * B / 32) * kXchPerWarp];
     constexpr int bs = bsym_of(B);
     S* tile = reinterpret_cast<S*>(smem_raw);
     const int bank0 = blockIdx.x * kL0Banks;
@@ -662,20 +663,17 @@ __global__ void __launch_bounds__(kL0Banks * B) k_apply_l0(int Mm, int L, const 
             rp[0] = rv0; rp[1] = rv1; rp[2] = rv2;
         }
     }
-    const Acc r0 = (Acc)rv0, r1 = (Acc)rv1, r2 = (Acc)rv2;
-    Acc s0 = 0, s1 = 0, s2 = 0;
-    #pragma unroll 4
-    for (int j = 0; j < B; ++j) {
-        const Acc y0 = shfl_acc(r0, j, B), y1 = shfl_acc(r1, j, B), y2 = shfl_acc(r2, j, B);
-        if (msk & (1u << j)) { s0 += y0; s1 += y1; s2 += y2; }
-    }
+    Acc* xb = bank_slot<B>(xch);
+    xch_put(xb, lane, (Acc)rv0, (Acc)rv1, (Acc)rv2);
+    Acc s0, s1, s2;
+    mask_sum<B, Acc>(msk, xb, s0, s1, s2);
     if (idx >= 0 && L > 1 && __popc(msk & lanemask_lt(lane)) == 0) {
         const int nx = going_next[idx];
         R[3 * (size_t)nx] = s0; R[3 * (size_t)nx + 1] = s1; R[3 * (size_t)nx + 2] = s2;
     }
     if (!ok) return;
     Acc z0, z1, z2;
-    schwarz_rows<B, S, Acc>(tile + (size_t)(threadIdx.x / B) * bs * 9, lane, r0, r1, r2, z0, z1, z2);
+    schwarz_rows<B, S, Acc>(tile + (size_t)(threadIdx.x / B) * bs * 9, lane, xb, z0, z1, z2);
     if (tdx < Mm) {
         Z[3 * (size_t)tdx] = z0; Z[3 * (size_t)tdx + 1] = z1; Z[3 * (size_t)tdx + 2] = z2;
     }
@@ -688,7 +686,8 @@ __global__ void __launch_bounds__(kL0Banks * B) k_apply_l0(int Mm, int L, const 
 template <int B, typename S, typename Acc, bool PUSH>
 __device__ __forceinline__ bool schwarz_banks(const S* __restrict__ inv, Acc* R, Acc* Z,
                                               const int* __restrict__ going_next, int node_end, int bank0, int nbk,
-                                              int chunk, S* tile, uint64_t* bar, unsigned& phase, int* err) {
+                                              int chunk, S* tile, uint64_t* bar, unsigned& phase, int* err,
+                                              Acc* xch) {
     constexpr int bs = bsym_of(B);
     const int per_pass = blockDim.x / B;
     const int lane = threadIdx.x % B;
@@ -708,15 +707,17 @@ __device__ __forceinline__ bool schwarz_banks(const S* __restrict__ inv, Acc* R,
             const Acc v0 = valid ? __ldcg(R + 3 * (size_t)node) : (Acc)0;
             const Acc v1 = valid ? __ldcg(R + 3 * (size_t)node + 1) : (Acc)0;
             const Acc v2 = valid ? __ldcg(R + 3 * (size_t)node + 2) : (Acc)0;
+            Acc* xb = bank_slot<B>(xch);
+            xch_put(xb, lane, v0, v1, v2);
             if (PUSH) {
                 const int par = (valid && node < node_end) ? going_next[node] : -1;
                 Acc s0, s1, s2;
                 bool lead;
-                group_sum<B, Acc>(par, v0, v1, v2, lane, s0, s1, s2, lead);
+                group_sum<B, Acc>(par, xb, lane, s0, s1, s2, lead);
                 if (lead) { R[3 * (size_t)par] = s0; R[3 * (size_t)par + 1] = s1; R[3 * (size_t)par + 2] = s2; }
             }
             Acc z0, z1, z2;
-            schwarz_rows<B, S, Acc>(tile + (size_t)(valid ? q : 0) * bs * 9, lane, v0, v1, v2, z0, z1, z2);
+            schwarz_rows<B, S, Acc>(tile + (size_t)(valid ? q : 0) * bs * 9, lane, xb, z0, z1, z2);
             if (valid) { Z[3 * (size_t)node] = z0; Z[3 * (size_t)node + 1] = z1; Z[3 * (size_t)node + 2] = z2; }
         }
     }
@@ -737,6 +738,7 @@ __global__ void __launch_bounds__(kCoarseThreads) k_apply_coarse(int L, const in
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t bar;
     __shared__ bool am_last;
+    __shared__ __align__(16) Acc xch[(kCoarseThreads / 32) * kXchPerWarp];
     constexpr int bs = bsym_of(B);
     constexpr int BPC = coarse_bpc<B>();
     S* tile = reinterpret_cast<S*>(smem_raw);
@@ -753,10 +755,10 @@ __global__ void __launch_bounds__(kCoarseThreads) k_apply_coarse(int L, const in
     bool ok;
     if (L > 2)
         ok = schwarz_banks<B, S, Acc, true>(inv, R, Z, going_next, beg1 + cnt1, bank0, min(BPC, b2 - bank0), chunk,
-                                            tile, &bar, phase, err);
+                                            tile, &bar, phase, err, xch);
     else
         ok = schwarz_banks<B, S, Acc, false>(inv, R, Z, going_next, 0, bank0, min(BPC, b2 - bank0), chunk, tile,
-                                             &bar, phase, err);
+                                             &bar, phase, err, xch);
     if (!ok || L <= 2) return;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -781,14 +783,17 @@ __global__ void __launch_bounds__(kCoarseThreads) k_apply_coarse(int L, const in
             const Acc v1 = valid ? __ldcg(R + 3 * (size_t)node + 1) : (Acc)0;
             const Acc v2 = valid ? __ldcg(R + 3 * (size_t)node + 2) : (Acc)0;
             const int par = valid ? going_next[node] : -1;
+            Acc* xb = bank_slot<B>(xch);
+            xch_put(xb, lane, v0, v1, v2);
             Acc s0, s1, s2;
             bool lead;
-            group_sum<B, Acc>(par, v0, v1, v2, lane, s0, s1, s2, lead);
+            group_sum<B, Acc>(par, xb, lane, s0, s1, s2, lead);
             if (lead) { R[3 * (size_t)par] = s0; R[3 * (size_t)par + 1] = s1; R[3 * (size_t)par + 2] = s2; }
         }
         __syncthreads();
     }
-    schwarz_banks<B, S, Acc, false>(inv, R, Z, going_next, 0, b2, total / B - b2, chunk, tile, &bar, phase, err);
+    schwarz_banks<B, S, Acc, false>(inv, R, Z, going_next, 0, b2, total / B - b2, chunk, tile, &bar, phase, err,
+                                    xch);
     if (threadIdx.x == 0) *ticket = 0u;
 }
 

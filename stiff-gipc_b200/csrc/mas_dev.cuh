@@ -13,94 +13,172 @@ __host__ __device__ __forceinline__ int round_up(int v, int b) { return (v + b -
 template <typename Acc>
 __device__ __forceinline__ Acc shfl_acc(Acc v, int src, int width) { return __shfl_sync(0xffffffffu, v, src, width); }
 
+// ---- bank value exchange ---------------------------------------------------
+// A bank's per-lane 3-vectors are exchanged through shared memory: each warp
+// owns kXchPerWarp values (16-byte aligned), one slot of 3 B values per bank
+// it works on (32 / B banks).  A lane stores its three values; reading four
+// columns (12 values) then takes three (FP32) or six (FP64) 16-byte loads
+// where register shuffles would take twelve.
+constexpr int kXchPerWarp = 96;
+
+// this thread's bank slot inside its warp's exchange area
+template <int B, typename Acc>
+__device__ __forceinline__ Acc* bank_slot(Acc* xch_block) {
+    return xch_block + (threadIdx.x >> 5) * kXchPerWarp + ((threadIdx.x & 31) / B) * (3 * B);
+}
+
+template <typename Acc>
+__device__ __forceinline__ void xch_put(Acc* xb, int lane, Acc a, Acc b, Acc c) {
+    __syncwarp();  // earlier readers of the slot are done
+    xb[3 * lane] = a;
+    xb[3 * lane + 1] = b;
+    xb[3 * lane + 2] = c;
+    __syncwarp();
+}
+
+__device__ __forceinline__ void xch_get4(const float* xb, int c0, float (&v)[12]) {
+    const float4* q = reinterpret_cast<const float4*>(xb + 3 * c0);
+    const float4 a = q[0], b = q[1], c = q[2];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    v[8] = c.x; v[9] = c.y; v[10] = c.z; v[11] = c.w;
+}
+__device__ __forceinline__ void xch_get4(const double* xb, int c0, double (&v)[12]) {
+    const double2* q = reinterpret_cast<const double2*>(xb + 3 * c0);
+    #pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const double2 t = q[i];
+        v[2 * i] = t.x;
+        v[2 * i + 1] = t.y;
+    }
+}
+
 // Factored tile (Fact<T>): slot sym_index(J, I), J <= I, holds the 3x3
 // block (I, J) of W = L^-1, column-major.  z = W^T (W r): pass 1 y_I =
 // sum_{J <= I} W_IJ r_J, pass 2 z_I = sum_{J >= I} W_JI^T y_J, J ascending,
-// each component an fma chain (the order the oracle restates).
+// each component an fma chain (the order the oracle restates).  xb holds r
+// on entry and y on return.
 template <int B, typename S, typename Acc>
-__device__ __forceinline__ void schwarz_factored(const S* tile, int lane, Acc r0, Acc r1, Acc r2, Acc& z0, Acc& z1,
-                                                 Acc& z2) {
+__device__ __forceinline__ void schwarz_factored(const S* tile, int lane, Acc* xb, Acc& z0, Acc& z1, Acc& z2) {
     Acc y0 = 0, y1 = 0, y2 = 0;
-    #pragma unroll 4
-    for (int c = 0; c < B; ++c) {
-        const Acc x0 = shfl_acc(r0, c, B), x1 = shfl_acc(r1, c, B), x2 = shfl_acc(r2, c, B);
-        if (c <= lane) {
-            const S* P = tile + sym_index(B, c, lane) * 9;  // block (lane, c)
-            y0 = fma_acc(Store<S>::to_acc(P[0]), x0, y0);
-            y0 = fma_acc(Store<S>::to_acc(P[3]), x1, y0);
-            y0 = fma_acc(Store<S>::to_acc(P[6]), x2, y0);
-            y1 = fma_acc(Store<S>::to_acc(P[1]), x0, y1);
-            y1 = fma_acc(Store<S>::to_acc(P[4]), x1, y1);
-            y1 = fma_acc(Store<S>::to_acc(P[7]), x2, y1);
-            y2 = fma_acc(Store<S>::to_acc(P[2]), x0, y2);
-            y2 = fma_acc(Store<S>::to_acc(P[5]), x1, y2);
-            y2 = fma_acc(Store<S>::to_acc(P[8]), x2, y2);
+    #pragma unroll 2
+    for (int c0 = 0; c0 < B; c0 += 4) {
+        Acc v[12];
+        xch_get4(xb, c0, v);
+        #pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int c = c0 + j;
+            if (c <= lane) {
+                const Acc x0 = v[3 * j], x1 = v[3 * j + 1], x2 = v[3 * j + 2];
+                const S* P = tile + sym_index(B, c, lane) * 9;  // block (lane, c)
+                y0 = fma_acc(Store<S>::to_acc(P[0]), x0, y0);
+                y0 = fma_acc(Store<S>::to_acc(P[3]), x1, y0);
+                y0 = fma_acc(Store<S>::to_acc(P[6]), x2, y0);
+                y1 = fma_acc(Store<S>::to_acc(P[1]), x0, y1);
+                y1 = fma_acc(Store<S>::to_acc(P[4]), x1, y1);
+                y1 = fma_acc(Store<S>::to_acc(P[7]), x2, y1);
+                y2 = fma_acc(Store<S>::to_acc(P[2]), x0, y2);
+                y2 = fma_acc(Store<S>::to_acc(P[5]), x1, y2);
+                y2 = fma_acc(Store<S>::to_acc(P[8]), x2, y2);
+            }
         }
     }
+    xch_put(xb, lane, y0, y1, y2);
     Acc a0 = 0, a1 = 0, a2 = 0;
-    #pragma unroll 4
-    for (int c = 0; c < B; ++c) {
-        const Acc w0 = shfl_acc(y0, c, B), w1 = shfl_acc(y1, c, B), w2 = shfl_acc(y2, c, B);
-        if (c >= lane) {
-            const S* P = tile + sym_index(B, lane, c) * 9;  // block (c, lane), used transposed
-            a0 = fma_acc(Store<S>::to_acc(P[0]), w0, a0);
-            a0 = fma_acc(Store<S>::to_acc(P[1]), w1, a0);
-            a0 = fma_acc(Store<S>::to_acc(P[2]), w2, a0);
-            a1 = fma_acc(Store<S>::to_acc(P[3]), w0, a1);
-            a1 = fma_acc(Store<S>::to_acc(P[4]), w1, a1);
-            a1 = fma_acc(Store<S>::to_acc(P[5]), w2, a1);
-            a2 = fma_acc(Store<S>::to_acc(P[6]), w0, a2);
-            a2 = fma_acc(Store<S>::to_acc(P[7]), w1, a2);
-            a2 = fma_acc(Store<S>::to_acc(P[8]), w2, a2);
+    #pragma unroll 2
+    for (int c0 = 0; c0 < B; c0 += 4) {
+        Acc v[12];
+        xch_get4(xb, c0, v);
+        #pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int c = c0 + j;
+            if (c >= lane) {
+                const Acc w0 = v[3 * j], w1 = v[3 * j + 1], w2 = v[3 * j + 2];
+                const S* P = tile + sym_index(B, lane, c) * 9;  // block (c, lane), used transposed
+                a0 = fma_acc(Store<S>::to_acc(P[0]), w0, a0);
+                a0 = fma_acc(Store<S>::to_acc(P[1]), w1, a0);
+                a0 = fma_acc(Store<S>::to_acc(P[2]), w2, a0);
+                a1 = fma_acc(Store<S>::to_acc(P[3]), w0, a1);
+                a1 = fma_acc(Store<S>::to_acc(P[4]), w1, a1);
+                a1 = fma_acc(Store<S>::to_acc(P[5]), w2, a1);
+                a2 = fma_acc(Store<S>::to_acc(P[6]), w0, a2);
+                a2 = fma_acc(Store<S>::to_acc(P[7]), w1, a2);
+                a2 = fma_acc(Store<S>::to_acc(P[8]), w2, a2);
+            }
         }
     }
     z0 = a0; z1 = a1; z2 = a2;
 }
 
-// z_lane = sum_c P(lane, c) r_c over one bank; columns ascending, each 3x3
-// row an fma chain (the order the oracle restates).  Factored tiles take
-// schwarz_factored.
+// z_lane = sum_c P(lane, c) r_c over one bank (xb holds r, put there by
+// xch_put); columns ascending, each 3x3 row an fma chain (the order the
+// oracle restates).  Factored tiles take schwarz_factored (which leaves W r
+// in xb).  Called by whole warps.
 template <int B, typename S, typename Acc>
-__device__ __forceinline__ void schwarz_rows(const S* tile, int lane, Acc r0, Acc r1, Acc r2, Acc& z0, Acc& z1,
-                                             Acc& z2) {
+__device__ __forceinline__ void schwarz_rows(const S* tile, int lane, Acc* xb, Acc& z0, Acc& z1, Acc& z2) {
     if constexpr (is_fact<S>::value) {
-        schwarz_factored<B, S, Acc>(tile, lane, r0, r1, r2, z0, z1, z2);
-        return;
+        schwarz_factored<B, S, Acc>(tile, lane, xb, z0, z1, z2);
+    } else {
+        Acc a0 = 0, a1 = 0, a2 = 0;
+        #pragma unroll 2
+        for (int c0 = 0; c0 < B; c0 += 4) {
+            Acc v[12];
+            xch_get4(xb, c0, v);
+            #pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c = c0 + j;
+                const Acc x0 = v[3 * j], x1 = v[3 * j + 1], x2 = v[3 * j + 2];
+                const bool tr = c < lane;
+                const S* P = tile + (tr ? sym_index(B, c, lane) : sym_index(B, lane, c)) * 9;
+                const int s1 = tr ? 1 : 3, s2 = tr ? 3 : 1;  // element (a, k) at a*s2 + k*s1
+                a0 = fma_acc(Store<S>::to_acc(P[0]), x0, a0);
+                a0 = fma_acc(Store<S>::to_acc(P[s1]), x1, a0);
+                a0 = fma_acc(Store<S>::to_acc(P[2 * s1]), x2, a0);
+                a1 = fma_acc(Store<S>::to_acc(P[s2]), x0, a1);
+                a1 = fma_acc(Store<S>::to_acc(P[s2 + s1]), x1, a1);
+                a1 = fma_acc(Store<S>::to_acc(P[s2 + 2 * s1]), x2, a1);
+                a2 = fma_acc(Store<S>::to_acc(P[2 * s2]), x0, a2);
+                a2 = fma_acc(Store<S>::to_acc(P[2 * s2 + s1]), x1, a2);
+                a2 = fma_acc(Store<S>::to_acc(P[2 * s2 + 2 * s1]), x2, a2);
+            }
+        }
+        z0 = a0; z1 = a1; z2 = a2;
     }
-    Acc a0 = 0, a1 = 0, a2 = 0;
-    #pragma unroll 4
-    for (int c = 0; c < B; ++c) {
-        const Acc x0 = shfl_acc(r0, c, B), x1 = shfl_acc(r1, c, B), x2 = shfl_acc(r2, c, B);
-        const bool tr = c < lane;
-        const S* P = tile + (tr ? sym_index(B, c, lane) : sym_index(B, lane, c)) * 9;
-        const int s1 = tr ? 1 : 3, s2 = tr ? 3 : 1;  // element (a, k) at a*s2 + k*s1
-        a0 = fma_acc(Store<S>::to_acc(P[0]), x0, a0);
-        a0 = fma_acc(Store<S>::to_acc(P[s1]), x1, a0);
-        a0 = fma_acc(Store<S>::to_acc(P[2 * s1]), x2, a0);
-        a1 = fma_acc(Store<S>::to_acc(P[s2]), x0, a1);
-        a1 = fma_acc(Store<S>::to_acc(P[s2 + s1]), x1, a1);
-        a1 = fma_acc(Store<S>::to_acc(P[s2 + 2 * s1]), x2, a1);
-        a2 = fma_acc(Store<S>::to_acc(P[2 * s2]), x0, a2);
-        a2 = fma_acc(Store<S>::to_acc(P[2 * s2 + s1]), x1, a2);
-        a2 = fma_acc(Store<S>::to_acc(P[2 * s2 + 2 * s1]), x2, a2);
-    }
-    z0 = a0; z1 = a1; z2 = a2;
 }
 
-// Sum `v` over the lanes of this bank that share `key` (lanes ascending, the
-// order the oracle restates); *lead = lowest lane of its group.
+// Sum over the lanes of this bank whose bit is set in msk (a level-0
+// component), lanes ascending; xb holds the bank's values.
 template <int B, typename Acc>
-__device__ __forceinline__ void group_sum(int key, Acc v0, Acc v1, Acc v2, int lane, Acc& s0, Acc& s1, Acc& s2,
-                                          bool& lead) {
+__device__ __forceinline__ void mask_sum(unsigned msk, const Acc* xb, Acc& s0, Acc& s1, Acc& s2) {
+    s0 = 0; s1 = 0; s2 = 0;
+    #pragma unroll 2
+    for (int c0 = 0; c0 < B; c0 += 4) {
+        Acc v[12];
+        xch_get4(xb, c0, v);
+        #pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (msk & (1u << (c0 + j))) { s0 += v[3 * j]; s1 += v[3 * j + 1]; s2 += v[3 * j + 2]; }
+    }
+}
+
+// Sum the bank's values (xb) over the lanes that share `key` (lanes
+// ascending, the order the oracle restates); *lead = lowest lane of its
+// group.  Called by whole warps.
+template <int B, typename Acc>
+__device__ __forceinline__ void group_sum(int key, const Acc* xb, int lane, Acc& s0, Acc& s1, Acc& s2, bool& lead) {
     s0 = 0; s1 = 0; s2 = 0;
     lead = key >= 0;
-    #pragma unroll 4
-    for (int j = 0; j < B; ++j) {
-        const int kj = __shfl_sync(0xffffffffu, key, j, B);
-        const Acc y0 = shfl_acc(v0, j, B), y1 = shfl_acc(v1, j, B), y2 = shfl_acc(v2, j, B);
-        if (key >= 0 && kj == key) {
-            s0 += y0; s1 += y1; s2 += y2;
-            if (j < lane) lead = false;
+    #pragma unroll 2
+    for (int c0 = 0; c0 < B; c0 += 4) {
+        Acc v[12];
+        xch_get4(xb, c0, v);
+        #pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int kj = __shfl_sync(0xffffffffu, key, c0 + j, B);
+            if (key >= 0 && kj == key) {
+                s0 += v[3 * j]; s1 += v[3 * j + 1]; s2 += v[3 * j + 2];
+                if (c0 + j < lane) lead = false;
+            }
         }
     }
 }

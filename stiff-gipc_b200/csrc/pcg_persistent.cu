@@ -204,7 +204,7 @@ __device__ __forceinline__ Own own_ranges(const PArgs& a) {
 // index) with tiles at `tiles`; results to zs.  Warps whose half-warps are all
 // idle skip (the shuffles need whole warps).
 template <int B, typename S, typename Acc>
-__device__ __forceinline__ void smem_banks(const S* tiles, const Acc* rs, Acc* zs, int nbk) {
+__device__ __forceinline__ void smem_banks(const S* tiles, const Acc* rs, Acc* zs, int nbk, Acc* xch) {
     constexpr int bs = bsym_of(B);
     constexpr int HPW = 32 / B;
     const int lane = threadIdx.x % B;
@@ -215,8 +215,10 @@ __device__ __forceinline__ void smem_banks(const S* tiles, const Acc* rs, Acc* z
         const int i = hw * B + lane;
         const Acc v0 = valid ? rs[3 * i] : (Acc)0, v1 = valid ? rs[3 * i + 1] : (Acc)0,
                   v2 = valid ? rs[3 * i + 2] : (Acc)0;
+        Acc* xb = bank_slot<B>(xch);
+        xch_put(xb, lane, v0, v1, v2);
         Acc z0, z1, z2;
-        schwarz_rows<B, S, Acc>(tiles + (size_t)(valid ? hw : 0) * bs * 9, lane, v0, v1, v2, z0, z1, z2);
+        schwarz_rows<B, S, Acc>(tiles + (size_t)(valid ? hw : 0) * bs * 9, lane, xb, z0, z1, z2);
         if (valid) { zs[3 * i] = z0; zs[3 * i + 1] = z1; zs[3 * i + 2] = z2; }
     }
 }
@@ -236,7 +238,7 @@ struct Anc {
 // this CTA's ancestor banks (cached tiles, or staged per level).
 template <int B, typename S, typename Acc>
 __device__ __forceinline__ bool levels_c(const PArgs& a, const Anc& anc, S* tilesC, Acc* Rc, Acc* Zc,
-                                         const int* parc, uint64_t* mbar, unsigned& mphase) {
+                                         const int* parc, uint64_t* mbar, unsigned& mphase, Acc* xch) {
     constexpr int bs = bsym_of(B);
     constexpr int HPW = 32 / B;
     const int base = a.lvl_begin[2];
@@ -259,9 +261,11 @@ __device__ __forceinline__ bool levels_c(const PArgs& a, const Anc& anc, S* tile
             const Acc v0 = valid ? Rc[3 * i] : (Acc)0, v1 = valid ? Rc[3 * i + 1] : (Acc)0,
                       v2 = valid ? Rc[3 * i + 2] : (Acc)0;
             const int par = valid ? parc[i] : -1;
+            Acc* xb = bank_slot<B>(xch);
+            xch_put(xb, lane, v0, v1, v2);
             Acc s0, s1, s2;
             bool lead;
-            group_sum<B, Acc>(par, v0, v1, v2, lane, s0, s1, s2, lead);
+            group_sum<B, Acc>(par, xb, lane, s0, s1, s2, lead);
             if (lead) { Rc[3 * par] = s0; Rc[3 * par + 1] = s1; Rc[3 * par + 2] = s2; }
         }
         __syncthreads();
@@ -276,8 +280,10 @@ __device__ __forceinline__ bool levels_c(const PArgs& a, const Anc& anc, S* tile
             const int i = valid ? (anc.lo[l] + hw - first - bbase) * B + lane : 0;
             const Acc v0 = valid ? Rc[3 * i] : (Acc)0, v1 = valid ? Rc[3 * i + 1] : (Acc)0,
                       v2 = valid ? Rc[3 * i + 2] : (Acc)0;
+            Acc* xb = bank_slot<B>(xch);
+            xch_put(xb, lane, v0, v1, v2);
             Acc z0, z1, z2;
-            schwarz_rows<B, S, Acc>(tilesC + (size_t)(valid ? hw : 0) * bs * 9, lane, v0, v1, v2, z0, z1, z2);
+            schwarz_rows<B, S, Acc>(tilesC + (size_t)(valid ? hw : 0) * bs * 9, lane, xb, z0, z1, z2);
             if (valid) { Zc[3 * i] = z0; Zc[3 * i + 1] = z1; Zc[3 * i + 2] = z2; }
         }
     } else {  // staged: each level's range in chunks of capc tiles
@@ -293,7 +299,7 @@ __device__ __forceinline__ bool levels_c(const PArgs& a, const Anc& anc, S* tile
                 if (!mbar_wait(mbar, mphase, a.err)) return false;
                 mphase ^= 1u;
                 const int off = (anc.lo[l] + c0 - bbase) * B;
-                smem_banks<B, S, Acc>(tilesC, Rc + 3 * (size_t)off, Zc + 3 * (size_t)off, ncb);
+                smem_banks<B, S, Acc>(tilesC, Rc + 3 * (size_t)off, Zc + 3 * (size_t)off, ncb, xch);
             }
         }
     }
@@ -306,6 +312,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t mbar;
     __shared__ double sh[32];
+    __shared__ __align__(16) Acc xch[(kPT / 32) * kXchPerWarp];
     constexpr int bs = bsym_of(B);
     constexpr int HPW = 32 / B;
     const size_t tb = (size_t)bs * 9;  // elements per tile
@@ -420,17 +427,14 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     // level-0 (+ level-1) part of the apply on r (registers)
     auto apply_b = [&]() {
         if (act0) {
-            const Acc ra = (Acc)r0, rb = (Acc)r1, rc = (Acc)r2;
-            Acc s0 = 0, s1 = 0, s2 = 0;
-            #pragma unroll 4
-            for (int j = 0; j < B; ++j) {
-                const Acc y0 = shfl_acc(ra, j, B), y1 = shfl_acc(rb, j, B), y2 = shfl_acc(rc, j, B);
-                if (msk & (1u << j)) { s0 += y0; s1 += y1; s2 += y2; }
-            }
+            Acc* xb = bank_slot<B>(xch);
+            xch_put(xb, lane, (Acc)r0, (Acc)r1, (Acc)r2);
+            Acc s0, s1, s2;
+            mask_sum<B, Acc>(msk, xb, s0, s1, s2);
             if (own && a.L >= 2 && __popc(msk & lanemask_lt(lane)) == 0) {
                 R1s[3 * n1loc] = s0; R1s[3 * n1loc + 1] = s1; R1s[3 * n1loc + 2] = s2;
             }
-            schwarz_rows<B, S, Acc>(tiles0 + (size_t)(hw < o.nbk0 ? hw : 0) * tb, lane, ra, rb, rc, zl0, zl1, zl2);
+            schwarz_rows<B, S, Acc>(tiles0 + (size_t)(hw < o.nbk0 ? hw : 0) * tb, lane, xb, zl0, zl1, zl2);
         }
         if (a.L < 2) return;
         __syncthreads();
@@ -439,17 +443,19 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             const int i = hw * B + lane;
             const Acc v0 = valid ? R1s[3 * i] : (Acc)0, v1 = valid ? R1s[3 * i + 1] : (Acc)0,
                       v2 = valid ? R1s[3 * i + 2] : (Acc)0;
+            Acc* xb = bank_slot<B>(xch);
+            xch_put(xb, lane, v0, v1, v2);
             if (a.L > 2) {
                 Acc s0, s1, s2;
                 bool lead;
-                group_sum<B, Acc>(par1, v0, v1, v2, lane, s0, s1, s2, lead);
+                group_sum<B, Acc>(par1, xb, lane, s0, s1, s2, lead);
                 if (lead) {
                     Acc* Rg = (Acc*)a.R + 3 * (size_t)(a.lvl_begin[2] + par1);
                     Rg[0] = s0; Rg[1] = s1; Rg[2] = s2;
                 }
             }
             Acc z0, z1, z2;
-            schwarz_rows<B, S, Acc>(tiles1 + (size_t)(valid ? hw : 0) * tb, lane, v0, v1, v2, z0, z1, z2);
+            schwarz_rows<B, S, Acc>(tiles1 + (size_t)(valid ? hw : 0) * tb, lane, xb, z0, z1, z2);
             if (valid) { Z1s[3 * i] = z0; Z1s[3 * i + 1] = z1; Z1s[3 * i + 2] = z2; }
         }
         __syncthreads();
@@ -484,7 +490,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         if (ok) apply_b();
         if (a.L > 2) {
             ok = ok && grid_barrier(a.sync, epoch, a.err);
-            if (ok) ok = levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase);
+            if (ok) ok = levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch);
         }
         if (ok) collect();
     } else {
@@ -552,7 +558,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             if (a.L > 2) {
                 if (!grid_barrier(a.sync, epoch, a.err, SLOT(3))) { ok = false; break; }
                 stamp(a, k, 3);
-                if (!levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase)) ok = false;
+                if (!levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch)) ok = false;
             }
             collect();
         } else {
@@ -629,7 +635,9 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
     const size_t tb = (size_t)bs * 9 * sizeof(S);
     int max_smem = 0;
     SG_CUDA(c, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
-    const size_t budget = (size_t)max_smem - 2048;  // static shared memory of the kernel
+    cudaFuncAttributes fa;
+    SG_CUDA(c, cudaFuncGetAttributes(&fa, k_pcg_persistent<B, S, Acc>));
+    const size_t budget = (size_t)max_smem - fa.sharedSizeBytes - 256;  // minus the kernel's static shared memory
     const int G = dev_sms;
     size_t smem = 0;
     if (a.precond == 1) {
