@@ -248,7 +248,9 @@ int sgmas_mas_apply(sgmas_context* c, const double* d_r, double* d_z) {
     if (!c || !d_r || !d_z) return SGMAS_ERR_ARG;
     if (!c->mas_assembled) return ctx_fail(c, SGMAS_ERR_STATE, "sgmas_mas_apply before sgmas_mas_assemble");
     SG_CUDA(c, cudaSetDevice(c->device));
-    return mas_launch_apply(c, d_r, d_z, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0ull, nullptr);
+    const ExtraRows none = {0, 0, c->N, 0, nullptr};
+    return mas_launch_apply(c, d_r, d_z, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0ull, nullptr,
+                            none);
 }
 
 int sgmas_mas_info(sgmas_context* c, int* levelnum, int* total_clusters, int* n_mas_blocks) {
@@ -331,9 +333,11 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
         return ctx_fail(c, SGMAS_ERR_ARG, "sgmas_pcg_solve: bad configuration");
     if (cfg->preconditioner == 1) {
         if (!c->mas_init) return ctx_fail(c, SGMAS_ERR_STATE, "MAS preconditioner requested before sgmas_mas_init");
-        if (cfg->abd_bodies != 0 || cfg->fem_offset != 0 || c->N != A->n_block_rows)
+        // bodies first (rows 0 .. 4 bodies), the MAS's N vertices at fem_offset (global_linear_system.cu:509-522)
+        if (cfg->fem_offset < 4 * cfg->abd_bodies || cfg->fem_offset + c->N > A->n_block_rows)
             return ctx_fail(c, SGMAS_ERR_ARG,
-                            "MAS-PCG needs the FEM range to cover the whole system (N=%d, rows=%d, offset=%d, bodies=%d)",
+                            "MAS range [fem_offset, fem_offset + N) must follow the body rows and fit the system "
+                            "(N=%d, rows=%d, offset=%d, bodies=%d)",
                             c->N, A->n_block_rows, cfg->fem_offset, cfg->abd_bodies);
     }
     SG_CUDA(c, cudaSetDevice(c->device));
@@ -356,7 +360,8 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
     int rc = pcg_prepare(c, A, rc_cfg);
     if (rc) return rc;
     if (rc_cfg.precond == 1) {
-        rc = mas_assemble_impl(c, A->d_values, A->d_rows, A->d_cols, nullptr, 0, A->n_blocks, c->cp_num);
+        rc = mas_assemble_impl(c, A->d_values, A->d_rows, A->d_cols, nullptr, rc_cfg.fem_offset, A->n_blocks,
+                               c->cp_num);
         if (rc) return rc;
     }
     float solve_ms = 0.f;

@@ -15,6 +15,15 @@ struct PcgState {
     int use_prec_norm, pad;
 };
 
+// Rows of a solve outside the MAS range (the reference's hybrid scenes:
+// affine bodies first, 4 block rows each, then the FEM vertices the MAS
+// covers at fem_off .. fem_off + N, then any further rows).  Each unit is a
+// body (12x12 block-Jacobi) or one other row (identity: z = r).
+struct ExtraRows {
+    int fem_off, abd_bodies, nrows, n_units;
+    const double* abd_inv;  // 144 per body, row-major inverse
+};
+
 struct PcgRunCfgLite {
     int precond, abd_bodies, valid;
 };
@@ -167,7 +176,9 @@ int mas_scatter_and_invert(sgmas_context* c, const double* vals, const int* rows
                            const uint32_t* indices, int offset, int n);
 int mas_launch_apply(sgmas_context* c, const double* r, double* z, int mode, const PcgState* st,
                      double* x, const double* p, const double* Ap, double* partials, unsigned* ticket,
-                     int iter_kind, unsigned long long cond_handle, int* launches);
+                     int iter_kind, unsigned long long cond_handle, int* launches, const ExtraRows& ex);
+// the extra rows of a MAS solve with configuration cfg (n_units = 0 when the MAS covers every row)
+ExtraRows extra_rows_of(const sgmas_context* c, const PcgRunCfg& cfg);
 int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* cols, int nblocks,
               int nrows);
 int bsr_spmv_plain(sgmas_context* c, double a, const double* x, double b, double* y);

@@ -18,6 +18,7 @@
 #include "ctx.hpp"
 #include "pcg_state.cuh"
 #include "mas_dev.cuh"
+#include "extra_dev.cuh"
 
 using namespace sgmas;
 
@@ -806,7 +807,8 @@ template <typename Acc>
 __global__ void __launch_bounds__(kCollectThreads) k_collect(int N, int L, int Mm, const int* __restrict__ level_size,
                                                       const int* __restrict__ real_map,
                                                       const int* __restrict__ coarse_table, const Acc* __restrict__ Z,
-                                                      Acc* R, const double* __restrict__ r, double* z, int kind,
+                                                      Acc* R, double* r, double* z, ExtraRows ex, int mode, double* x,
+                                                      const double* p, const double* Ap, int kind,
                                                       PcgState* st, double* partials, unsigned* ticket,
                                                       int set_cond, unsigned long long cond) {
     if (st && st->done) {
@@ -816,22 +818,25 @@ __global__ void __launch_bounds__(kCollectThreads) k_collect(int N, int L, int M
         return;
     }
     __shared__ double sh[32];
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;  // MAS vertex v is row ex.fem_off + v of r, z
     double rz = 0.0, rr = 0.0;
     if (v < N) {
         const int rd = real_map[v];
+        const size_t o = 3 * (size_t)(ex.fem_off + v);
         Acc c0 = Z[3 * (size_t)rd], c1 = Z[3 * (size_t)rd + 1], c2 = Z[3 * (size_t)rd + 2];
         for (int i = 1; i < L; ++i) {
             const int now = coarse_table[(size_t)kMaxLevels * v + i - 1];
             c0 += Z[3 * (size_t)now]; c1 += Z[3 * (size_t)now + 1]; c2 += Z[3 * (size_t)now + 2];
         }
         const double z0 = (double)c0, z1 = (double)c1, z2 = (double)c2;
-        z[3 * (size_t)v] = z0; z[3 * (size_t)v + 1] = z1; z[3 * (size_t)v + 2] = z2;
+        z[o] = z0; z[o + 1] = z1; z[o + 2] = z2;
         if (kind >= 1) {
-            const double r0 = r[3 * (size_t)v], r1 = r[3 * (size_t)v + 1], r2 = r[3 * (size_t)v + 2];
+            const double r0 = r[o], r1 = r[o + 1], r2 = r[o + 2];
             rz = r0 * z0 + r1 * z1 + r2 * z2;
             rr = r0 * r0 + r1 * r1 + r2 * r2;
         }
+    } else if (kind >= 1 && v - N < ex.n_units) {  // rows outside the MAS range
+        extra_unit(v - N, ex, N, mode, mode == 1 ? st->alpha : 0.0, x, r, p, Ap, z, rz, rr);
     }
     if (kind < 1) return;
     const double brz = block_sum<kCollectThreads>(rz, sh);
@@ -933,7 +938,10 @@ int scatter_invert_t(sgmas_context* c, const double* vals, const int* rows, cons
 
 template <int B, typename S, typename Acc>
 int apply_t(sgmas_context* c, const double* r, double* z, int mode, const PcgState* st, double* x, const double* p,
-            const double* Ap, double* partials, unsigned* ticket, int kind, unsigned long long cond, int* launches) {
+            const double* Ap, double* partials, unsigned* ticket, int kind, unsigned long long cond, int* launches,
+            const ExtraRows& ex) {
+    // r, z, x, p, Ap are whole-system vectors; the MAS kernels see the FEM range
+    const size_t fo = 3 * (size_t)ex.fem_off;
     cudaStream_t s = c->stream;
     constexpr int bs = bsym_of(B);
     const size_t smem0 = (size_t)kL0Banks * bs * 9 * sizeof(S);
@@ -947,19 +955,20 @@ int apply_t(sgmas_context* c, const double* r, double* z, int mode, const PcgSta
     const int parts = c->apply_parts;
     if (parts & 1)
         k0<<<(nbank0 + kL0Banks - 1) / kL0Banks, kL0Banks * B, smem0, s>>>(
-            c->Mm, c->L, c->d_part_map, c->d_fine_mask, c->d_going_next, (const S*)c->d_inv, (double*)r,
-            (Acc*)c->d_R, (Acc*)c->d_Z, mode, x, p, Ap, st, c->d_err);
+            c->Mm, c->L, c->d_part_map, c->d_fine_mask, c->d_going_next, (const S*)c->d_inv, (double*)r + fo,
+            (Acc*)c->d_R, (Acc*)c->d_Z, mode, x ? x + fo : nullptr, p ? p + fo : nullptr, Ap ? Ap + fo : nullptr,
+            st, c->d_err);
     // level-1 banks are bounded by the vertex count (extra CTAs return at once)
     const int l1_cap = (c->N + B - 1) / B + 1;
     if (parts & 2)
         k1<<<(l1_cap + coarse_bpc<B>() - 1) / coarse_bpc<B>(), kCoarseThreads, smem1, s>>>(
             c->L, c->d_level_size, c->d_going_next, (const S*)c->d_inv, (Acc*)c->d_R, (Acc*)c->d_Z, st,
             c->d_coarse_ticket, c->d_err);
-    const int gN = (c->N + kCollectThreads - 1) / kCollectThreads;
+    const int gN = (c->N + (kind >= 1 ? ex.n_units : 0) + kCollectThreads - 1) / kCollectThreads;
     if (parts & 4)
-    k_collect<Acc><<<gN, kCollectThreads, 0, s>>>(c->N, c->L, c->Mm, c->d_level_size, c->d_real_map, c->d_coarse_table,
-                                          (const Acc*)c->d_Z, (Acc*)c->d_R, r, z, kind, (PcgState*)st, partials,
-                                          ticket, cond != 0ull, cond);
+        k_collect<Acc><<<gN, kCollectThreads, 0, s>>>(
+            c->N, c->L, c->Mm, c->d_level_size, c->d_real_map, c->d_coarse_table, (const Acc*)c->d_Z, (Acc*)c->d_R,
+            (double*)r, z, ex, mode, x, p, Ap, kind, (PcgState*)st, partials, ticket, cond != 0ull, cond);
     SG_CUDA(c, cudaGetLastError());
     if (launches) *launches += 3;
     return 0;
@@ -993,21 +1002,21 @@ int mas_scatter_and_invert(sgmas_context* c, const double* vals, const int* rows
 
 int mas_launch_apply(sgmas_context* c, const double* r, double* z, int mode, const PcgState* st, double* x,
                      const double* p, const double* Ap, double* partials, unsigned* ticket, int iter_kind,
-                     unsigned long long cond_handle, int* launches) {
+                     unsigned long long cond_handle, int* launches, const ExtraRows& ex) {
 #define SG_DISPATCH(B)                                                                                          \
     switch (c->precision) {                                                                                     \
         case SGMAS_MAS_FP32:                                                                                    \
             return apply_t<B, float, float>(c, r, z, mode, st, x, p, Ap, partials, ticket, iter_kind, cond_handle, \
-                                            launches);                                                          \
+                                            launches, ex);                                                          \
         case SGMAS_MAS_BF16:                                                                                    \
             return apply_t<B, Fact<__nv_bfloat16>, float>(c, r, z, mode, st, x, p, Ap, partials, ticket,        \
-                                                          iter_kind, cond_handle, launches);                    \
+                                                          iter_kind, cond_handle, launches, ex);                \
         case SGMAS_MAS_FP32_FACTORED:                                                                           \
             return apply_t<B, Fact<float>, float>(c, r, z, mode, st, x, p, Ap, partials, ticket, iter_kind,     \
-                                                  cond_handle, launches);                                       \
+                                                  cond_handle, launches, ex);                                   \
         default:                                                                                                \
             return apply_t<B, double, double>(c, r, z, mode, st, x, p, Ap, partials, ticket, iter_kind,         \
-                                              cond_handle, launches);                                           \
+                                              cond_handle, launches, ex);                                       \
     }
     if (c->bank == 16) { SG_DISPATCH(16) }
     SG_DISPATCH(32)

@@ -469,10 +469,12 @@ int bcoo_spmv_ref(sgmas_context* c, double a, const double* vals, const int* row
 
 // Prepare the preconditioner data that depends on A (block-Jacobi inverses).
 static int jacobi_setup(sgmas_context* c, const double* vals, const int* rows, const int* cols, int nb, int nrows,
-                        int abd_bodies) {
+                        int abd_bodies, bool diag = true) {
     cudaStream_t s = c->stream;
-    SG_CUDA(c, cudaMemsetAsync(c->d_diag_inv, 0, sizeof(double) * 9 * nrows, s));
-    if (nb > 0) k_diag_inverse<<<(nb + kT - 1) / kT, kT, 0, s>>>(nb, rows, cols, vals, c->d_diag_inv);
+    if (diag) {
+        SG_CUDA(c, cudaMemsetAsync(c->d_diag_inv, 0, sizeof(double) * 9 * nrows, s));
+        if (nb > 0) k_diag_inverse<<<(nb + kT - 1) / kT, kT, 0, s>>>(nb, rows, cols, vals, c->d_diag_inv);
+    }
     if (abd_bodies > 0) {
         if (abd_bodies > c->abd_cap) {
             if (ctx_alloc(c, &c->d_abd_inv, 144 * (size_t)abd_bodies)) return SGMAS_ERR_CUDA;
@@ -481,7 +483,7 @@ static int jacobi_setup(sgmas_context* c, const double* vals, const int* rows, c
         k_abd_inverse<<<(abd_bodies + 63) / 64, 64, 0, s>>>(abd_bodies, nb, rows, cols, vals, c->bsr.first, c->bsr.cnt,
                                                             c->bsr.cnt_lower, c->d_abd_inv, c->d_err);
     }
-    c->build_launches += (nb > 0 ? 1 : 0) + (abd_bodies > 0 ? 1 : 0);
+    c->build_launches += (diag && nb > 0 ? 1 : 0) + (abd_bodies > 0 ? 1 : 0);
     SG_CUDA(c, cudaGetLastError());
     return 0;
 }
@@ -499,8 +501,8 @@ static int record_prologue(sgmas_context* c, const double* b, double* x, const P
                                  cfg.check_every, cfg.use_prec_norm);
     *nk = 1;
     if (cfg.precond == 1) {
-        int rc = mas_launch_apply(c, c->d_r, c->d_z, 0, c->d_state, nullptr, nullptr, nullptr, c->d_partials,
-                                  c->d_ticket, 1, 0ull, nk);
+        int rc = mas_launch_apply(c, c->d_r, c->d_z, 0, c->d_state, x, nullptr, nullptr, c->d_partials,
+                                  c->d_ticket, 1, 0ull, nk, extra_rows_of(c, cfg));
         if (rc) return rc;
     } else {
         const int g = (nrows + kT - 1) / kT;
@@ -539,7 +541,7 @@ static int record_body(sgmas_context* c, cudaStream_t s, const double* b, double
         }
         if (cfg.precond == 1) {
             rc = mas_launch_apply(c, c->d_r, c->d_z, check ? 0 : 1, c->d_state, x, pnew, c->d_Ap, c->d_partials,
-                                  c->d_ticket, 2, cnd, nk);
+                                  c->d_ticket, 2, cnd, nk, extra_rows_of(c, cfg));
         } else if (check) {
             k_jacobi_iter<0><<<gj, kT, 0, s>>>(nrows, 4 * cfg.abd_bodies, x, c->d_r, pnew, c->d_Ap, c->d_z,
                                                c->d_diag_inv, c->d_abd_inv, 2, c->d_state, c->d_partials,
@@ -574,8 +576,9 @@ int pcg_run(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, 
                                  (unsigned long long)(uintptr_t)x,
                                  (unsigned long long)nrows | ((unsigned long long)c->bsr.cap << 24) ^
                                      ((unsigned long long)c->bsr.n_long << 44),
-                                 (unsigned long long)cfg.precond | ((unsigned long long)cfg.abd_bodies << 8) |
-                                     ((unsigned long long)c->precision << 40),
+                                 (unsigned long long)cfg.precond | ((unsigned long long)c->precision << 4) |
+                                     ((unsigned long long)cfg.abd_bodies << 8) |
+                                     ((unsigned long long)cfg.fem_offset << 36),
                                  (unsigned long long)(uintptr_t)c->bsr.vals,
                                  (unsigned long long)(uintptr_t)c->d_inv ^ ((unsigned long long)c->cap_total << 1),
                                  (unsigned long long)(uintptr_t)c->d_r,
@@ -767,7 +770,7 @@ int pcg_profile(sgmas_context* c, int reps, float* ms, int n_ms) {
             } else {
                 c->apply_parts = 1 << (part - 1);
                 rc = mas_launch_apply(c, c->d_r, c->d_z, part == 1 ? 1 : 0, c->d_state, c->last_x, c->d_p1, c->d_Ap,
-                                      c->d_partials, c->d_ticket, 3, 0ull, nullptr);
+                                      c->d_partials, c->d_ticket, 3, 0ull, nullptr, extra_rows_of(c, c->last_run));
                 c->apply_parts = 7;
             }
         }
@@ -789,7 +792,19 @@ int pcg_prepare(sgmas_context* c, const sgmas_bcoo* A, const PcgRunCfg& cfg) {
     int rc = bsr_build(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows);
     if (rc) return rc;
     if (cfg.precond == 0) return jacobi_setup(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows, cfg.abd_bodies);
+    if (cfg.abd_bodies > 0)  // MAS on the FEM range + 12x12 block-Jacobi on the bodies
+        return jacobi_setup(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows, cfg.abd_bodies, false);
     return 0;
+}
+
+ExtraRows extra_rows_of(const sgmas_context* c, const PcgRunCfg& cfg) {
+    ExtraRows ex;
+    ex.fem_off = cfg.precond == 1 ? cfg.fem_offset : 0;
+    ex.abd_bodies = cfg.precond == 1 ? cfg.abd_bodies : 0;
+    ex.nrows = c->bsr.nrows;
+    ex.n_units = cfg.precond == 1 ? ex.abd_bodies + (ex.fem_off - 4 * ex.abd_bodies) + (ex.nrows - ex.fem_off - c->N) : 0;
+    ex.abd_inv = c->d_abd_inv;
+    return ex;
 }
 
 int pcg_read_state(sgmas_context* c, PcgState* h) {

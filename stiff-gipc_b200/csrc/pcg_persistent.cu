@@ -37,6 +37,7 @@
 #include "ctx.hpp"
 #include "mas_dev.cuh"
 #include "spmv_dev.cuh"
+#include "extra_dev.cuh"
 
 using namespace sgmas;
 
@@ -60,6 +61,7 @@ struct PArgs {
     int k0, k1, nb0, nb1;  // level-0 banks per CTA (max), level-1 banks per CTA, bank counts
     int nc;                // nodes of levels >= 2 (a multiple of B)
     int capc;              // tiles of levels >= 2 a CTA holds in shared memory (<= kPT / B)
+    ExtraRows ex;          // rows outside the MAS range (bodies, other rows); MAS vertex v is row ex.fem_off + v
     // block-Jacobi
     const double* dinv;
     int abd_rows, precond;
@@ -339,6 +341,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     // ---- ownership, per-thread constants, cached tiles ----------------------
     Own o = {0, 0, 0, 0};
     int v = -1, n1loc = -1, par1 = -1;
+    int vo = 0;  // 3 * (global row of vertex v)
     unsigned msk = 0u;
     bool own = false;
     if (mas) {
@@ -402,6 +405,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         }
         if (hw < o.nbk0) v = a.part_map[(o.lo + hw) * B + lane];
         if (v >= 0) {
+            vo = 3 * (a.ex.fem_off + v);
             msk = a.fine_mask[v];
             if (a.L >= 2) {
                 const int n1 = a.going_next[v] - a.lvl_begin[1];
@@ -461,8 +465,10 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         __syncthreads();
     };
     // CollectFinalZ for the owned slot + r.z, r.r partials
-    auto collect = [&]() {
+    auto collect = [&](int mode, double alpha, const double* pcur) {
         double rz = 0.0, rr = 0.0;
+        for (int u = blockIdx.x * kPT + threadIdx.x; u < a.ex.n_units; u += gridDim.x * kPT)
+            extra_unit(u, a.ex, a.N, mode, alpha, a.x, a.r, pcur, a.Ap, a.z, rz, rr);
         if (own) {
             Acc c0 = zl0, c1 = zl1, c2 = zl2;
             if (a.L >= 2) { c0 += Z1s[3 * n1loc]; c1 += Z1s[3 * n1loc + 1]; c2 += Z1s[3 * n1loc + 2]; }
@@ -471,9 +477,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                 c0 += Zc[3 * n]; c1 += Zc[3 * n + 1]; c2 += Zc[3 * n + 2];
             }
             const double z0 = (double)c0, z1 = (double)c1, z2 = (double)c2;
-            a.z[3 * (size_t)v] = z0; a.z[3 * (size_t)v + 1] = z1; a.z[3 * (size_t)v + 2] = z2;
-            rz = r0 * z0 + r1 * z1 + r2 * z2;
-            rr = r0 * r0 + r1 * r1 + r2 * r2;
+            a.z[vo] = z0; a.z[vo + 1] = z1; a.z[vo + 2] = z2;
+            rz += r0 * z0 + r1 * z1 + r2 * z2;
+            rr += r0 * r0 + r1 * r1 + r2 * r2;
         }
         rz = block_sum<kPT>(rz, sh);
         rr = block_sum<kPT>(rr, sh);
@@ -483,16 +489,16 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     // ---- prologue: x = 0, r = b, p_old = 0, z = M^-1 r, r.z, r.r
     for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT) {
         a.p0[i] = 0.0;
-        if (!mas) { a.x[i] = 0.0; a.r[i] = a.b[i]; }
+        if (!mas || a.ex.n_units > 0) { a.x[i] = 0.0; a.r[i] = a.b[i]; }
     }
     if (mas) {
-        if (v >= 0) { r0 = a.b[3 * (size_t)v]; r1 = a.b[3 * (size_t)v + 1]; r2 = a.b[3 * (size_t)v + 2]; }
+        if (v >= 0) { r0 = a.b[vo]; r1 = a.b[vo + 1]; r2 = a.b[vo + 2]; }
         if (ok) apply_b();
         if (a.L > 2) {
             ok = ok && grid_barrier(a.sync, epoch, a.err);
             if (ok) ok = levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch);
         }
-        if (ok) collect();
+        if (ok) collect(0, 0.0, a.p1);
     } else {
         ok = ok && grid_barrier(a.sync, epoch, a.err);
         if (ok) phase_jacobi(a, 0, 0.0, a.p1, part_rz, part_rr, sh);
@@ -529,15 +535,21 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         // B: the slot's p and Ap are loaded before the partials are summed
         double p0v = 0.0, p1v = 0.0, p2v = 0.0, q0 = 0.0, q1 = 0.0, q2 = 0.0;
         if (mas && v >= 0) {
-            if (own) { p0v = pnew[3 * (size_t)v]; p1v = pnew[3 * (size_t)v + 1]; p2v = pnew[3 * (size_t)v + 2]; }
-            if (!refresh) { q0 = a.Ap[3 * (size_t)v]; q1 = a.Ap[3 * (size_t)v + 1]; q2 = a.Ap[3 * (size_t)v + 2]; }
+            if (own) { p0v = pnew[vo]; p1v = pnew[vo + 1]; p2v = pnew[vo + 2]; }
+            if (!refresh) { q0 = a.Ap[vo]; q1 = a.Ap[vo + 1]; q2 = a.Ap[vo + 2]; }
         }
         const double alpha = rz / sum_partials(part_pap, sh);
         if (refresh) {
             if (mas) {
                 if (own) {
                     x0 += alpha * p0v; x1 += alpha * p1v; x2 += alpha * p2v;
-                    a.x[3 * (size_t)v] = x0; a.x[3 * (size_t)v + 1] = x1; a.x[3 * (size_t)v + 2] = x2;
+                    a.x[vo] = x0; a.x[vo + 1] = x1; a.x[vo + 2] = x2;
+                }
+                // rows outside the MAS range
+                const int lo_n = 3 * a.ex.fem_off, hi_n = 3 * (a.ex.fem_off + a.N);
+                for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows - (hi_n - lo_n); i += gridDim.x * kPT) {
+                    const int e = i < lo_n ? i : i + (hi_n - lo_n);
+                    a.x[e] = a.x[e] + alpha * pnew[e];
                 }
             } else {
                 for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT)
@@ -547,7 +559,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             for (int u = gw0; u < a.units; u += gridDim.x * warps)
                 spmv_unit<2, true>(a.A, u, threadIdx.x & 31, a.x, nullptr, nullptr, a.r, a.b, 1.0, 0.0, 0.0);
             if (!grid_barrier(a.sync, epoch, a.err, SLOT(2))) { ok = false; break; }
-            if (mas && v >= 0) { r0 = a.r[3 * (size_t)v]; r1 = a.r[3 * (size_t)v + 1]; r2 = a.r[3 * (size_t)v + 2]; }
+            if (mas && v >= 0) { r0 = a.r[vo]; r1 = a.r[vo + 1]; r2 = a.r[vo + 2]; }
         } else if (mas && v >= 0) {
             r0 = r0 - alpha * q0; r1 = r1 - alpha * q1; r2 = r2 - alpha * q2;
             if (own) { x0 += alpha * p0v; x1 += alpha * p1v; x2 += alpha * p2v; }
@@ -560,7 +572,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                 stamp(a, k, 3);
                 if (!levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch)) ok = false;
             }
-            collect();
+            collect(refresh ? 0 : 1, alpha, pnew);
         } else {
             phase_jacobi(a, refresh ? 0 : 1, alpha, pnew, part_rz, part_rr, sh);
         }
@@ -590,8 +602,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     }
 #undef SLOT
     if (mas && own) {
-        a.x[3 * (size_t)v] = x0; a.x[3 * (size_t)v + 1] = x1; a.x[3 * (size_t)v + 2] = x2;
-        a.r[3 * (size_t)v] = r0; a.r[3 * (size_t)v + 1] = r1; a.r[3 * (size_t)v + 2] = r2;
+        a.x[vo] = x0; a.x[vo + 1] = x1; a.x[vo + 2] = x2;
+        a.r[vo] = r0; a.r[vo + 1] = r1; a.r[vo + 2] = r2;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         PcgState s = {};
@@ -700,7 +712,7 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
 int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, float* solve_ms,
                        int* launches, unsigned long long* stamps, int stamp_iters) {
     const BsrMatrix& M = c->bsr;
-    if (cfg.precond == 0 && cfg.abd_bodies > 0) return 1;  // 12x12 body blocks: graph form
+    if (cfg.precond == 0 && cfg.abd_bodies > 0) return 1;  // block-Jacobi with 12x12 body blocks: graph form
     PArgs a = {};
     a.A = BsrView{M.row_ptr, M.cols, M.vals, M.cap, M.row_list, M.nrows, M.n_long};
     a.b = b; a.x = x; a.r = c->d_r; a.z = c->d_z; a.p0 = c->d_p0; a.p1 = c->d_p1; a.Ap = c->d_Ap;
@@ -736,6 +748,7 @@ int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRu
         a.part_map = c->d_part_map; a.going_next = c->d_going_next;
         a.coarse_table = c->d_coarse_table; a.fine_mask = c->d_fine_mask;
         a.inv = c->d_inv; a.R = c->d_R;
+        a.ex = extra_rows_of(c, cfg);
     }
     int rc;
     switch ((c->bank == 16 ? 0 : 4) + c->precision) {

@@ -293,3 +293,47 @@ def full_matrix(s: System):
     off = s.rows != s.cols
     AT = sp.coo_matrix((v3[off].ravel(), (r3[off].ravel(), c3[off].ravel())), shape=(3 * n, 3 * n)).tocsr().T
     return (A + AT).tocsc()
+
+
+def hybrid_system(n_bodies=8, fem=(8, 8, 8), n_contacts=200, body_ratio=1e3, kappa_ratio=10.0, seed=0):
+    """Affine bodies + FEM mesh, as the reference's hybrid scenes lay them out:
+    each body is 12 DOF = 4 block rows, the bodies' rows come first
+    (SG/GIPC.cu:10082-10083, :10217), the FEM vertices follow at
+    fem_offset = 4 * n_bodies.  Body blocks: a dense SPD 12x12 (shape
+    stiffness) per body, scaled body_ratio times the FEM diagonal.
+    Couplings: body point x = t + A xbar against an FEM vertex, with
+    J = [I | xbar1 I | xbar2 I | xbar3 I] (3x12); the pair's 15x15 block is
+    kappa g g^T + eps I, g = [J^T n; -n], written as upper 3x3 blocks over
+    the body's 4 rows and the vertex's row.  pos / tets describe the FEM part
+    only (the MAS covers the FEM range)."""
+    rng = np.random.default_rng(seed + 17)
+    fs = make_grid_system(*fem, seed=seed)
+    off = 4 * n_bodies
+    N = fs.n_verts
+    diag = fs.vals[fs.rows == fs.cols]
+    dscale = float(np.mean(diag[:, [0, 4, 8]]))
+    G = rng.normal(size=(n_bodies, 12, 12))
+    Hb = (np.einsum("bij,bkj->bik", G, G) / 12.0 + 0.5 * np.eye(12)[None]) * dscale * body_ratio
+    nodes_b = off * 0 + 4 * np.arange(n_bodies)[:, None] + np.arange(4)[None, :]
+    rb, cb, vb = upper_triplets(Hb, nodes_b)
+    bod = rng.integers(0, n_bodies, n_contacts)
+    ver = rng.integers(0, N, n_contacts)
+    xbar = rng.uniform(-1.0, 1.0, (n_contacts, 3))
+    nrm = rng.normal(size=(n_contacts, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    J = np.zeros((n_contacts, 3, 12))
+    J[:, :, 0:3] = np.eye(3)
+    for k in range(3):
+        J[:, :, 3 + 3 * k:6 + 3 * k] = xbar[:, k, None, None] * np.eye(3)[None]
+    g = np.concatenate([np.einsum("pij,pi->pj", J, nrm), -nrm], 1)        # [p, 15]
+    Hc = dscale * kappa_ratio * (g[:, :, None] * g[:, None, :] + 1e-3 * np.eye(15)[None])
+    nodes_c = np.concatenate([4 * bod[:, None] + np.arange(4)[None, :], (off + ver)[:, None]], 1)
+    rc, cc, vc = upper_triplets(Hc, nodes_c)
+    rows = np.concatenate([fs.rows.astype(np.int64) + off, rb, rc])
+    cols = np.concatenate([fs.cols.astype(np.int64) + off, cb, cc])
+    vals = np.concatenate([fs.vals, vb, vc])
+    mr, mc, mv = merge_triplets(rows, cols, vals)
+    b = np.concatenate([rng.normal(size=3 * off) * float(np.abs(fs.b).mean()), fs.b])
+    return System(n_verts=off + N, rows=mr, cols=mc, vals=mv, b=b, pos=fs.pos, tets=fs.tets,
+                  pairs=np.zeros((0, 4), np.int32), raw_rows=rows, raw_cols=cols, raw_vals=vals,
+                  info=dict(abd_bodies=n_bodies, fem_offset=off, fem_n=N))
