@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--impl", default="sgmas", choices=["sgmas", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = benchmark size)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-other", action="store_true", help="skip the brief config 1 / config 3 lines")
     ap.add_argument("--variants", default="bf16,fp32,fp32f,fp64,jacobi,fp32-graph",
                     help="MAS storage precision (or jacobi); suffix -graph = kernel-per-phase CUDA graph "
                          "instead of the persistent cooperative kernel")
@@ -358,6 +359,8 @@ def run_sgmas(args):
            "speedup_vs_plain_fp64": (round(results["fp64"]["ms"] / results[head]["ms"], 3)
                                      if "ms" in results.get("fp64", {}) else None),
            "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "clocks": clocks_rec}
+    if not args.no_other:
+        out["other_configs"] = other_configs(args, dev, stream)
     if rank == 0 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(s, results)
     if world > 1:
@@ -367,6 +370,58 @@ def run_sgmas(args):
         ctx.close()
     if rank == 0:
         print(json.dumps(out))
+
+
+def other_configs(args, dev, stream):
+    """The other single-system configs, measured briefly beside the headline:
+    config 1 (small tet grid: latency-bound) and config 3 (affine bodies on a
+    cloth sheet, MAS on the cloth + 12x12 ABD block-Jacobi on the bodies)."""
+    import torch
+    import sgmas
+    from sgmas import synth
+
+    def tdev(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    out = {}
+    warm, steps = 2, max(1, min(args.steps, 3))
+    specs = [("config1", synth.config1(seed=0), None), ("config3", synth.config3(seed=0, scale=args.scale), "c3")]
+    for name, s, kind in specs:
+        if kind == "c3":
+            N, nb, off = s.info["fem_n"], s.info["abd_bodies"], s.info["fem_offset"]
+            nbs = sgmas.vert_neighbors(np.zeros((0, 4), np.int32), N, tris=s.info["tris"])
+        else:
+            N, nb, off = s.n_verts, 0, 0
+            nbs = sgmas.vert_neighbors(s.tets, s.n_verts)
+        vals, rows, cols, b, pos = tdev(s.vals), tdev(s.rows), tdev(s.cols), tdev(s.b), tdev(s.pos)
+        res = {"n_block_rows": int(s.n_verts), "n_blocks": int(len(s.rows)), "abd_bodies": nb}
+        for v in ("bf16", "fp32", "fp64", "jacobi"):
+            prec = "fp32" if v == "jacobi" else v
+            ctx = sgmas.Context(dev.index or 0, bank=16, precision=prec)
+            ctx.set_stream(stream.cuda_stream)
+            pm, rm = ctx.morton_partition(pos)
+            ctx.mas_init(N, *nbs, pm, rm)
+            x = torch.zeros_like(b)
+            kw = dict(rel_tol=REL_TOL, max_iter=MAX_ITER, preconditioner="jacobi" if v == "jacobi" else "mas",
+                      abd_bodies=nb, fem_offset=off if v != "jacobi" else 0)
+            try:
+                times = []
+                for i in range(warm + steps):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    rep = ctx.pcg_solve(vals, rows, cols, s.n_verts, b, x, **kw)
+                    e1.record(stream)
+                    e1.synchronize()
+                    if i >= warm:
+                        times.append(e0.elapsed_time(e1))
+                res[v] = {"ms": round(statistics.mean(times), 4), "iterations": rep["iterations"],
+                          "converged": bool(rep["converged"]), "loop_launches": rep["kernel_launches"]}
+            except sgmas.SgmasError as e:
+                res[v] = {"error": str(e)}
+            ctx.close()
+        out[name] = res
+    return out
 
 
 def run_e2e(args, ctx, s, dev, stream, head):

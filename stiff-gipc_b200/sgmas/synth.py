@@ -337,3 +337,136 @@ def hybrid_system(n_bodies=8, fem=(8, 8, 8), n_contacts=200, body_ratio=1e3, kap
     return System(n_verts=off + N, rows=mr, cols=mc, vals=mv, b=b, pos=fs.pos, tets=fs.tets,
                   pairs=np.zeros((0, 4), np.int32), raw_rows=rows, raw_cols=cols, raw_vals=vals,
                   info=dict(abd_bodies=n_bodies, fem_offset=off, fem_n=N))
+
+
+def cst_membrane(X, tris, E, nu, thickness):
+    """Linear (StVK at rest) constant-strain membrane Hessians of triangles
+    lying in the x-z plane: 9x9 per triangle, in-plane (x, z) stiffness only
+    (PSD; the out-of-plane direction is carried by the mass)."""
+    P = X[tris][:, :, [0, 2]]                         # [t, 3, 2] in-plane coordinates
+    e1, e2 = P[:, 1] - P[:, 0], P[:, 2] - P[:, 0]
+    area = 0.5 * np.abs(e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0])
+    # shape-function gradients of the 3 nodes
+    Dm = np.stack([e1, e2], 2)                        # [t, 2, 2]
+    Dinv = np.linalg.inv(Dm)
+    grads = np.zeros((len(tris), 3, 2))
+    grads[:, 1] = Dinv[:, 0, :]
+    grads[:, 2] = Dinv[:, 1, :]
+    grads[:, 0] = -grads[:, 1] - grads[:, 2]
+    # strain-displacement B [t, 3, 9] over (x, y, z) of 3 nodes; y (out of plane) unused
+    Bm = np.zeros((len(tris), 3, 9))
+    for a in range(3):
+        gx, gz = grads[:, a, 0], grads[:, a, 1]
+        Bm[:, 0, 3 * a + 0] = gx                      # eps_xx
+        Bm[:, 1, 3 * a + 2] = gz                      # eps_zz
+        Bm[:, 2, 3 * a + 0] = gz                      # gamma_xz
+        Bm[:, 2, 3 * a + 2] = gx
+    D = E / (1.0 - nu * nu) * np.array([[1.0, nu, 0.0], [nu, 1.0, 0.0], [0.0, 0.0, 0.5 * (1.0 - nu)]])
+    K = np.einsum("tij,jk,tkl->til", Bm.transpose(0, 2, 1), D, Bm) * (thickness * area)[:, None, None]
+    return K, area
+
+
+def config3(seed=0, scale=1.0, n_bodies=200, cloth_side=200, n_pairs=80000, E_body=1e10, E_cloth=1e5,
+            nu=0.3, thickness=1e-3, rho=1000.0, dt=0.01, dhat=1e-3, kappa=1e3, eps=1e-6, dmin=1e-2, chunk=8000):
+    """Stiff hybrid (config 3): affine bodies resting on a cloth sheet.
+
+    Bodies: 12-DOF affine bodies (4 block rows each, rows 0 .. 4 n_bodies,
+    before the FEM rows as SG/GIPC.cu:10082-10083 places ABD), cubes of
+    8x8x8 vertices; mass matrix int rho J^T J dV in the body's centroid
+    frame (m I3 for the translation, m s^2/12 I9 for the affine part) plus
+    dt^2 x the shape stiffness E_body * V on the symmetric part of the
+    affine map.  Cloth: cloth_side^2 vertices in the x-z plane, lumped mass,
+    constant-strain membrane (E_cloth, thickness).  Contacts: n_pairs barrier
+    pairs between a point of a body's bottom face, x = t + A xbar
+    (J = [I | xbar1 I | xbar2 I | xbar3 I]), and a cloth triangle under the
+    body: 21x21 kappa b''(d) g g^T + kappa eps I, g = [J^T n; -b_k n], with
+    d ~ U(dmin dhat, dhat) and kappa chosen (the reference adapts kappa) so
+    that cond(A) stays near 1e8-1e9.  scale shrinks the cloth side, the
+    bodies and the pairs together."""
+    rng = np.random.default_rng(seed)
+    side = max(8, int(round(cloth_side * np.sqrt(scale))))
+    nbod = max(1, int(round(n_bodies * scale)))
+    npr = int(round(n_pairs * scale))
+    hc = 0.01
+    gx, gz = np.meshgrid(np.arange(side), np.arange(side), indexing="ij")
+    Xc = np.stack([gx.ravel() * hc, np.zeros(side * side), gz.ravel() * hc], 1)
+    Xc += rng.normal(0.0, 1e-5, Xc.shape) * np.array([1.0, 0.0, 1.0])
+    vid = lambda i, k: i * side + k
+    qi, qk = np.meshgrid(np.arange(side - 1), np.arange(side - 1), indexing="ij")
+    qi, qk = qi.ravel(), qk.ravel()
+    a, b1, c1, d1 = vid(qi, qk), vid(qi + 1, qk), vid(qi, qk + 1), vid(qi + 1, qk + 1)
+    tris = np.concatenate([np.stack([a, b1, d1], 1), np.stack([a, d1, c1], 1)])
+    nc = side * side
+    off = 4 * nbod
+    K, area = cst_membrane(Xc, tris, E_cloth, nu, thickness)
+    rows, cols, vals = [], [], []
+    r_el, c_el, v_el = upper_triplets(K * dt * dt, tris + off)
+    rows.append(r_el); cols.append(c_el); vals.append(v_el)
+    mass = np.zeros(nc)
+    np.add.at(mass, tris.ravel(), np.repeat(rho * thickness * area / 3.0, 3))
+    v_m = np.zeros((nc, 9))
+    v_m[:, 0] = v_m[:, 4] = v_m[:, 8] = mass
+    rows.append(np.arange(nc) + off); cols.append(np.arange(nc) + off); vals.append(v_m)
+    # bodies: side s, centred over random cloth cells
+    s_b = 0.07
+    m_b = rho * s_b ** 3
+    Mb = np.zeros((12, 12))
+    Mb[:3, :3] = m_b * np.eye(3)
+    Mb[3:, 3:] = m_b * s_b * s_b / 12.0 * np.eye(9)
+    # shape stiffness on the symmetric part of A (9 affine dofs, A row-major in q[3:12])
+    Psym = np.zeros((9, 9))
+    for i in range(3):
+        for j in range(3):
+            Psym[3 * i + j, 3 * i + j] += 0.5
+            Psym[3 * i + j, 3 * j + i] += 0.5
+    Kb = np.zeros((12, 12))
+    Kb[3:, 3:] = 4.0 * E_body * s_b ** 3 * Psym
+    Ab = Mb + dt * dt * Kb
+    Hb = np.repeat(Ab[None], nbod, 0) * (1.0 + 0.05 * rng.uniform(-1, 1, (nbod, 1, 1)))
+    nodes_b = 4 * np.arange(nbod)[:, None] + np.arange(4)[None, :]
+    rb, cb, vb = upper_triplets(Hb, nodes_b)
+    rows.append(rb); cols.append(cb); vals.append(vb)
+    foot = int(round(s_b / hc))                      # footprint in cells
+    cx = rng.integers(0, max(1, side - 1 - foot), nbod)
+    cz = rng.integers(0, max(1, side - 1 - foot), nbod)
+    # contacts, in chunks (21x21 blocks)
+    done = 0
+    while done < npr:
+        m = min(chunk, npr - done)
+        bod = rng.integers(0, nbod, m)
+        ti = cx[bod] + rng.integers(0, foot, m)
+        tk = cz[bod] + rng.integers(0, foot, m)
+        which = rng.integers(0, 2, m)
+        qid = ti * (side - 1) + tk
+        tri = tris[which * (side - 1) * (side - 1) + qid]
+        xbar = np.stack([rng.uniform(-0.5, 0.5, m) * s_b, np.full(m, -0.5 * s_b), rng.uniform(-0.5, 0.5, m) * s_b], 1)
+        J = np.zeros((m, 3, 12))
+        J[:, :, 0:3] = np.eye(3)
+        for k in range(3):
+            J[:, :, 3 + 3 * k:6 + 3 * k] = xbar[:, k, None, None] * np.eye(3)[None]
+        nrm = np.tile([0.0, 1.0, 0.0], (m, 1)) + rng.normal(0.0, 0.05, (m, 3))
+        nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+        bary = rng.dirichlet(np.ones(3), m)
+        d = np.maximum(rng.uniform(0.0, dhat, m), dhat * dmin)
+        bpp = (-2.0 * np.log(d / dhat) - 4.0 * (d - dhat) / d + (d - dhat) ** 2 / d ** 2)
+        g = np.concatenate([np.einsum("pij,pi->pj", J, nrm), -bary[:, 0:1] * nrm, -bary[:, 1:2] * nrm,
+                            -bary[:, 2:3] * nrm], 1)
+        H = (kappa * bpp)[:, None, None] * g[:, :, None] * g[:, None, :] + kappa * eps * np.eye(21)[None]
+        H *= dt * dt
+        nodes = np.concatenate([4 * bod[:, None] + np.arange(4)[None, :], tri + off], 1)
+        r_c, c_c, v_c = upper_triplets(H, nodes)
+        rows.append(r_c); cols.append(c_c); vals.append(v_c)
+        done += m
+    raw_r = np.concatenate(rows).astype(np.int64)
+    raw_c = np.concatenate(cols).astype(np.int64)
+    raw_v = np.concatenate(vals)
+    mr, mc, mv = merge_triplets(raw_r, raw_c, raw_v)
+    n = off + nc
+    grav = np.zeros((n, 3))
+    grav[:off:4, 1] = -9.8 * m_b * dt                 # body translation rows
+    grav[off:, 1] = -9.8 * mass * dt
+    b = grav.ravel() + rng.normal(0.0, 1e-6, 3 * n)
+    return System(n_verts=n, rows=mr, cols=mc, vals=mv, b=b, pos=Xc, tets=np.zeros((0, 4), np.int32),
+                  pairs=np.zeros((0, 4), np.int32),
+                  info=dict(abd_bodies=nbod, fem_offset=off, fem_n=nc, tris=tris.astype(np.int32),
+                            n_pairs=npr, n_blocks=len(mr), side=side, dt=dt))
