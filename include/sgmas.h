@@ -80,11 +80,30 @@ typedef struct {
     int n_block_rows;       /* block rows = DOF / 3 */
 } sgmas_bcoo;
 
+/* ---- MatrixMarket boundary (host only, no context, no GPU) --------------
+ * The files GlobalLinearSystem::export_matrix_market_files writes
+ * (SG/linear_system/linear_system/global_linear_system.cu:98-261): A as a
+ * general coordinate real matrix with every stored block expanded to both
+ * triangles ("%d %d %.17g", 1-based), b as an M x 1 real array.
+ * sgmas_mtx_write writes exactly that from a host BCOO (values 9 doubles
+ * column-major per upper block); path_b may be NULL.
+ * sgmas_mtx_read reads such files (or symmetric ones) back into an upper,
+ * (row, col)-sorted BCOO with duplicates summed in file order, as
+ * read_mm_coordinate_real + to_upper_triangle_block_triplets do
+ * (SG/main.cu:398-646); a missing diagonal block is an error.  It sets
+ * *n_blocks / *n_block_rows first and returns SGMAS_ERR_CAPACITY (nothing
+ * copied) when the arrays are NULL or too small: call once to size, once to
+ * read.  path_b may be NULL.  Failures: sgmas_last_error(NULL). */
+int sgmas_mtx_write(const char* path_A, const char* path_b, const double* values, const int* rows,
+                    const int* cols, int n_blocks, int n_block_rows, const double* b);
+int sgmas_mtx_read(const char* path_A, const char* path_b, double* values, int* rows, int* cols,
+                   int cap_blocks, double* b, int cap_b, int* n_blocks, int* n_block_rows);
+
 /* ---- context ---------------------------------------------------------- */
 int sgmas_create(const sgmas_config* cfg, sgmas_context** out);
 /* MASPreconditioner::FreeMAS (SG/MASPreconditioner.cu:2321-2350) + release */
 void sgmas_destroy(sgmas_context* ctx);
-const char* sgmas_last_error(const sgmas_context* ctx);
+const char* sgmas_last_error(const sgmas_context* ctx);  /* NULL: this thread's last context-free call */
 /* the reference runs on the per-thread default stream (CMakeLists.txt:101);
  * a new context uses a stream of its own; NULL selects the legacy default
  * stream, as everywhere in the CUDA runtime */

@@ -12,6 +12,9 @@
 
 using namespace sgmas;
 
+// message of the last failed call of this thread that had no context
+static thread_local std::string g_host_err = "no error";
+
 int ctx_fail(sgmas_context* c, int code, const char* fmt, ...) {
     char buf[1024];
     va_list ap;
@@ -19,6 +22,7 @@ int ctx_fail(sgmas_context* c, int code, const char* fmt, ...) {
     vsnprintf(buf, sizeof(buf), fmt, ap);
     va_end(ap);
     if (c) c->err = buf;
+    else g_host_err = buf;
     return code;
 }
 
@@ -132,7 +136,7 @@ void sgmas_destroy(sgmas_context* c) {
     delete c;
 }
 
-const char* sgmas_last_error(const sgmas_context* c) { return c ? c->err.c_str() : "null context"; }
+const char* sgmas_last_error(const sgmas_context* c) { return c ? c->err.c_str() : g_host_err.c_str(); }
 
 int sgmas_set_stream(sgmas_context* c, void* stream) {
     if (!c) return SGMAS_ERR_ARG;

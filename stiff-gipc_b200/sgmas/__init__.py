@@ -56,6 +56,7 @@ EXPORTS = [
     "sgmas_pcg_solve", "sgmas_pcg_solve_host", "sgmas_spmv", "sgmas_convert", "sgmas_write_upper_blocks",
     "sgmas_morton_codes", "sgmas_morton_partition", "sgmas_pcg_profile", "sgmas_vert_neighbors",
     "sgmas_part_maps", "sgmas_morton_codes_noalloc", "sgmas_set_pcg_mode", "sgmas_pcg_last_vectors",
+    "sgmas_mtx_write", "sgmas_mtx_read",
 ]
 
 MORTON_NOALLOC_MAX_VERTS = 2097152  # SGMAS_MORTON_NOALLOC_MAX_VERTS in include/sgmas.h
@@ -100,6 +101,8 @@ def lib(build_if_missing: bool = False):
     L.sgmas_morton_codes_noalloc.argtypes = [vp, i, vp, vp, vp]
     L.sgmas_set_pcg_mode.argtypes = [vp, i]
     L.sgmas_pcg_last_vectors.argtypes = [vp, vp, vp]
+    L.sgmas_mtx_write.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, i, vp]
+    L.sgmas_mtx_read.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, vp, i, C.POINTER(i), C.POINTER(i)]
     _lib = L
     return L
 
@@ -113,6 +116,35 @@ def morton_codes_noalloc(pos, codes, aabb=None, stream=None, n=None):
     box = None if aabb is None else _h(aabb, np.float64)
     count = int(pos.shape[0]) if n is None else n
     return lib().sgmas_morton_codes_noalloc(_ptr(pos), count, _ptr(box), _ptr(codes), stream)
+
+
+def mtx_write(path_A, vals, rows, cols, n_block_rows, b=None, path_b=None):
+    """Write a host BCOO (and b) in the reference's MatrixMarket export format."""
+    vals, rows, cols = _h(vals, np.float64), _h(rows, np.int32), _h(cols, np.int32)
+    bb = None if b is None else _h(b, np.float64)
+    rc = lib().sgmas_mtx_write(str(path_A).encode(), None if path_b is None else str(path_b).encode(), _ptr(vals),
+                               _ptr(rows), _ptr(cols), len(rows), n_block_rows, _ptr(bb))
+    if rc != 0:
+        raise SgmasError(rc, lib().sgmas_last_error(None).decode())
+
+
+def mtx_read(path_A, path_b=None):
+    """Read MatrixMarket A (and b) into an upper sorted BCOO: (vals, rows, cols, n_block_rows, b)."""
+    L = lib()
+    nb, nr = C.c_int(), C.c_int()
+    pa, pb = str(path_A).encode(), None if path_b is None else str(path_b).encode()
+    rc = L.sgmas_mtx_read(pa, pb, None, None, None, 0, None, 0, C.byref(nb), C.byref(nr))
+    if rc not in (0, -4):
+        raise SgmasError(rc, L.sgmas_last_error(None).decode())
+    vals = np.zeros((nb.value, 9))
+    rows = np.zeros(nb.value, np.int32)
+    cols = np.zeros(nb.value, np.int32)
+    b = np.zeros(3 * nr.value) if path_b is not None else None
+    rc = L.sgmas_mtx_read(pa, pb, _ptr(vals), _ptr(rows), _ptr(cols), nb.value, _ptr(b), 0 if b is None else len(b),
+                          C.byref(nb), C.byref(nr))
+    if rc != 0:
+        raise SgmasError(rc, L.sgmas_last_error(None).decode())
+    return vals, rows, cols, nr.value, b
 
 
 def vert_neighbors(tets, n_verts, tris=None, abd_vert_offset=0):
