@@ -120,6 +120,8 @@ struct sgmas_context {
     size_t stamps_cap = 0;
     int* d_l1_bank = nullptr;             // level-0 bank of each level-1 node (persistent ownership)
     int l1_bank_cap = 0;
+    int* d_own1 = nullptr;                // first level-1 bank of each CTA of the persistent kernel
+    int own1_cap = 0;
     int partial_cap = 0;
     PcgState* d_state = nullptr;
     // uploaded host systems (sgmas_pcg_solve_host)

@@ -5,9 +5,10 @@
 //
 // Ownership.  Level-1 nodes of the MAS hierarchy are numbered in level-0 bank
 // order (component ids are an exclusive scan over the banks), so a range of
-// level-1 banks is fed by a range of level-0 banks.  CTA c owns level-1 banks
-// [c k1, (c+1) k1) and processes every level-0 bank whose components fall in
-// them (a bank split between two CTAs is processed by both; each vertex
+// level-1 banks is fed by a range of level-0 banks.  CTA c owns a contiguous
+// range of level-1 banks (chosen on the host so that the largest number of
+// level-0 banks any CTA processes is as small as possible) and processes
+// every level-0 bank whose components fall in them (a bank split between two CTAs is processed by both; each vertex
 // belongs to the CTA that owns its level-1 node).  Level 0, level 1 and the
 // push of level-1 residuals into level 2 then need no grid-wide step; the few
 // nodes of levels >= 2 are processed redundantly by every CTA in shared
@@ -32,6 +33,7 @@
 //    sums in lane order, Schwarz columns ascending, collect in level order),
 //    so z is bit-identical to sgmas_mas_apply.
 #include <algorithm>
+#include <vector>
 
 #include "../../include/sgmas.h"
 #include "ctx.hpp"
@@ -56,11 +58,13 @@ struct PArgs {
     const int *part_map, *going_next, *coarse_table;
     const unsigned* fine_mask;
     const int* l1_bank;  // level-0 bank of each level-1 node
+    const int* own1;     // [grid + 1]: CTA c owns level-1 banks [own1[c], own1[c + 1])
     const void* inv;
     void* R;             // level-2 residual pushes (Acc, global node ids)
     int k0, k1, nb0, nb1;  // level-0 banks per CTA (max), level-1 banks per CTA, bank counts
     int nc;                // nodes of levels >= 2 (a multiple of B)
     int capc;              // tiles of levels >= 2 a CTA holds in shared memory (<= kPT / B)
+    int upw;               // SpMV unit descriptors cached per warp in shared memory
     ExtraRows ex;          // rows outside the MAS range (bodies, other rows); MAS vertex v is row ex.fem_off + v
     // block-Jacobi
     const double* dinv;
@@ -134,6 +138,36 @@ __device__ __forceinline__ double sum_partials(const double* part, double* sh) {
     return v;
 }
 
+// both sums of the end of an iteration in one pass
+__device__ __forceinline__ void sum_partials2(const double* pa, const double* pb, double* sh, double& va,
+                                              double& vb) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += kPT) { s0 += pa[i]; s1 += pb[i]; }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_down_sync(0xffffffffu, s0, o);
+        s1 += __shfl_down_sync(0xffffffffu, s1, o);
+    }
+    __shared__ double out2[2];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sh[w] = s0; sh[16 + w] = s1; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double r0 = threadIdx.x < kPT / 32 ? sh[threadIdx.x] : 0.0;
+        double r1 = threadIdx.x < kPT / 32 ? sh[16 + threadIdx.x] : 0.0;
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            r0 += __shfl_down_sync(0xffffffffu, r0, o);
+            r1 += __shfl_down_sync(0xffffffffu, r1, o);
+        }
+        if (threadIdx.x == 0) { out2[0] = r0; out2[1] = r1; }
+    }
+    __syncthreads();
+    va = out2[0];
+    vb = out2[1];
+    __syncthreads();
+}
+
 // ---- block-Jacobi tail (z = D^-1 r with 3x3 inverses) ----------------------
 __device__ void phase_jacobi(const PArgs& a, int mode, double alpha, const double* pcur, double* part_rz,
                              double* part_rr, double* sh) {
@@ -182,8 +216,8 @@ __device__ __forceinline__ Own own_ranges(const PArgs& a) {
     Own o;
     if (a.L >= 2) {
         const int cnt1 = a.lvl_count[1];
-        o.j0 = blockIdx.x * a.k1;
-        const int j1 = min(o.j0 + a.k1, a.nb1);
+        o.j0 = a.own1[blockIdx.x];
+        const int j1 = a.own1[blockIdx.x + 1];
         o.nbk1 = max(0, j1 - o.j0);
         const int n_lo = o.j0 * B, n_hi = min(j1 * B, cnt1) - 1;
         if (n_lo <= n_hi) {
@@ -330,6 +364,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     Acc* Rc = Z1s + 3 * (size_t)a.k1 * B;
     Acc* Zc = Rc + 3 * (size_t)a.nc;
     int* parc = reinterpret_cast<int*>(Zc + 3 * (size_t)a.nc);
+    // SpMV unit descriptors: [warp][unit of the warp][lane group of 8]
+    int4* udesc = reinterpret_cast<int4*>(smem_raw + (((size_t)(reinterpret_cast<unsigned char*>(parc + a.nc) -
+                                                                smem_raw) + 15) & ~(size_t)15));
     if (a.stamps && blockIdx.x == 0 && threadIdx.x == 0) a.stamps[0] = clock64();
     unsigned epoch = 0u, mphase = 0u;
     double* part_pap = a.partials;
@@ -486,6 +523,17 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         if (threadIdx.x == 0) { part_rz[blockIdx.x] = rz; part_rr[blockIdx.x] = rr; }
     };
 
+    // ---- SpMV unit descriptors of this CTA's warps (fixed for the solve)
+    {
+        const int w = threadIdx.x / 32, lane32 = threadIdx.x & 31;
+        const int gw = blockIdx.x * (kPT / 32) + w;
+        for (int i = 0; i < a.upw; ++i) {
+            const int u = gw + i * (int)gridDim.x * (kPT / 32);
+            int4 d = {-1, 0, 0, 0};
+            if (u < a.units) d = unit_desc(a.A, u, lane32);
+            if ((lane32 & 7) == 0) udesc[(w * a.upw + i) * 4 + (lane32 >> 3)] = d;
+        }
+    }
     // ---- prologue: x = 0, r = b, p_old = 0, z = M^-1 r, r.z, r.r
     for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT) {
         a.p0[i] = 0.0;
@@ -525,8 +573,11 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         // A: p_new = z + beta p_old, Ap = A p_new, p.Ap
         stamp(a, k, 0);
         double dot = 0.0;
-        for (int u = gw0; u < a.units; u += gridDim.x * warps)
-            dot += spmv_unit<1, true>(a.A, u, threadIdx.x & 31, a.z, pold, pnew, a.Ap, nullptr, 1.0, 0.0, beta);
+        const int4* ud = udesc + (threadIdx.x / 32) * a.upw * 4 + ((threadIdx.x & 31) >> 3);
+        for (int u = gw0, i = 0; u < a.units; u += gridDim.x * warps, ++i) {
+            const int4 d = i < a.upw ? ud[4 * i] : unit_desc(a.A, u, threadIdx.x & 31);
+            dot += spmv_unit_d<1, true>(a.A, d, threadIdx.x & 31, a.z, pold, pnew, a.Ap, nullptr, 1.0, 0.0, beta);
+        }
         dot = block_sum<kPT>(dot, sh);
         if (threadIdx.x == 0) part_pap[blockIdx.x] = dot;
         if (!grid_barrier(a.sync, epoch, a.err, SLOT(0))) { ok = false; break; }
@@ -556,8 +607,11 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                     a.x[i] = a.x[i] + alpha * pnew[i];
             }
             if (!grid_barrier(a.sync, epoch, a.err, SLOT(1))) { ok = false; break; }
-            for (int u = gw0; u < a.units; u += gridDim.x * warps)
-                spmv_unit<2, true>(a.A, u, threadIdx.x & 31, a.x, nullptr, nullptr, a.r, a.b, 1.0, 0.0, 0.0);
+            const int4* ud = udesc + (threadIdx.x / 32) * a.upw * 4 + ((threadIdx.x & 31) >> 3);
+            for (int u = gw0, i = 0; u < a.units; u += gridDim.x * warps, ++i) {
+                const int4 d = i < a.upw ? ud[4 * i] : unit_desc(a.A, u, threadIdx.x & 31);
+                spmv_unit_d<2, true>(a.A, d, threadIdx.x & 31, a.x, nullptr, nullptr, a.r, a.b, 1.0, 0.0, 0.0);
+            }
             if (!grid_barrier(a.sync, epoch, a.err, SLOT(2))) { ok = false; break; }
             if (mas && v >= 0) { r0 = a.r[vo]; r1 = a.r[vo + 1]; r2 = a.r[vo + 2]; }
         } else if (mas && v >= 0) {
@@ -578,8 +632,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         }
         if (!grid_barrier(a.sync, epoch, a.err, SLOT(5)) || !ok) { ok = false; break; }
         stamp(a, k, 5);
-        const double rz_new = sum_partials(part_rz, sh);
-        const double rr = sum_partials(part_rr, sh);
+        double rz_new, rr;
+        sum_partials2(part_rz, part_rr, sh, rz_new, rr);
         bool conv = false;
         if (k % a.check_every == 0) {
             rr_last = rr;
@@ -629,16 +683,6 @@ __global__ void k_l1_bank(int Mm, int l1_begin, const int* __restrict__ part_map
     if (v >= 0) l1_bank[going_next[v] - l1_begin] = s / B;
 }
 
-// largest number of level-0 banks any CTA processes
-template <int B>
-__global__ void k_cta_span(int G, int k1, int nb1, int cnt1, const int* __restrict__ l1_bank, unsigned* out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= G) return;
-    const int j0 = c * k1, j1 = min(j0 + k1, nb1);
-    const int n_lo = j0 * B, n_hi = min(j1 * B, cnt1) - 1;
-    if (n_lo <= n_hi) atomicMax(out, (unsigned)(l1_bank[n_hi] - l1_bank[n_lo] + 1));
-}
-
 template <int B, typename S, typename Acc>
 int launch_t(sgmas_context* c, PArgs& a, float* ms) {
     int dev_sms = 0;
@@ -656,20 +700,56 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
         a.nb0 = a.Mm / B;
         if (a.L >= 2) {
             a.nb1 = (a.lvl_count[1] + B - 1) / B;
-            a.k1 = (a.nb1 + G - 1) / G;
-            // level-0 banks per CTA follow the level-1 ranges
             if (ctx_alloc_grow(c, &c->d_l1_bank, &c->l1_bank_cap, a.lvl_count[1])) return SGMAS_ERR_CUDA;
+            if (ctx_alloc_grow(c, &c->d_own1, &c->own1_cap, G + 1)) return SGMAS_ERR_CUDA;
             a.l1_bank = c->d_l1_bank;
+            a.own1 = c->d_own1;
             k_l1_bank<B><<<(a.Mm + 255) / 256, 256, 0, c->stream>>>(a.Mm, a.lvl_begin[1], a.part_map, a.going_next,
                                                                  c->d_l1_bank);
-            SG_CUDA(c, cudaMemsetAsync(c->d_psync + 4, 0, sizeof(unsigned), c->stream));
-            k_cta_span<B><<<(G + 127) / 128, 128, 0, c->stream>>>(G, a.k1, a.nb1, a.lvl_count[1], c->d_l1_bank,
-                                                                c->d_psync + 4);
-            c->build_launches += 2;
-            unsigned span = 0;
-            SG_CUDA(c, cudaMemcpyAsync(&span, c->d_psync + 4, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+            c->build_launches += 1;
+            // level-0 span of every level-1 bank, then contiguous CTA ranges of level-1 banks whose
+            // largest level-0 span is minimal (binary search on that span, greedy fill)
+            std::vector<int> l1b(a.lvl_count[1]);
+            SG_CUDA(c, cudaMemcpyAsync(l1b.data(), c->d_l1_bank, sizeof(int) * l1b.size(), cudaMemcpyDeviceToHost,
+                                       c->stream));
             SG_CUDA(c, cudaStreamSynchronize(c->stream));
-            a.k0 = (int)span;
+            const int cnt1 = a.lvl_count[1], nb1 = a.nb1;
+            auto first0 = [&](int j) { return l1b[(size_t)j * B]; };
+            auto last0 = [&](int j) { return l1b[std::min((size_t)j * B + B - 1, (size_t)cnt1 - 1)]; };
+            auto groups_for = [&](int M, std::vector<int>* starts) {  // CTAs needed with span <= M
+                int n = 0, j = 0;
+                while (j < nb1) {
+                    if (starts) starts->push_back(j);
+                    const int lo = first0(j);
+                    int e = j + 1;
+                    while (e < nb1 && e - j < kPT / B && last0(e) - lo + 1 <= M) ++e;
+                    j = e;
+                    ++n;
+                }
+                return n;
+            };
+            int lo_m = 1, hi_m = std::max(1, last0(nb1 - 1) - first0(0) + 1);
+            for (int j = 0; j < nb1; ++j) lo_m = std::max(lo_m, last0(j) - first0(j) + 1);
+            while (lo_m < hi_m) {
+                const int mid = (lo_m + hi_m) / 2;
+                if (groups_for(mid, nullptr) <= G) hi_m = mid;
+                else lo_m = mid + 1;
+            }
+            std::vector<int> starts;
+            groups_for(lo_m, &starts);
+            std::vector<int> own(G + 1, nb1);
+            for (size_t g = 0; g < starts.size() && g < (size_t)G; ++g) own[g] = starts[g];
+            a.k0 = 0;
+            a.k1 = 0;
+            for (int g = 0; g < G; ++g) {
+                const int j0 = own[g], j1 = own[g + 1];
+                if (j1 <= j0) continue;
+                a.k1 = std::max(a.k1, j1 - j0);
+                a.k0 = std::max(a.k0, last0(j1 - 1) - first0(j0) + 1);
+            }
+            SG_CUDA(c, cudaMemcpyAsync(c->d_own1, own.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice,
+                                       c->stream));
+            SG_CUDA(c, cudaStreamSynchronize(c->stream));  // own is a host temporary
         } else {
             a.nb1 = 0;
             a.k1 = 0;
@@ -689,6 +769,15 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
         smem = fixed + (size_t)a.capc * tb;
     } else {
         a.k0 = a.k1 = a.nb0 = a.nb1 = a.nc = a.capc = 0;
+    }
+    // SpMV unit descriptors (16 B per warp, unit and lane group), as many as fit, at most 16 units per warp
+    {
+        const int per_warp = (a.units + G * (kPT / 32) - 1) / (G * (kPT / 32));
+        smem = (smem + 15) & ~(size_t)15;
+        const size_t per_unit = (size_t)(kPT / 32) * 4 * sizeof(int4);
+        const size_t room = budget > smem ? (budget - smem) / per_unit : 0;
+        a.upw = (int)std::min<size_t>({(size_t)per_warp, (size_t)16, room});
+        smem += (size_t)a.upw * per_unit;
     }
     auto kern = k_pcg_persistent<B, S, Acc>;
     SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));

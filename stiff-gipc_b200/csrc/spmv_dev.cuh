@@ -26,30 +26,50 @@ __device__ __forceinline__ double ldv(const double* p) {
     return *p;
 }
 
+// The block range of this lane's row in work unit gw: {row (-1: none), begin,
+// end, 1 for a whole-warp (long) row}.  Fixed for a given matrix.
+__device__ __forceinline__ int4 unit_desc(const BsrView& A, int gw, int lane) {
+    int4 d = {-1, 0, 0, 0};
+    if (gw < A.n_long) {
+        d.x = A.row_list[gw];
+        d.w = 1;
+    } else {
+        const int g = (gw - A.n_long) * 4 + (lane >> 3);
+        if (g < A.nrows - A.n_long) d.x = A.row_list[A.n_long + g];
+    }
+    if (d.x >= 0) {
+        d.y = A.row_ptr[d.x];
+        d.z = A.row_ptr[d.x + 1];
+    }
+    return d;
+}
+
+template <int MODE, bool LIVE = false>
+__device__ __forceinline__ double spmv_unit_d(const BsrView& A, int4 desc, int lane, const double* __restrict__ xin,
+                                              const double* __restrict__ pold, double* pnew, double* y,
+                                              const double* __restrict__ rhs, double a, double b, double beta);
+
 template <int MODE, bool LIVE = false>
 __device__ __forceinline__ double spmv_unit(const BsrView& A, int gw, int lane, const double* __restrict__ xin,
                                             const double* __restrict__ pold, double* pnew, double* y,
                                             const double* __restrict__ rhs, double a, double b, double beta) {
-    const int* __restrict__ row_ptr = A.row_ptr;
+    return spmv_unit_d<MODE, LIVE>(A, unit_desc(A, gw, lane), lane, xin, pold, pnew, y, rhs, a, b, beta);
+}
+
+// One work unit given its descriptor (unit_desc); desc.w is warp-uniform.
+template <int MODE, bool LIVE>
+__device__ __forceinline__ double spmv_unit_d(const BsrView& A, int4 desc, int lane, const double* __restrict__ xin,
+                                              const double* __restrict__ pold, double* pnew, double* y,
+                                              const double* __restrict__ rhs, double a, double b, double beta) {
     const int* __restrict__ bcols = A.cols;
     const double* __restrict__ bvals = A.vals;
     const long long cap = A.cap;
-    const bool longw = gw < A.n_long;
-    int row = -1, l, G;
-    if (longw) {
-        row = A.row_list[gw];
-        l = lane;
-        G = 32;
-    } else {
-        const int g = (gw - A.n_long) * 4 + (lane >> 3);
-        if (g < A.nrows - A.n_long) row = A.row_list[A.n_long + g];
-        l = lane & 7;
-        G = 8;
-    }
+    const bool longw = desc.w != 0;
+    const int row = desc.x, l = longw ? lane : (lane & 7), G = longw ? 32 : 8;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     double dot = 0.0;
     {
-        const int beg = row >= 0 ? row_ptr[row] : 0, end = row >= 0 ? row_ptr[row + 1] : 0;
+        const int beg = desc.y, end = desc.z;
         for (int p = beg + 2 * l; p < end; p += 2 * G) {
             const int2 cc = *reinterpret_cast<const int2*>(bcols + p);
             double2 v[9];
