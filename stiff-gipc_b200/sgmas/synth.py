@@ -470,3 +470,111 @@ def config3(seed=0, scale=1.0, n_bodies=200, cloth_side=200, n_pairs=80000, E_bo
                   pairs=np.zeros((0, 4), np.int32),
                   info=dict(abd_bodies=nbod, fem_offset=off, fem_n=nc, tris=tris.astype(np.int32),
                             n_pairs=npr, n_blocks=len(mr), side=side, dt=dt))
+
+
+def stencil_grid_system(nx, ny, nz, h=0.01, E=1e5, nu=0.4, rho=1000.0, dt=0.01, n_pairs=0, dhat=1e-3,
+                        kappa=1e5, eps=1e-6, seed=0):
+    """A tet grid system assembled directly in merged (stencil) form.
+
+    The grid is regular, so each of the 6 tets of a cube has the same
+    rest-state stiffness (the Neo-Hookean Hessian at F = I, PSD-projected):
+    each tet type's 3x3 blocks are added into per-offset block arrays by
+    slicing, and the sorted upper BCOO is read off the stencil -- no element
+    loop, no triplet sort (used for the many large systems of config 5).
+    n_pairs barrier pairs couple top-face points to nearby top-face
+    triangles (12x12 blocks, merged in), with their reference int4 encoding."""
+    rng = np.random.default_rng(seed)
+    # one cube's 6 tets at rest
+    Xc, tc = tet_grid(2, 2, 2, h)
+    He, _, vol = neo_hookean_elements(Xc, Xc, tc, E, nu)
+    He = He * dt * dt
+    n = nx * ny * nz
+    strides = np.array([1, nx, nx * ny])
+    cub = (nx - 1, ny - 1, nz - 1)
+    blocks = {}   # offset delta >= 0 -> [nz, ny, nx, 3, 3] (row vertex grid)
+
+    def add(delta, dr, blk):
+        a = blocks.setdefault(delta, np.zeros((nz, ny, nx, 3, 3)))
+        a[dr[2]:dr[2] + cub[2], dr[1]:dr[1] + cub[1], dr[0]:dr[0] + cub[0]] += blk
+
+    for t in range(6):
+        cs = _TET_SPLIT[t]
+        for ii in range(4):
+            for jj in range(ii, 4):
+                da, db = _CORNER[cs[ii]], _CORNER[cs[jj]]
+                va, vb = int(da @ strides), int(db @ strides)
+                B = He[t, 3 * ii:3 * ii + 3, 3 * jj:3 * jj + 3]
+                if va <= vb:
+                    add(vb - va, da, B if va != vb else B)
+                else:
+                    add(va - vb, db, B.T)
+    # lumped mass on the diagonal
+    m_cube = rho * vol.sum() / 4.0   # each tet gives vol/4 to each of its 4 vertices
+    mass = np.zeros((nz, ny, nx))
+    for t in range(6):
+        for ii in range(4):
+            d = _CORNER[_TET_SPLIT[t][ii]]
+            mass[d[2]:d[2] + cub[2], d[1]:d[1] + cub[1], d[0]:d[0] + cub[0]] += rho * vol[t] / 4.0
+    del m_cube
+    blocks[0] = blocks[0] + mass[..., None, None] * np.eye(3)
+    # read the upper BCOO off the stencil: rows ascending, then offsets ascending
+    deltas = sorted(blocks)
+    vidx = np.arange(n)
+    rows, cols, vals = [], [], []
+    touched = {d: np.abs(blocks[d]).reshape(n, 9).max(1) > 0 for d in deltas}
+    for d in deltas:
+        ok = touched[d]
+        rows.append(vidx[ok])
+        cols.append(vidx[ok] + d)
+        vals.append(np.swapaxes(blocks[d].reshape(n, 3, 3)[ok], 1, 2).reshape(-1, 9))  # column-major
+    r = np.concatenate(rows); c = np.concatenate(cols); v = np.concatenate(vals)
+    order = np.lexsort((c, r))
+    r, c, v = r[order], c[order], v[order]
+    X = tet_grid(nx, ny, nz, h)[0]
+    pairs = np.zeros((0, 4), np.int32)
+    if n_pairs > 0:
+        # top face (y = ny - 1): points against triangles of nearby quads
+        gx, gz = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+        top = lambda x_, z_: x_ + nx * ((ny - 1) + ny * z_)
+        pi = rng.integers(0, nx * nz, n_pairs)
+        px, pz = gx.ravel()[pi], gz.ravel()[pi]
+        qx = np.clip(px + rng.integers(-2, 2, n_pairs), 0, nx - 2)
+        qz = np.clip(pz + rng.integers(-2, 2, n_pairs), 0, nz - 2)
+        a0, b0, c0, d0 = top(qx, qz), top(qx + 1, qz), top(qx, qz + 1), top(qx + 1, qz + 1)
+        w = rng.integers(0, 2, n_pairs)
+        tri = np.where(w[:, None] == 0, np.stack([a0, b0, d0], 1), np.stack([a0, d0, c0], 1))
+        pt = top(px, pz)
+        keep = (pt != tri[:, 0]) & (pt != tri[:, 1]) & (pt != tri[:, 2])
+        pt, tri = pt[keep], tri[keep]
+        m = len(pt)
+        d_ = np.maximum(rng.uniform(0.0, dhat, m), dhat * 1e-2)
+        normal = np.tile([0.0, 1.0, 0.0], (m, 1)) + rng.normal(0.0, 0.05, (m, 3))
+        normal /= np.linalg.norm(normal, axis=1, keepdims=True)
+        bary = rng.dirichlet(np.ones(3), m)
+        Hc = barrier_hessian(d_, dhat, kappa, eps, normal, bary, rng) * dt * dt
+        nodes = np.stack([pt, tri[:, 0], tri[:, 1], tri[:, 2]], 1)
+        r_c, c_c, v_c = upper_triplets(Hc, nodes)
+        r, c, v = merge_triplets(np.concatenate([r, r_c]), np.concatenate([c, c_c]), np.concatenate([v, v_c]))
+        pairs = np.stack([-(nodes[:, 0] + 1), nodes[:, 1], nodes[:, 2], nodes[:, 3]], 1).astype(np.int32)
+    b = rng.normal(0.0, 1.0, 3 * n) * float(np.median(v[r == c][:, 0])) * 1e-3
+    _, tets = tet_grid(nx, ny, nz, h)
+    return System(n_verts=n, rows=r.astype(np.int32), cols=c.astype(np.int32), vals=v, b=b, pos=X,
+                  tets=tets.astype(np.int32), pairs=pairs,
+                  info=dict(nx=nx, ny=ny, nz=nz, E=E, n_pairs=len(pairs), n_blocks=len(r)))
+
+
+def config5(seed=0, n_scenes=64, nmin=2000, nmax=200000, scale=1.0):
+    """Batched serving of uneven scenes (config 5): n_scenes tet grids with
+    vertex counts log-uniform in [nmin, nmax] * scale, E log-uniform in
+    [1e4, 1e8], barrier pairs 0 to 20 % of the vertices."""
+    rng = np.random.default_rng(seed)
+    scenes = []
+    for k in range(n_scenes):
+        N = float(np.exp(rng.uniform(np.log(nmin * scale), np.log(nmax * scale))))
+        # box with aspect 2:1:1
+        side = (N / 2.0) ** (1.0 / 3.0)
+        nx, ny, nz = max(3, int(round(2 * side))), max(3, int(round(side))), max(3, int(round(side)))
+        E = float(np.exp(rng.uniform(np.log(1e4), np.log(1e8))))
+        npairs = int(rng.uniform(0.0, 0.2) * nx * ny * nz)
+        scenes.append(stencil_grid_system(nx, ny, nz, E=E, n_pairs=min(npairs, 4 * nx * nz), seed=seed * 1000 + k))
+    return scenes
