@@ -446,7 +446,7 @@ static BsrView bsr_view(const BsrMatrix& B) {
     return BsrView{B.row_ptr, B.cols, B.vals, B.cap, B.row_list, B.nrows, B.n_long};
 }
 static int spmv_grid(const BsrMatrix& B) {
-    const int warps = B.n_long + (B.nrows - B.n_long + 3) / 4;
+    const int warps = spmv_units(B.n_long, B.nrows);
     return (warps + kT / 32 - 1) / (kT / 32);
 }
 

@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             const int u = gw + i * (int)gridDim.x * (kPT / 32);
             int4 d = {-1, 0, 0, 0};
             if (u < a.units) d = unit_desc(a.A, u, lane32);
-            if ((lane32 & 7) == 0) udesc[(w * a.upw + i) * 4 + (lane32 >> 3)] = d;
+            if (lane32 % kRowLanes == 0) udesc[(w * a.upw + i) * kRowGroups + lane32 / kRowLanes] = d;
         }
     }
     // ---- prologue: x = 0, r = b, p_old = 0, z = M^-1 r, r.z, r.r
@@ -573,9 +573,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         // A: p_new = z + beta p_old, Ap = A p_new, p.Ap
         stamp(a, k, 0);
         double dot = 0.0;
-        const int4* ud = udesc + (threadIdx.x / 32) * a.upw * 4 + ((threadIdx.x & 31) >> 3);
+        const int4* ud = udesc + (threadIdx.x / 32) * a.upw * kRowGroups + (threadIdx.x & 31) / kRowLanes;
         for (int u = gw0, i = 0; u < a.units; u += gridDim.x * warps, ++i) {
-            const int4 d = i < a.upw ? ud[4 * i] : unit_desc(a.A, u, threadIdx.x & 31);
+            const int4 d = i < a.upw ? ud[kRowGroups * i] : unit_desc(a.A, u, threadIdx.x & 31);
             dot += spmv_unit_d<1, true>(a.A, d, threadIdx.x & 31, a.z, pold, pnew, a.Ap, nullptr, 1.0, 0.0, beta);
         }
         dot = block_sum<kPT>(dot, sh);
@@ -607,9 +607,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                     a.x[i] = a.x[i] + alpha * pnew[i];
             }
             if (!grid_barrier(a.sync, epoch, a.err, SLOT(1))) { ok = false; break; }
-            const int4* ud = udesc + (threadIdx.x / 32) * a.upw * 4 + ((threadIdx.x & 31) >> 3);
+            const int4* ud = udesc + (threadIdx.x / 32) * a.upw * kRowGroups + (threadIdx.x & 31) / kRowLanes;
             for (int u = gw0, i = 0; u < a.units; u += gridDim.x * warps, ++i) {
-                const int4 d = i < a.upw ? ud[4 * i] : unit_desc(a.A, u, threadIdx.x & 31);
+                const int4 d = i < a.upw ? ud[kRowGroups * i] : unit_desc(a.A, u, threadIdx.x & 31);
                 spmv_unit_d<2, true>(a.A, d, threadIdx.x & 31, a.x, nullptr, nullptr, a.r, a.b, 1.0, 0.0, 0.0);
             }
             if (!grid_barrier(a.sync, epoch, a.err, SLOT(2))) { ok = false; break; }
@@ -774,7 +774,7 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
     {
         const int per_warp = (a.units + G * (kPT / 32) - 1) / (G * (kPT / 32));
         smem = (smem + 15) & ~(size_t)15;
-        const size_t per_unit = (size_t)(kPT / 32) * 4 * sizeof(int4);
+        const size_t per_unit = (size_t)(kPT / 32) * kRowGroups * sizeof(int4);
         const size_t room = budget > smem ? (budget - smem) / per_unit : 0;
         a.upw = (int)std::min<size_t>({(size_t)per_warp, (size_t)16, room});
         smem += (size_t)a.upw * per_unit;
@@ -806,7 +806,7 @@ int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRu
     a.A = BsrView{M.row_ptr, M.cols, M.vals, M.cap, M.row_list, M.nrows, M.n_long};
     a.b = b; a.x = x; a.r = c->d_r; a.z = c->d_z; a.p0 = c->d_p0; a.p1 = c->d_p1; a.Ap = c->d_Ap;
     a.nrows = M.nrows;
-    a.units = M.n_long + (M.nrows - M.n_long + 3) / 4;
+    a.units = spmv_units(M.n_long, M.nrows);
     a.precond = cfg.precond;
     a.dinv = c->d_diag_inv; a.abd_rows = 0;
     a.max_iter = cfg.max_iter == 0 ? 3 * M.nrows : cfg.max_iter;

@@ -10,8 +10,8 @@
 namespace sgmas {
 
 // Work split: warps [0, n_long) take one long row each (all 32 lanes), the
-// remaining warps take four short rows (8 lanes each); row_list holds the
-// long rows first, both parts in row order.
+// remaining warps take kRowGroups short rows (kRowLanes lanes each); row_list
+// holds the long rows first, both parts in row order.
 // LIVE = the vector is written by other CTAs earlier in the same launch (the
 // persistent kernel): it is read with an explicit weak ld.global, never the
 // read-only (.nc) path that const __restrict__ would allow; the grid
@@ -26,6 +26,15 @@ __device__ __forceinline__ double ldv(const double* p) {
     return *p;
 }
 
+// lanes per short row (a warp takes 32 / kRowLanes short rows at once)
+constexpr int kRowLanes = 8;
+constexpr int kRowGroups = 32 / kRowLanes;
+
+// warp work units of a matrix: one per long row, one per kRowGroups short rows
+__host__ __device__ __forceinline__ int spmv_units(int n_long, int nrows) {
+    return n_long + (nrows - n_long + kRowGroups - 1) / kRowGroups;
+}
+
 // The block range of this lane's row in work unit gw: {row (-1: none), begin,
 // end, 1 for a whole-warp (long) row}.  Fixed for a given matrix.
 __device__ __forceinline__ int4 unit_desc(const BsrView& A, int gw, int lane) {
@@ -34,7 +43,7 @@ __device__ __forceinline__ int4 unit_desc(const BsrView& A, int gw, int lane) {
         d.x = A.row_list[gw];
         d.w = 1;
     } else {
-        const int g = (gw - A.n_long) * 4 + (lane >> 3);
+        const int g = (gw - A.n_long) * kRowGroups + lane / kRowLanes;
         if (g < A.nrows - A.n_long) d.x = A.row_list[A.n_long + g];
     }
     if (d.x >= 0) {
@@ -65,7 +74,7 @@ __device__ __forceinline__ double spmv_unit_d(const BsrView& A, int4 desc, int l
     const double* __restrict__ bvals = A.vals;
     const long long cap = A.cap;
     const bool longw = desc.w != 0;
-    const int row = desc.x, l = longw ? lane : (lane & 7), G = longw ? 32 : 8;
+    const int row = desc.x, l = longw ? lane : (lane % kRowLanes), G = longw ? 32 : kRowLanes;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     double dot = 0.0;
     {
@@ -99,10 +108,10 @@ __device__ __forceinline__ double spmv_unit_d(const BsrView& A, int4 desc, int l
             }
         } else {
             #pragma unroll
-            for (int o = 4; o > 0; o >>= 1) {
-                a0 += __shfl_xor_sync(0xffffffffu, a0, o, 8);
-                a1 += __shfl_xor_sync(0xffffffffu, a1, o, 8);
-                a2 += __shfl_xor_sync(0xffffffffu, a2, o, 8);
+            for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o, kRowLanes);
+                a1 += __shfl_xor_sync(0xffffffffu, a1, o, kRowLanes);
+                a2 += __shfl_xor_sync(0xffffffffu, a2, o, kRowLanes);
             }
         }
         if (l == 0 && row >= 0) {
