@@ -9,23 +9,48 @@
 
 namespace sgmas {
 
-// Unit u of ex: mode 1 first applies x += alpha p, r -= alpha Ap to its rows;
-// then z = P^-1 r for a body (its 12x12 inverse) or z = r for any other row;
-// adds r.z and r.r of its rows.  (No array is indexed at run time, and the
-// 12x12 product keeps one row in flight, so the caller's registers stay free.)
-__device__ __forceinline__ void extra_unit(int u, const ExtraRows& ex, int N, int mode, double alpha, double* x,
-                                           double* r, const double* p, const double* Ap, double* z, double& rz,
-                                           double& rr) {
+// Rows outside the MAS range, shared by the warps wid = 0 .. nw-1 of a
+// grid (called by whole warps).  Mode 1 first applies x += alpha p,
+// r -= alpha Ap to each row.  Bodies: 16 lanes per body, lane k < 12 owns
+// row k of the body and forms z_k = sum_c P^-1(k, c) r_c with the body's r
+// from shuffles; other rows: one lane each, z = r.  Adds r.z and r.r.
+__device__ __forceinline__ void extra_rows_work(const ExtraRows& ex, int N, int mode, double alpha, double* x,
+                                                double* r, const double* p, const double* Ap, double* z, int wid,
+                                                int nw, int lane, double& rz, double& rr) {
     const int nb = ex.abd_bodies;
-    const bool body = u < nb;
-    const int j = u - nb, gap = ex.fem_off - 4 * nb;
-    const size_t o = body ? 12 * (size_t)u : 3 * (size_t)(j < gap ? 4 * nb + j : ex.fem_off + N + (j - gap));
-    const int len = body ? 12 : 3;
-    double rv[12];
-    #pragma unroll
-    for (int d = 0; d < 12; ++d) {
-        rv[d] = 0.0;
-        if (d < len) {
+    for (int g0 = 2 * wid; g0 < nb; g0 += 2 * nw) {  // warp-uniform trip count
+        const int g = g0 + lane / 16, k = lane % 16;
+        const bool valid = g < nb && k < 12;
+        const size_t o = 12 * (size_t)g + k;
+        double rv = 0.0;
+        const double* M = ex.abd_inv + 144 * (size_t)(valid ? g : 0) + 12 * (valid ? k : 0);  // row k of P^-1
+        if (valid) {
+            rv = r[o];
+            if (mode == 1) {
+                const double xd = x[o], pd = p[o], qd = Ap[o];
+                rv = rv - alpha * qd;
+                x[o] = xd + alpha * pd;
+                r[o] = rv;
+            }
+        }
+        double s = 0.0;
+        #pragma unroll 4  // the row is streamed, not held: the callers' registers stay free
+        for (int c = 0; c < 12; ++c) {
+            const double rc = __shfl_sync(0xffffffffu, rv, c, 16);
+            if (valid) s += M[c] * rc;
+        }
+        if (valid) {
+            z[o] = s;
+            rz += rv * s;
+            rr += rv * rv;
+        }
+    }
+    const int gap = ex.fem_off - 4 * nb;
+    const int n_ident = ex.n_units - nb;  // rows that are neither body nor MAS rows
+    for (int j = wid * 32 + lane; j < n_ident; j += nw * 32) {
+        const size_t o = 3 * (size_t)(j < gap ? 4 * nb + j : ex.fem_off + N + (j - gap));
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) {
             double rd = r[o + d];
             if (mode == 1) {
                 const double xd = x[o + d], pd = p[o + d], qd = Ap[o + d];
@@ -33,29 +58,10 @@ __device__ __forceinline__ void extra_unit(int u, const ExtraRows& ex, int N, in
                 x[o + d] = xd + alpha * pd;
                 r[o + d] = rd;
             }
-            rv[d] = rd;
+            z[o + d] = rd;
+            rz += rd * rd;
             rr += rd * rd;
         }
-    }
-    if (!body) {
-        #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            z[o + d] = rv[d];
-            rz += rv[d] * rv[d];
-        }
-        return;
-    }
-    const double* M = ex.abd_inv + 144 * (size_t)u;
-    #pragma unroll 1
-    for (int a = 0; a < 12; ++a) {
-        double s = 0.0, ra = 0.0;
-        #pragma unroll
-        for (int c = 0; c < 12; ++c) {
-            s += M[a * 12 + c] * rv[c];
-            if (c == a) ra = rv[c];
-        }
-        z[o + a] = s;
-        rz += ra * s;
     }
 }
 

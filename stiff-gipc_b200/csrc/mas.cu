@@ -835,8 +835,12 @@ __global__ void __launch_bounds__(kCollectThreads) k_collect(int N, int L, int M
             rz = r0 * z0 + r1 * z1 + r2 * z2;
             rr = r0 * r0 + r1 * r1 + r2 * r2;
         }
-    } else if (kind >= 1 && v - N < ex.n_units) {  // rows outside the MAS range
-        extra_unit(v - N, ex, N, mode, mode == 1 ? st->alpha : 0.0, x, r, p, Ap, z, rz, rr);
+    }
+    const int npad = (N + 31) & ~31;  // warps from npad on take the rows outside the MAS range
+    if (kind >= 1 && ex.n_units > 0 && v >= npad) {
+        const int wid = (v - npad) >> 5, nw = (gridDim.x * blockDim.x - npad) >> 5;
+        extra_rows_work(ex, N, mode, mode == 1 ? st->alpha : 0.0, x, r, p, Ap, z, wid, nw, threadIdx.x & 31, rz,
+                        rr);
     }
     if (kind < 1) return;
     const double brz = block_sum<kCollectThreads>(rz, sh);
@@ -964,7 +968,9 @@ int apply_t(sgmas_context* c, const double* r, double* z, int mode, const PcgSta
         k1<<<(l1_cap + coarse_bpc<B>() - 1) / coarse_bpc<B>(), kCoarseThreads, smem1, s>>>(
             c->L, c->d_level_size, c->d_going_next, (const S*)c->d_inv, (Acc*)c->d_R, (Acc*)c->d_Z, st,
             c->d_coarse_ticket, c->d_err);
-    const int gN = (c->N + (kind >= 1 ? ex.n_units : 0) + kCollectThreads - 1) / kCollectThreads;
+    // threads past the MAS vertices (padded to a warp): 16 per body, then one per other row
+    const int n_extra = kind >= 1 && ex.n_units > 0 ? 16 * ex.abd_bodies + (ex.n_units - ex.abd_bodies) : 0;
+    const int gN = (((c->N + 31) & ~31) + n_extra + kCollectThreads - 1) / kCollectThreads;
     if (parts & 4)
         k_collect<Acc><<<gN, kCollectThreads, 0, s>>>(
             c->N, c->L, c->Mm, c->d_level_size, c->d_real_map, c->d_coarse_table, (const Acc*)c->d_Z, (Acc*)c->d_R,

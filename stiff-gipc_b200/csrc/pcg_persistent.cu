@@ -64,6 +64,7 @@ struct PArgs {
     int k0, k1, nb0, nb1;  // level-0 banks per CTA (max), level-1 banks per CTA, bank counts
     int nc;                // nodes of levels >= 2 (a multiple of B)
     int capc;              // tiles of levels >= 2 a CTA holds in shared memory (<= kPT / B)
+    int t0g, t1g;          // level-0 / level-1 tiles read from global memory (they did not fit)
     int upw;               // SpMV unit descriptors cached per warp in shared memory
     ExtraRows ex;          // rows outside the MAS range (bodies, other rows); MAS vertex v is row ex.fem_off + v
     // block-Jacobi
@@ -172,7 +173,10 @@ __device__ __forceinline__ void sum_partials2(const double* pa, const double* pb
 __device__ void phase_jacobi(const PArgs& a, int mode, double alpha, const double* pcur, double* part_rz,
                              double* part_rr, double* sh) {
     double rz = 0.0, rr = 0.0;
-    for (int i = blockIdx.x * kPT + threadIdx.x; i < a.nrows; i += gridDim.x * kPT) {
+    // body rows first: 12x12 block-Jacobi per affine body (a.ex lists the bodies)
+    extra_rows_work(a.ex, 0, mode, alpha, a.x, a.r, pcur, a.Ap, a.z, blockIdx.x * (kPT / 32) + threadIdx.x / 32,
+                    gridDim.x * (kPT / 32), threadIdx.x & 31, rz, rr);
+    for (int i = a.abd_rows + blockIdx.x * kPT + threadIdx.x; i < a.nrows; i += gridDim.x * kPT) {
         double rv[3], xv[3], pv[3], qv[3], D[9];
         #pragma unroll
         for (int d = 0; d < 3; ++d) rv[d] = a.r[3 * (size_t)i + d];
@@ -343,7 +347,8 @@ __device__ __forceinline__ bool levels_c(const PArgs& a, const Anc& anc, S* tile
     return true;
 }
 
-template <int B, typename S, typename Acc>
+// TG: some level-0 / level-1 tiles are read from global memory (a.t0g, a.t1g)
+template <int B, typename S, typename Acc, bool TG>
 __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ uint64_t mbar;
@@ -355,8 +360,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     const bool mas = a.precond == 1;
     // shared memory: tiles0 [k0] | tiles1 [k1] | tilesC [capc] | R1s, Z1s [k1 B 3] | Rc, Zc [nc 3] | parc [nc]
     S* tiles0 = reinterpret_cast<S*>(smem_raw);
-    S* tiles1 = tiles0 + (size_t)a.k0 * tb;
-    S* tilesC = tiles1 + (size_t)a.k1 * tb;
+    S* tiles1 = tiles0 + (size_t)(a.t0g ? 0 : a.k0) * tb;
+    S* tilesC = tiles1 + (size_t)(a.t1g ? 0 : a.k1) * tb;
     Acc* R1s = reinterpret_cast<Acc*>(tilesC + (size_t)a.capc * tb);
     __shared__ Anc anc;
     __shared__ int rng[2];
@@ -424,7 +429,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            const unsigned by0 = (unsigned)(o.nbk0 * tb * sizeof(S)), by1 = (unsigned)(o.nbk1 * tb * sizeof(S));
+            const unsigned by0 = a.t0g ? 0u : (unsigned)(o.nbk0 * tb * sizeof(S));
+            const unsigned by1 = a.t1g ? 0u : (unsigned)(o.nbk1 * tb * sizeof(S));
             const bool cache_c = anc.total <= a.capc;
             const unsigned byc = cache_c ? (unsigned)(anc.total * tb * sizeof(S)) : 0u;
             mbar_expect_tx(&mbar, by0 + by1 + byc);
@@ -475,7 +481,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             if (own && a.L >= 2 && __popc(msk & lanemask_lt(lane)) == 0) {
                 R1s[3 * n1loc] = s0; R1s[3 * n1loc + 1] = s1; R1s[3 * n1loc + 2] = s2;
             }
-            schwarz_rows<B, S, Acc>(tiles0 + (size_t)(hw < o.nbk0 ? hw : 0) * tb, lane, xb, zl0, zl1, zl2);
+            // level-0 tiles: shared memory, or global memory when they did not fit
+            const S* t0 = TG && a.t0g ? (const S*)a.inv + (size_t)o.lo * tb : tiles0;
+            schwarz_rows<B, S, Acc>(t0 + (size_t)(hw < o.nbk0 ? hw : 0) * tb, lane, xb, zl0, zl1, zl2);
         }
         if (a.L < 2) return;
         __syncthreads();
@@ -496,7 +504,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                 }
             }
             Acc z0, z1, z2;
-            schwarz_rows<B, S, Acc>(tiles1 + (size_t)(valid ? hw : 0) * tb, lane, xb, z0, z1, z2);
+            const S* t1 = TG && a.t1g ? (const S*)a.inv + (size_t)(a.lvl_begin[1] / B + o.j0) * tb : tiles1;
+            schwarz_rows<B, S, Acc>(t1 + (size_t)(valid ? hw : 0) * tb, lane, xb, z0, z1, z2);
             if (valid) { Z1s[3 * i] = z0; Z1s[3 * i + 1] = z1; Z1s[3 * i + 2] = z2; }
         }
         __syncthreads();
@@ -504,8 +513,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     // CollectFinalZ for the owned slot + r.z, r.r partials
     auto collect = [&](int mode, double alpha, const double* pcur) {
         double rz = 0.0, rr = 0.0;
-        for (int u = blockIdx.x * kPT + threadIdx.x; u < a.ex.n_units; u += gridDim.x * kPT)
-            extra_unit(u, a.ex, a.N, mode, alpha, a.x, a.r, pcur, a.Ap, a.z, rz, rr);
+        extra_rows_work(a.ex, a.N, mode, alpha, a.x, a.r, pcur, a.Ap, a.z, blockIdx.x * (kPT / 32) + threadIdx.x / 32,
+                        gridDim.x * (kPT / 32), threadIdx.x & 31, rz, rr);
         if (own) {
             Acc c0 = zl0, c1 = zl1, c2 = zl2;
             if (a.L >= 2) { c0 += Z1s[3 * n1loc]; c1 += Z1s[3 * n1loc + 1]; c2 += Z1s[3 * n1loc + 2]; }
@@ -691,8 +700,8 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
     const size_t tb = (size_t)bs * 9 * sizeof(S);
     int max_smem = 0;
     SG_CUDA(c, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
-    cudaFuncAttributes fa;
-    SG_CUDA(c, cudaFuncGetAttributes(&fa, k_pcg_persistent<B, S, Acc>));
+    cudaFuncAttributes fa;  // both instantiations have the same static shared memory
+    SG_CUDA(c, cudaFuncGetAttributes(&fa, k_pcg_persistent<B, S, Acc, false>));
     const size_t budget = (size_t)max_smem - fa.sharedSizeBytes - 256;  // minus the kernel's static shared memory
     const int G = dev_sms;
     size_t smem = 0;
@@ -757,8 +766,13 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
         }
         a.nc = a.L > 2 ? a.total - a.lvl_begin[2] : 0;
         if (a.k0 > kPT / B || a.k1 > kPT / B) return 1;  // one slot per thread: use the graph form
-        const size_t fixed = (size_t)(a.k0 + a.k1) * tb + 2 * 3 * (size_t)a.k1 * B * sizeof(Acc) +
-                             2 * 3 * (size_t)a.nc * sizeof(Acc) + (size_t)a.nc * sizeof(int);
+        const size_t small = 2 * 3 * (size_t)a.k1 * B * sizeof(Acc) + 2 * 3 * (size_t)a.nc * sizeof(Acc) +
+                             (size_t)a.nc * sizeof(int);
+        // level-0 tiles stay in shared memory if anything does; level-1 tiles next
+        a.t0g = a.t1g = 0;
+        if (small + (size_t)(a.k0 + a.k1) * tb + (a.L > 2 ? tb : 0) > budget) a.t1g = 1;
+        if (small + (size_t)a.k0 * tb + (a.L > 2 ? tb : 0) > budget) a.t0g = 1;
+        const size_t fixed = small + (size_t)((a.t0g ? 0 : a.k0) + (a.t1g ? 0 : a.k1)) * tb;
         if (a.L > 2) {
             if (fixed + tb > budget) return 1;
             a.capc = (int)std::min<size_t>({(size_t)(a.nc / B), (size_t)(kPT / B), (budget - fixed) / tb});
@@ -768,7 +782,7 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
         }
         smem = fixed + (size_t)a.capc * tb;
     } else {
-        a.k0 = a.k1 = a.nb0 = a.nb1 = a.nc = a.capc = 0;
+        a.k0 = a.k1 = a.nb0 = a.nb1 = a.nc = a.capc = a.t0g = a.t1g = 0;
     }
     // SpMV unit descriptors (16 B per warp, unit and lane group), as many as fit, at most 16 units per warp
     {
@@ -779,7 +793,7 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
         a.upw = (int)std::min<size_t>({(size_t)per_warp, (size_t)16, room});
         smem += (size_t)a.upw * per_unit;
     }
-    auto kern = k_pcg_persistent<B, S, Acc>;
+    auto kern = (a.t0g || a.t1g) ? k_pcg_persistent<B, S, Acc, true> : k_pcg_persistent<B, S, Acc, false>;
     SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
     int per_sm = 0;
     SG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPT, smem));
@@ -801,14 +815,17 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
 int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, float* solve_ms,
                        int* launches, unsigned long long* stamps, int stamp_iters) {
     const BsrMatrix& M = c->bsr;
-    if (cfg.precond == 0 && cfg.abd_bodies > 0) return 1;  // block-Jacobi with 12x12 body blocks: graph form
+
     PArgs a = {};
     a.A = BsrView{M.row_ptr, M.cols, M.vals, M.cap, M.row_list, M.nrows, M.n_long};
     a.b = b; a.x = x; a.r = c->d_r; a.z = c->d_z; a.p0 = c->d_p0; a.p1 = c->d_p1; a.Ap = c->d_Ap;
     a.nrows = M.nrows;
     a.units = spmv_units(M.n_long, M.nrows);
     a.precond = cfg.precond;
-    a.dinv = c->d_diag_inv; a.abd_rows = 0;
+    a.dinv = c->d_diag_inv;
+    a.abd_rows = cfg.precond == 0 ? 4 * cfg.abd_bodies : 0;
+    if (cfg.precond == 0)  // block-Jacobi: the bodies are the only extra units
+        a.ex = ExtraRows{4 * cfg.abd_bodies, cfg.abd_bodies, M.nrows, cfg.abd_bodies, c->d_abd_inv};
     a.max_iter = cfg.max_iter == 0 ? 3 * M.nrows : cfg.max_iter;
     a.check_every = cfg.check_every;
     a.use_prec_norm = cfg.use_prec_norm;

@@ -340,6 +340,7 @@ def test_hybrid_mas_abd_solve(sgm, hybrid, mode, precision):
     x2 = torch.zeros_like(x)
     rj = ctx.pcg_solve(vals, rows, cols, s.n_verts, b, x2, rel_tol=1e-6, preconditioner="jacobi", abd_bodies=nb)
     assert rj["converged"] == 1 and rep["iterations"] < rj["iterations"]
+    assert rj["kernel_launches"] == 1 if mode == "persistent" else rj["kernel_launches"] > 1
     ctx.close()
 
 
