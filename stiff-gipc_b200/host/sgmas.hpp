@@ -37,6 +37,8 @@ class Context {
     Context& operator=(const Context&) = delete;
     sgmas_context* get() const { return ctx_; }
     void set_stream(void* s) { check(ctx_, sgmas_set_stream(ctx_, s), "sgmas_set_stream"); }
+    // SGMAS_PCG_PERSISTENT (default) or SGMAS_PCG_GRAPH
+    void set_pcg_mode(int mode) { check(ctx_, sgmas_set_pcg_mode(ctx_, mode), "sgmas_set_pcg_mode"); }
 
   private:
     sgmas_context* ctx_ = nullptr;
@@ -92,7 +94,8 @@ struct PCGSolverConfig {
     double abs_tol = 0.0;
     bool use_preconditioned_residual_norm = true;
     int preconditioner = 1;  // 0: block-Jacobi (P_type 0), 1: MAS (P_type 1)
-    int abd_bodies = 0;
+    int abd_bodies = 0;      // affine bodies first, 4 block rows each (12x12 block-Jacobi)
+    int fem_offset = 0;      // first block row of the MAS range (the FEM vertices)
 };
 
 // gipc::PCGSolver::solve (pcg_solver.cu:155-168): x = 0, PCG, returns the
@@ -101,17 +104,55 @@ class PCGSolver {
   public:
     PCGSolver(Context& ctx, const PCGSolverConfig& cfg) : ctx_(ctx.get()), cfg_(cfg) {}
     int solve(const sgmas_bcoo& A, double* d_x, const double* d_b, sgmas_pcg_report* report = nullptr) {
-        sgmas_pcg_config c = {cfg_.max_iter, cfg_.rel_tol,    cfg_.abs_tol, cfg_.use_preconditioned_residual_norm,
-                              cfg_.preconditioner, cfg_.abd_bodies, 0,  10};
+        sgmas_pcg_config c = {cfg_.max_iter,       cfg_.rel_tol,    cfg_.abs_tol, cfg_.use_preconditioned_residual_norm,
+                              cfg_.preconditioner, cfg_.abd_bodies, cfg_.fem_offset, 10};
         sgmas_pcg_report rep = {};
         check(ctx_, sgmas_pcg_solve(ctx_, &A, d_b, d_x, &c, &rep), "PCGSolver::solve");
         if (report) *report = rep;
         return rep.iterations;
+    }
+    // the solver's members r and z after the last solve (pcg_solver.h:29-30), device arrays
+    void last_vectors(double* d_r, double* d_z) {
+        check(ctx_, sgmas_pcg_last_vectors(ctx_, d_r, d_z), "PCGSolver::last_vectors");
     }
 
   private:
     sgmas_context* ctx_;
     PCGSolverConfig cfg_;
 };
+
+// A host BCOO system: the reference's export / import files
+// (GlobalLinearSystem::export_matrix_market_files; SG/main.cu:398-646).
+struct HostSystem {
+    std::vector<double> values;  // 9 per block, column-major
+    std::vector<int> rows, cols;
+    int n_block_rows = 0;
+    std::vector<double> b;
+};
+
+inline void mtx_write(const std::string& path_A, const std::string& path_b, const HostSystem& s) {
+    check(nullptr,
+          sgmas_mtx_write(path_A.c_str(), path_b.empty() ? nullptr : path_b.c_str(), s.values.data(), s.rows.data(),
+                          s.cols.data(), (int)s.rows.size(), s.n_block_rows, s.b.empty() ? nullptr : s.b.data()),
+          "mtx_write");
+}
+
+inline HostSystem mtx_read(const std::string& path_A, const std::string& path_b = "") {
+    HostSystem s;
+    int nb = 0, nr = 0;
+    const char* pb = path_b.empty() ? nullptr : path_b.c_str();
+    int rc = sgmas_mtx_read(path_A.c_str(), pb, nullptr, nullptr, nullptr, 0, nullptr, 0, &nb, &nr);
+    if (rc != SGMAS_OK && rc != SGMAS_ERR_CAPACITY) check(nullptr, rc, "mtx_read");
+    s.values.resize(9 * (size_t)nb);
+    s.rows.resize(nb);
+    s.cols.resize(nb);
+    s.n_block_rows = nr;
+    if (pb) s.b.resize(3 * (size_t)nr);
+    check(nullptr,
+          sgmas_mtx_read(path_A.c_str(), pb, s.values.data(), s.rows.data(), s.cols.data(), nb,
+                         pb ? s.b.data() : nullptr, (int)s.b.size(), &nb, &nr),
+          "mtx_read");
+    return s;
+}
 
 }  // namespace sgmas
