@@ -286,9 +286,7 @@ def run_sgmas(args):
         res = float(torch.linalg.norm(b - y) / torch.linalg.norm(b))
         ms = statistics.mean(times)
         if world > 1:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(ms, dev)
         results[v] = {"ms": ms, "ms_min": min(times), "ms_max": max(times), "iterations": int(statistics.median(iters)),
                       "rel_residual": res, "converged": bool(rep["converged"]),
                       "precond_build_ms": rep["precond_ms"], "pcg_loop_ms": rep["solve_ms"], "mode": mode,
@@ -519,6 +517,42 @@ def run_reference(args):
                               "d2h_bytes_per_step": 0}}))
 
 
+def max_over_ranks(v, dev):
+    """The slowest rank's value (device-timed numbers are reported as the max over ranks)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def shard_by_cost(costs, world):
+    """Scenes per rank: largest first, each to the least loaded rank (ties to
+    the lowest rank); every rank computes the same assignment."""
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for k in sorted(range(len(costs)), key=lambda i: (-costs[i], i)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += costs[k]
+        parts[r].append(k)
+    return [sorted(p) for p in parts]
+
+
+def reduce_batch_timings(total_ms, dofs, lat, dev):
+    """Whole-batch numbers over the ranks of the process group: wall time =
+    max of the ranks' device times, DOF = sum, latencies gathered."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size()
+    t = torch.tensor([total_ms, float(dofs)], device=dev, dtype=torch.float64)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    all_lat = [None] * world
+    dist.all_gather_object(all_lat, lat)
+    return float(mx[0].item()), int(t[1].item()), [v for part in all_lat for v in part]
+
+
 def run_c5(args):
     """Config 5, batched serving of uneven scenes: 64 tet-grid systems (N
     log-uniform in [2k, 200k] x scale, E log-uniform in [1e4, 1e8], barrier
@@ -541,14 +575,7 @@ def run_c5(args):
     t0 = time.time()
     scenes = synth.config5(seed=0, n_scenes=args.c5_scenes, scale=args.scale)
     gen_s = time.time() - t0
-    order = sorted(range(len(scenes)), key=lambda k: -len(scenes[k].rows))
-    load = [0] * world
-    mine = []
-    for k in order:                        # greedy: largest scene to the least loaded rank
-        r = min(range(world), key=lambda q: load[q])
-        load[r] += len(scenes[k].rows)
-        if r == rank:
-            mine.append(k)
+    mine = shard_by_cost([len(sc.rows) for sc in scenes], world)[rank]
 
     def tdev(a):
         return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -585,14 +612,7 @@ def run_c5(args):
         del vals, rows, cols, b, pos, pairs, x
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([total_ms, float(dofs)], device=dev, dtype=torch.float64)
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        all_lat = [None] * world
-        dist.all_gather_object(all_lat, lat)
-        lat = [v for part in all_lat for v in part]
-        wall_ms, dofs = float(mx[0].item()), int(t[1].item())
+        wall_ms, dofs, lat = reduce_batch_timings(total_ms, dofs, lat, dev)
         dist.barrier()
         dist.destroy_process_group()
     else:
