@@ -58,6 +58,11 @@ typedef struct {
     int abd_bodies;              /* 12x12 block-Jacobi on block rows [0, 4*abd_bodies) */
     int fem_offset;              /* first FEM block row (MAS sub-range) */
     int check_every;             /* convergence-test cadence; 10 = reference (pcg_solver.cu:240,260) */
+    int initial_guess;           /* 0: x0 = 0, r0 = b (reference, pcg_solver.cu:175).  1: d_x holds a start
+                                    guess x0 (e.g. a learned warm start, sgmas_mlp_warm_start): the solve
+                                    scales it by alpha = x0.b / x0.A x0 (0 unless positive), rejects it
+                                    (x0 = 0) when ||b - alpha A x0|| > ||b||, and tests convergence
+                                    against ||b|| instead of ||r0|| */
 } sgmas_pcg_config;
 
 typedef struct {
@@ -69,6 +74,10 @@ typedef struct {
     float precond_ms;    /* device time of the preconditioner build */
     int kernel_launches; /* kernels of the PCG loop (1 for the persistent form, graph nodes executed otherwise) */
     int build_launches;  /* kernels of the solve's set-up: block CSR, MAS hierarchy, scatter, inverses */
+    int x0_rejected;     /* initial_guess = 1: 1 when the start guess was rejected (the solve began at 0) */
+    double x0_scale;     /* initial_guess = 1: the scale alpha applied to the start guess */
+    double rr_x0;        /* initial_guess = 1: ||b - alpha A x0||^2 before the rejection test */
+    double bb;           /* initial_guess = 1: ||b||^2, the reference of the convergence test */
 } sgmas_pcg_report;
 
 /* One BCOO matrix on the device (borrowed). */
@@ -145,7 +154,7 @@ int sgmas_mas_download_matrices(sgmas_context* ctx, double* hess64, double* inv_
 int sgmas_mas_invert_host(sgmas_context* ctx, const double* hess64, int nblocks, double* inv64);
 
 /* ---- PCGSolver (SG/linear_system/solver/pcg_solver.cu:155-304) -------- */
-/* x = 0, then PCG on the device with device-side scalars; the whole loop is
+/* x = 0 (or the start guess in d_x, cfg->initial_guess), then PCG on the device with device-side scalars; the whole loop is
  * one CUDA graph (conditional WHILE node).  Requires sgmas_mas_init (and
  * assembles the MAS itself) when cfg->preconditioner == 1. */
 int sgmas_pcg_solve(sgmas_context* ctx, const sgmas_bcoo* A, const double* d_b, double* d_x,

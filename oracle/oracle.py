@@ -25,12 +25,13 @@ f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 class PCGCfg(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("rel_tol", C.c_double), ("abs_tol", C.c_double),
                 ("use_preconditioned_norm", C.c_int), ("precond", C.c_int),
-                ("abd_bodies", C.c_int), ("fem_offset", C.c_int), ("nthreads", C.c_int)]
+                ("abd_bodies", C.c_int), ("fem_offset", C.c_int), ("nthreads", C.c_int),
+                ("initial_guess", C.c_int)]
 
 
 class PCGReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("rel_residual", C.c_double), ("rz0", C.c_double),
-                ("rr0", C.c_double), ("ms", C.c_double)]
+                ("rr0", C.c_double), ("ms", C.c_double), ("x0_scale", C.c_double), ("x0_rejected", C.c_int)]
 
 
 def build():
@@ -257,13 +258,15 @@ def factor_blocks(hess, nblocks, bank=16):
 
 
 def pcg(s_vals, rows, cols, nrows, b, precond=1, rel_tol=1e-4, abs_tol=0.0, max_iter=0,
-        use_preconditioned_norm=False, mas=None, fem_offset=0, abd_bodies=0, nthreads=1):
+        use_preconditioned_norm=False, mas=None, fem_offset=0, abd_bodies=0, nthreads=1, x0=None):
+    """x0: a start guess (scaled by x0.b / x0.A x0, rejected when it raises
+    the residual, convergence against ||b||); None = x0 = 0 (the reference)."""
     cfg = PCGCfg(max_iter, rel_tol, abs_tol, int(use_preconditioned_norm), precond, abd_bodies,
-                 fem_offset, nthreads)
+                 fem_offset, nthreads, int(x0 is not None))
     rep = PCGReport()
     b = cf64(b)
-    x = np.zeros_like(b)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64, copy=True)
     lib().or_pcg(cf64(s_vals).reshape(-1), c32(rows), c32(cols), len(rows), nrows, b, x,
                  C.byref(cfg), mas.h if mas is not None else None, C.byref(rep))
     return x, dict(iterations=rep.iterations, rel_residual=rep.rel_residual, ms=rep.ms,
-                   rz0=rep.rz0, rr0=rep.rr0)
+                   rz0=rep.rz0, rr0=rep.rr0, x0_scale=rep.x0_scale, x0_rejected=rep.x0_rejected)

@@ -1463,13 +1463,34 @@ int or_pcg(const double* vals, const int* rows, const int* cols, int nb, int nro
     } while(0)
 
     int max_iter = cfg->max_iter == 0 ? n : cfg->max_iter;
-    for(int i = 0; i < n; i++) x[i] = 0;
-    memcpy(r, b, sizeof(double) * (size_t)n);
+    /* start guess: x0 scaled by the A-norm-optimal alpha = x0.b / x0.A x0
+       (0 unless positive), rejected when ||b - alpha A x0|| > ||b||; the
+       convergence test is then relative to ||b|| */
+    double bb = 0;
+    int warm = cfg->initial_guess;
+    rep->x0_scale = 0;
+    rep->x0_rejected = 0;
+    if(warm)
+    {
+        csr_spmv(&A, x, Ap);
+        const double xax = pdot(x, Ap, n), xb = pdot(x, b, n);
+        bb = pdot(b, b, n);
+        const double alpha = (xax > 0 && xb > 0) ? xb / xax : 0.0;
+        for(int i = 0; i < n; i++) { r[i] = b[i] - alpha * Ap[i]; x[i] = alpha * x[i]; }
+        const double rr = pdot(r, r, n);
+        rep->x0_scale = alpha;
+        rep->x0_rejected = !(rr <= bb) || alpha == 0.0;
+    }
+    if(!warm || rep->x0_rejected)
+    {
+        for(int i = 0; i < n; i++) x[i] = 0;
+        memcpy(r, b, sizeof(double) * (size_t)n);
+    }
     OR_APPLY();
     double rz = pdot(r, z, n);
     memcpy(p, z, sizeof(double) * (size_t)n);
     double rz0 = rz, rr0 = 0;
-    if(!cfg->use_preconditioned_norm) rr0 = pdot(r, r, n);
+    if(!cfg->use_preconditioned_norm) rr0 = warm ? bb : pdot(r, r, n);
     const double rel2 = cfg->rel_tol * cfg->rel_tol, abs2 = cfg->abs_tol * cfg->abs_tol;
     int k;
     for(k = 1; k < max_iter; ++k)

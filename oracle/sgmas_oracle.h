@@ -82,6 +82,8 @@ typedef struct {
     int abd_bodies;        /* bodies whose 12x12 diagonal blocks are inverted */
     int fem_offset;        /* first FEM block row (MAS sub-range) */
     int nthreads;          /* OpenMP threads for the timed CPU arm (0 = all) */
+    int initial_guess;     /* 1: x holds x0; scaled by x0.b / x0.A x0, rejected when it raises ||r||,
+                              convergence against ||b|| (the library's start-guess rule) */
 } or_pcg_cfg;
 
 typedef struct {
@@ -89,6 +91,8 @@ typedef struct {
     double rel_residual;   /* ||b - Ax|| / ||b|| at exit, recomputed */
     double rz0, rr0;
     double ms;
+    double x0_scale;       /* initial_guess: the scale applied to x0 */
+    int x0_rejected;       /* initial_guess: 1 when x0 was rejected */
 } or_pcg_report;
 
 int or_pcg(const double* vals, const int* rows, const int* cols, int nb,

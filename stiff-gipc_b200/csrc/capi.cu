@@ -345,7 +345,7 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
                             c->N, A->n_block_rows, cfg->fem_offset, cfg->abd_bodies);
     }
     SG_CUDA(c, cudaSetDevice(c->device));
-    PcgRunCfg rc_cfg;
+    PcgRunCfg rc_cfg = {};
     rc_cfg.max_iter = cfg->max_iter;
     rc_cfg.rel_tol = cfg->rel_tol;
     rc_cfg.abs_tol = cfg->abs_tol;
@@ -354,6 +354,9 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
     rc_cfg.abd_bodies = cfg->abd_bodies;
     rc_cfg.fem_offset = cfg->fem_offset;
     rc_cfg.check_every = cfg->check_every > 0 ? cfg->check_every : 10;
+    if (cfg->initial_guess != 0 && cfg->initial_guess != 1)
+        return ctx_fail(c, SGMAS_ERR_ARG, "initial_guess must be 0 (x0 = 0) or 1 (x holds the start guess)");
+    rc_cfg.warm = cfg->initial_guess;
     if (!c->ev0) {
         SG_CUDA(c, cudaEventCreate(&c->ev0));
         SG_CUDA(c, cudaEventCreate(&c->ev1));
@@ -391,6 +394,10 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
         report->precond_ms = prep_ms;
         report->kernel_launches = launches;
         report->build_launches = c->build_launches;
+        report->x0_rejected = rc_cfg.warm ? h.w_reject : 0;
+        report->x0_scale = rc_cfg.warm ? h.w_alpha : 0.0;
+        report->rr_x0 = rc_cfg.warm ? h.w_rr : 0.0;
+        report->bb = rc_cfg.warm ? h.w_bb : h.rr0;
     }
     if (!(h.rz == h.rz) || !(h.rr == h.rr)) return ctx_fail(c, SGMAS_ERR_NUMERIC, "non-finite residual in PCG");
     return SGMAS_OK;
@@ -417,6 +424,8 @@ int sgmas_pcg_solve_host(sgmas_context* c, const double* values, const int* rows
     SG_CUDA(c, cudaMemcpyAsync(c->d_hrows, rows, sizeof(int) * n_blocks, cudaMemcpyHostToDevice, s));
     SG_CUDA(c, cudaMemcpyAsync(c->d_hcols, cols, sizeof(int) * n_blocks, cudaMemcpyHostToDevice, s));
     SG_CUDA(c, cudaMemcpyAsync(c->d_hb, b, sizeof(double) * 3 * n_block_rows, cudaMemcpyHostToDevice, s));
+    if (cfg && cfg->initial_guess == 1)  // x carries the start guess in
+        SG_CUDA(c, cudaMemcpyAsync(c->d_hx, x, sizeof(double) * 3 * n_block_rows, cudaMemcpyHostToDevice, s));
     sgmas_bcoo A = {c->d_hvals, c->d_hrows, c->d_hcols, n_blocks, n_block_rows};
     int rc = sgmas_pcg_solve(c, &A, c->d_hb, c->d_hx, cfg, report);
     if (rc) return rc;

@@ -13,6 +13,9 @@ struct PcgState {
     int max_iter, check_every;
     double rel2, abs2;
     int use_prec_norm, pad;
+    // start guess (initial_guess = 1): x0.b, b.b, scale, ||b - alpha A x0||^2
+    double w_xb, w_bb, w_alpha, w_rr;
+    int warm, w_reject;
 };
 
 // Rows of a solve outside the MAS range (the reference's hybrid scenes:
@@ -36,6 +39,7 @@ struct PcgRunCfg {
     int abd_bodies;
     int fem_offset;
     int check_every;
+    int warm;          // 1: x holds a start guess (scaled, rejected when it raises ||r0||)
 };
 
 struct BsrMatrix {

@@ -345,7 +345,8 @@ __global__ void __launch_bounds__(kT) k_jacobi_iter(int nrows, int abd_rows, dou
     }
 }
 
-__global__ void k_init_state(PcgState* st, int max_iter, double rel2, double abs2, int check_every, int prec_norm) {
+__global__ void k_init_state(PcgState* st, int max_iter, double rel2, double abs2, int check_every, int prec_norm,
+                             int warm) {
     PcgState s = {};
     s.max_iter = max_iter;
     s.rel2 = rel2;
@@ -353,7 +354,84 @@ __global__ void k_init_state(PcgState* st, int max_iter, double rel2, double abs
     s.check_every = check_every;
     s.use_prec_norm = prec_norm;
     s.k = 1;
+    s.warm = warm;
     *st = s;
+}
+
+// Two grid sums with the last-CTA-done pattern (partials summed in CTA
+// order); true in thread 0 of the last CTA with the totals in s1, s2.
+__device__ __forceinline__ bool grid_sum2_last(double v1, double v2, double* partials, unsigned* ticket, double* sh,
+                                               double& s1, double& s2) {
+    const double b1 = block_sum<kT>(v1, sh);
+    const double b2 = block_sum<kT>(v2, sh);
+    __shared__ bool am_last;
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = b1;
+        partials[gridDim.x + blockIdx.x] = b2;
+        __threadfence();
+        am_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+    double t1 = 0.0, t2 = 0.0;
+    for (int t = threadIdx.x; t < (int)gridDim.x; t += kT) {
+        t1 += ((volatile double*)partials)[t];
+        t2 += ((volatile double*)partials)[gridDim.x + t];
+    }
+    s1 = block_sum<kT>(t1, sh);
+    s2 = block_sum<kT>(t2, sh);
+    if (threadIdx.x == 0) *ticket = 0u;
+    return threadIdx.x == 0;
+}
+
+// Start guess (graph form).  (1) x0.b and b.b; then k_bsr_spmv<1> with
+// beta = 0 gives Ap = A x0 and x0.A x0 (st->pAp); (2) alpha = x0.b / x0.A x0
+// (0 unless positive), r = b - alpha Ap, x = alpha x0, r.r and the rejection
+// test ||r|| > ||b||; (3) a rejected guess restarts from x = 0, r = b.
+__global__ void __launch_bounds__(kT) k_warm_dots(int n, const double* __restrict__ x, const double* __restrict__ b,
+                                                  PcgState* st, double* partials, unsigned* ticket) {
+    __shared__ double sh[32];
+    double xb = 0.0, bb = 0.0;
+    for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
+        const double bi = b[i];
+        xb += x[i] * bi;
+        bb += bi * bi;
+    }
+    double s1, s2;
+    if (grid_sum2_last(xb, bb, partials, ticket, sh, s1, s2)) {
+        st->w_xb = s1;
+        st->w_bb = s2;
+    }
+}
+__global__ void __launch_bounds__(kT) k_warm_residual(int n, double* x, double* r, const double* __restrict__ b,
+                                                      const double* __restrict__ Ap, PcgState* st, double* partials,
+                                                      unsigned* ticket) {
+    __shared__ double sh[32];
+    const double xax = st->pAp, xb = st->w_xb;
+    const double alpha = (xax > 0.0 && xb > 0.0) ? xb / xax : 0.0;
+    double rr = 0.0;
+    for (int i = blockIdx.x * kT + threadIdx.x; i < n; i += gridDim.x * kT) {
+        const double ri = b[i] - alpha * Ap[i];
+        r[i] = ri;
+        x[i] = alpha * x[i];
+        rr += ri * ri;
+    }
+    double s1, s2;
+    if (grid_sum2_last(rr, 0.0, partials, ticket, sh, s1, s2)) {
+        st->w_alpha = alpha;
+        st->w_rr = s1;
+        st->w_reject = !(s1 <= st->w_bb) || alpha == 0.0;
+        st->pAp = 0.0;
+        st->alpha = 0.0;
+    }
+}
+__global__ void k_warm_reject(int n, double* x, double* r, const double* __restrict__ b, const PcgState* st) {
+    if (!st->w_reject) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        r[i] = b[i];
+        x[i] = 0.0;
+    }
 }
 
 // reference-faithful symmetric BCOO SpMV (Spmv::warp_reduce_sym_spmv,
@@ -493,13 +571,24 @@ static int jacobi_setup(sgmas_context* c, const double* vals, const int* rows, c
 static int record_prologue(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, int* nk) {
     cudaStream_t s = c->stream;
     const int nrows = c->bsr.nrows, n = 3 * nrows;
-    SG_CUDA(c, cudaMemsetAsync(x, 0, sizeof(double) * n, s));
-    SG_CUDA(c, cudaMemcpyAsync(c->d_r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    if (!cfg.warm) {
+        SG_CUDA(c, cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+        SG_CUDA(c, cudaMemcpyAsync(c->d_r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    }
     SG_CUDA(c, cudaMemsetAsync(c->d_p0, 0, sizeof(double) * n, s));
     const int max_iter = cfg.max_iter == 0 ? n : cfg.max_iter;
     k_init_state<<<1, 1, 0, s>>>(c->d_state, max_iter, cfg.rel_tol * cfg.rel_tol, cfg.abs_tol * cfg.abs_tol,
-                                 cfg.check_every, cfg.use_prec_norm);
+                                 cfg.check_every, cfg.use_prec_norm, cfg.warm);
     *nk = 1;
+    if (cfg.warm) {
+        const int gv = std::min((n + kT - 1) / kT, 4 * 148);
+        k_warm_dots<<<gv, kT, 0, s>>>(n, x, b, c->d_state, c->d_partials, c->d_ticket);
+        k_bsr_spmv<1><<<spmv_grid(c->bsr), kT, 0, s>>>(bsr_view(c->bsr), x, x, c->d_p1, c->d_Ap, nullptr, 1.0, 0.0,
+                                                       c->d_state, c->d_partials, c->d_ticket);
+        k_warm_residual<<<gv, kT, 0, s>>>(n, x, c->d_r, b, c->d_Ap, c->d_state, c->d_partials, c->d_ticket);
+        k_warm_reject<<<gv, kT, 0, s>>>(n, x, c->d_r, b, c->d_state);
+        *nk += 4;
+    }
     if (cfg.precond == 1) {
         int rc = mas_launch_apply(c, c->d_r, c->d_z, 0, c->d_state, x, nullptr, nullptr, c->d_partials,
                                   c->d_ticket, 1, 0ull, nk, extra_rows_of(c, cfg));
@@ -577,6 +666,7 @@ int pcg_run(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, 
                                  (unsigned long long)nrows | ((unsigned long long)c->bsr.cap << 24) ^
                                      ((unsigned long long)c->bsr.n_long << 44),
                                  (unsigned long long)cfg.precond | ((unsigned long long)c->precision << 4) |
+                                     ((unsigned long long)cfg.warm << 6) |
                                      ((unsigned long long)cfg.abd_bodies << 8) |
                                      ((unsigned long long)cfg.fem_offset << 36),
                                  (unsigned long long)(uintptr_t)c->bsr.vals,
@@ -685,7 +775,9 @@ static int pcg_profile_persistent(sgmas_context* c, float* ms, int n_ms) {
     if (!c->d_stamps && ctx_alloc(c, &c->d_stamps, n_st)) return SGMAS_ERR_CUDA;
     SG_CUDA(c, cudaMemsetAsync(c->d_stamps, 0, n_st * sizeof(unsigned long long), c->stream));
     float loop_ms = 0.f;
-    int rc = pcg_run_persistent(c, c->last_b, c->last_x, c->last_run, &loop_ms, nullptr, c->d_stamps, kStampIters);
+    PcgRunCfg cfg = c->last_run;
+    cfg.warm = 0;  // x now holds the last solution: profile the solve from x = 0
+    int rc = pcg_run_persistent(c, c->last_b, c->last_x, cfg, &loop_ms, nullptr, c->d_stamps, kStampIters);
     if (rc) return rc < 0 ? rc : ctx_fail(c, SGMAS_ERR_STATE, "persistent solve no longer fits");
     unsigned long long* h = new unsigned long long[n_st];
     cudaError_t e = cudaMemcpy(h, c->d_stamps, n_st * sizeof(unsigned long long), cudaMemcpyDeviceToHost);

@@ -72,8 +72,9 @@ struct PArgs {
     int abd_rows, precond;
     // control
     int max_iter, check_every, use_prec_norm;
+    int warm;          // x holds a start guess (scaled, rejected when it raises ||r0||)
     double rel2, abs2;
-    double* partials;  // [3][grid]
+    double* partials;  // [4][grid]
     unsigned* sync;    // [0] barrier arrivals (monotonic)
     PcgState* st;
     int* err;
@@ -546,10 +547,73 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     // ---- prologue: x = 0, r = b, p_old = 0, z = M^-1 r, r.z, r.r
     for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT) {
         a.p0[i] = 0.0;
-        if (!mas || a.ex.n_units > 0) { a.x[i] = 0.0; a.r[i] = a.b[i]; }
+        if (!a.warm && (!mas || a.ex.n_units > 0)) { a.x[i] = 0.0; a.r[i] = a.b[i]; }
+    }
+    // start guess x0 (in x): Ap = A x0 with x0.A x0 (the SpMV with p = x0,
+    // beta = 0, p written to p1 as scratch), x0.b, b.b; then alpha = x0.b /
+    // x0.A x0 (0 unless positive), r = b - alpha A x0, x = alpha x0, r.r; a
+    // guess that raises ||r|| above ||b|| is rejected (x = 0, r = b).  All
+    // CTAs sum the same partials, so all take the same branch.
+    double w_bb = 0.0;
+    if (a.warm) {
+        double w_alpha = 0.0, w_rr = 0.0;
+        double* part_w = a.partials + 3 * gridDim.x;
+        double xax = 0.0, xb = 0.0, bb = 0.0;
+        {
+            const int4* ud = udesc + (threadIdx.x / 32) * a.upw * kRowGroups + (threadIdx.x & 31) / kRowLanes;
+            const int gw = blockIdx.x * (kPT / 32) + threadIdx.x / 32;
+            for (int u = gw, i = 0; u < a.units; u += gridDim.x * (kPT / 32), ++i) {
+                const int4 d = i < a.upw ? ud[kRowGroups * i] : unit_desc(a.A, u, threadIdx.x & 31);
+                xax += spmv_unit_d<1, true>(a.A, d, threadIdx.x & 31, a.x, a.x, a.p1, a.Ap, nullptr, 1.0, 0.0, 0.0);
+            }
+        }
+        for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT) {
+            const double bi = a.b[i];
+            xb += a.x[i] * bi;
+            bb += bi * bi;
+        }
+        xax = block_sum<kPT>(xax, sh);
+        xb = block_sum<kPT>(xb, sh);
+        bb = block_sum<kPT>(bb, sh);
+        if (threadIdx.x == 0) { part_pap[blockIdx.x] = xax; part_rz[blockIdx.x] = xb; part_rr[blockIdx.x] = bb; }
+        ok = ok && grid_barrier(a.sync, epoch, a.err);
+        if (ok) {
+            xax = sum_partials(part_pap, sh);
+            sum_partials2(part_rz, part_rr, sh, xb, bb);
+            w_bb = bb;
+            w_alpha = (xax > 0.0 && xb > 0.0) ? xb / xax : 0.0;
+            double rr = 0.0;
+            for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT) {
+                const double ri = a.b[i] - w_alpha * a.Ap[i];
+                a.r[i] = ri;
+                a.x[i] = w_alpha * a.x[i];
+                rr += ri * ri;
+            }
+            rr = block_sum<kPT>(rr, sh);
+            if (threadIdx.x == 0) part_w[blockIdx.x] = rr;
+        }
+        ok = ok && grid_barrier(a.sync, epoch, a.err);
+        if (ok) {
+            w_rr = sum_partials(part_w, sh);
+            const int w_rej = !(w_rr <= w_bb) || w_alpha == 0.0;
+            if (blockIdx.x == 0 && threadIdx.x == 0) {  // read back by the same thread at the end
+                a.st->w_alpha = w_alpha; a.st->w_rr = w_rr; a.st->w_reject = w_rej;
+            }
+            if (w_rej) {
+                for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT) {
+                    a.r[i] = a.b[i];
+                    a.x[i] = 0.0;
+                }
+                ok = grid_barrier(a.sync, epoch, a.err);
+            }
+        }
     }
     if (mas) {
-        if (v >= 0) { r0 = a.b[vo]; r1 = a.b[vo + 1]; r2 = a.b[vo + 2]; }
+        if (v >= 0) {
+            const double* r_in = a.warm ? a.r : a.b;
+            r0 = r_in[vo]; r1 = r_in[vo + 1]; r2 = r_in[vo + 2];
+            if (a.warm && own) { x0 = a.x[vo]; x1 = a.x[vo + 1]; x2 = a.x[vo + 2]; }
+        }
         if (ok) apply_b();
         if (a.L > 2) {
             ok = ok && grid_barrier(a.sync, epoch, a.err);
@@ -563,8 +627,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     ok = ok && grid_barrier(a.sync, epoch, a.err);
     double rz = ok ? sum_partials(part_rz, sh) : 0.0;
     const double rz0 = rz;
-    const double rr0 = ok ? sum_partials(part_rr, sh) : 0.0;
-    double rr_last = rr0, beta = 0.0;
+    const double rr0_r = ok ? sum_partials(part_rr, sh) : 0.0;
+    const double rr0 = a.warm ? w_bb : rr0_r;  // a start guess: convergence relative to ||b||
+    double rr_last = rr0_r, beta = 0.0;
     int k = 1, iters = 1, converged = 0;
     bool done = !ok || a.max_iter <= 1;
     double* pold = a.p0;
@@ -674,6 +739,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         s.converged = converged;
         s.max_iter = a.max_iter;
         s.check_every = a.check_every;
+        s.warm = a.warm;
+        if (a.warm) { s.w_alpha = a.st->w_alpha; s.w_rr = a.st->w_rr; s.w_reject = a.st->w_reject; s.w_bb = rr0; }
         *a.st = s;
         if (a.stamps) {
             a.stamps[1] = clock64();
@@ -829,6 +896,7 @@ int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRu
     a.max_iter = cfg.max_iter == 0 ? 3 * M.nrows : cfg.max_iter;
     a.check_every = cfg.check_every;
     a.use_prec_norm = cfg.use_prec_norm;
+    a.warm = cfg.warm;
     a.rel2 = cfg.rel_tol * cfg.rel_tol;
     a.abs2 = cfg.abs_tol * cfg.abs_tol;
     a.err = c->d_err;
@@ -840,8 +908,8 @@ int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRu
     a.sync = c->d_psync;
     int dev_sms = 0;
     SG_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device));
-    if (2 * c->partial_cap < 3 * dev_sms) {  // partials of p.Ap, r.z, r.r per CTA (2 * partial_cap doubles)
-        const int cap = (3 * dev_sms + 1) / 2;
+    if (2 * c->partial_cap < 4 * dev_sms) {  // partials of p.Ap, r.z, r.r (+ start guess) per CTA (2 * partial_cap doubles)
+        const int cap = 2 * dev_sms;
         if (ctx_alloc(c, &c->d_partials, 2 * (size_t)cap)) return SGMAS_ERR_CUDA;
         c->partial_cap = cap;
     }

@@ -14,7 +14,7 @@ __device__ __forceinline__ void pcg_end_iteration(PcgState* st, double rz_new, d
     if (kind == 1) {
         st->rz = rz_new;
         st->rz0 = rz_new;
-        st->rr0 = rr;
+        st->rr0 = st->warm ? st->w_bb : rr;  // a start guess: convergence relative to ||b||
         st->rr = rr;
         st->k = 1;
         st->beta = 0.0;

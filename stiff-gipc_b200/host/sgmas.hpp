@@ -96,16 +96,18 @@ struct PCGSolverConfig {
     int preconditioner = 1;  // 0: block-Jacobi (P_type 0), 1: MAS (P_type 1)
     int abd_bodies = 0;      // affine bodies first, 4 block rows each (12x12 block-Jacobi)
     int fem_offset = 0;      // first block row of the MAS range (the FEM vertices)
+    bool initial_guess = false;  // d_x holds a start guess (scaled; rejected when it raises ||r0||)
 };
 
-// gipc::PCGSolver::solve (pcg_solver.cu:155-168): x = 0, PCG, returns the
-// iteration count.
+// gipc::PCGSolver::solve (pcg_solver.cu:155-168): x = 0 (or the start guess
+// in d_x with initial_guess), PCG, returns the iteration count.
 class PCGSolver {
   public:
     PCGSolver(Context& ctx, const PCGSolverConfig& cfg) : ctx_(ctx.get()), cfg_(cfg) {}
     int solve(const sgmas_bcoo& A, double* d_x, const double* d_b, sgmas_pcg_report* report = nullptr) {
         sgmas_pcg_config c = {cfg_.max_iter,       cfg_.rel_tol,    cfg_.abs_tol, cfg_.use_preconditioned_residual_norm,
-                              cfg_.preconditioner, cfg_.abd_bodies, cfg_.fem_offset, 10};
+                              cfg_.preconditioner, cfg_.abd_bodies, cfg_.fem_offset, 10,
+                              cfg_.initial_guess ? 1 : 0};
         sgmas_pcg_report rep = {};
         check(ctx_, sgmas_pcg_solve(ctx_, &A, d_b, d_x, &c, &rep), "PCGSolver::solve");
         if (report) *report = rep;

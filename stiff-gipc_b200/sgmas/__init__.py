@@ -35,13 +35,15 @@ class Config(C.Structure):
 class PcgConfig(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("rel_tol", C.c_double), ("abs_tol", C.c_double),
                 ("use_preconditioned_norm", C.c_int), ("preconditioner", C.c_int),
-                ("abd_bodies", C.c_int), ("fem_offset", C.c_int), ("check_every", C.c_int)]
+                ("abd_bodies", C.c_int), ("fem_offset", C.c_int), ("check_every", C.c_int),
+                ("initial_guess", C.c_int)]
 
 
 class PcgReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("rz0", C.c_double), ("rr0", C.c_double),
                 ("rr_last", C.c_double), ("solve_ms", C.c_float), ("precond_ms", C.c_float),
-                ("kernel_launches", C.c_int), ("build_launches", C.c_int)]
+                ("kernel_launches", C.c_int), ("build_launches", C.c_int), ("x0_rejected", C.c_int),
+                ("x0_scale", C.c_double), ("rr_x0", C.c_double), ("bb", C.c_double)]
 
 
 class Bcoo(C.Structure):
@@ -191,10 +193,13 @@ def _h(a, dtype):
 
 
 def pcg_config(max_iter=0, rel_tol=1e-4, abs_tol=0.0, use_preconditioned_norm=False, preconditioner="mas",
-               abd_bodies=0, fem_offset=0, check_every=10):
+               abd_bodies=0, fem_offset=0, check_every=10, initial_guess=False):
+    """initial_guess=True: x holds a start guess x0 on entry (scaled by
+    x0.b / x0.A x0, rejected when it raises the residual; convergence is then
+    tested against ||b||)."""
     pc = {"jacobi": 0, "mas": 1, 0: 0, 1: 1}[preconditioner]
     return PcgConfig(max_iter, rel_tol, abs_tol, int(use_preconditioned_norm), pc, abd_bodies, fem_offset,
-                     check_every)
+                     check_every, int(bool(initial_guess)))
 
 
 class Context:
@@ -310,9 +315,11 @@ class Context:
         self._check(self.L.sgmas_pcg_solve(self.h, C.byref(A), _ptr(b), _ptr(x), C.byref(c), C.byref(rep)))
         return {k: getattr(rep, k) for k, _ in PcgReport._fields_}
 
-    def pcg_solve_host(self, vals, rows, cols, n_block_rows, b, **cfg):
+    def pcg_solve_host(self, vals, rows, cols, n_block_rows, b, x0=None, **cfg):
         vals, rows, cols, b = _h(vals, np.float64), _h(rows, np.int32), _h(cols, np.int32), _h(b, np.float64)
-        x = np.zeros_like(b)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64, copy=True)
+        if x0 is not None:
+            cfg["initial_guess"] = True
         c = pcg_config(**cfg)
         rep = PcgReport()
         self._check(self.L.sgmas_pcg_solve_host(self.h, _ptr(vals), _ptr(rows), _ptr(cols), len(rows),

@@ -276,6 +276,25 @@ def test_oracle_preconditioned_norm_and_max_iter():
     assert r2["iterations"] % 10 == 0 and r2["iterations"] > 0
 
 
+def test_oracle_start_guess_rule():
+    """Start guess: scaled by x0.b / x0.A x0, kept when it lowers ||r||, and
+    the convergence test is relative to ||b||; a guess with x0.b <= 0 or no
+    finite scale is rejected and the solve equals the cold one."""
+    import scipy.sparse.linalg as spl
+    s = cases.build("c1").s
+    xs = spl.spsolve(synth.full_matrix(s), s.b)
+    _, cold = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=1, rel_tol=1e-6)
+    x, near = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=1, rel_tol=1e-6, x0=2.0 * xs)
+    assert near["x0_rejected"] == 0 and abs(near["x0_scale"] - 0.5) < 1e-9
+    assert near["iterations"] == 10 and near["rel_residual"] <= 1e-6
+    assert abs(near["rr0"] - float(s.b @ s.b)) <= 1e-12 * float(s.b @ s.b)
+    xc, _ = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=1, rel_tol=1e-6)
+    for bad in (-xs, np.zeros_like(xs), np.full_like(xs, np.nan)):
+        xr, rr = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=1, rel_tol=1e-6, x0=bad)
+        assert rr["x0_rejected"] == 1 and rr["iterations"] == cold["iterations"]
+        np.testing.assert_array_equal(xr, xc)
+
+
 def test_mas_apply_is_symmetric_positive():
     case = cases.build("c1")
     m = case.oracle_mas(pairs=False, precision=2)
