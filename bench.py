@@ -50,7 +50,11 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = benchmark size)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-other", action="store_true", help="skip the brief config 1 / config 3 lines")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c5"],
+    ap.add_argument("--c4-scale", type=float, default=None, help="config-4 scene scale (default 1.0 for --workload c4)")
+    ap.add_argument("--c4-train", type=int, default=None, help="config-4 training sequences (20 steps each)")
+    ap.add_argument("--c4-eval", type=int, default=None, help="config-4 held-out sequences")
+    ap.add_argument("--no-learned", action="store_true", help="skip the reduced config-4 line of the default run")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c4", "c5"],
                     help="c2: the headline contact solve; c5: batched uneven scenes (throughput, p50/p99)")
     ap.add_argument("--c5-scenes", type=int, default=64)
     ap.add_argument("--c5-precision", default="bf16", choices=["bf16", "fp32", "fp64"])
@@ -363,6 +367,8 @@ def run_sgmas(args):
            "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "clocks": clocks_rec}
     if not args.no_other:
         out["other_configs"] = other_configs(args, dev, stream)
+    if not args.no_learned:
+        out["learned_c4"] = learned_c4(dev, stream, scale=0.5, n_train=16, n_eval=4, epochs=40)
     if rank == 0 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(s, results)
     if world > 1:
@@ -424,6 +430,141 @@ def other_configs(args, dev, stream):
             ctx.close()
         out[name] = res
     return out
+
+
+def learned_c4(dev, stream, scale, n_train, n_eval, epochs, steps_per_seq=20, batch_banks=256, keep=1.0):
+    """Config 4, the learned start guess, on drop sequences (sgmas.sequence:
+    the contact scene's two tet blocks, the top one released from U(0.01,
+    0.1) m, one linearly implicit Euler step per system).  Training data are
+    the solver's own solves (BF16 MAS-PCG to 1e-6) of n_train seeded
+    sequences; the network trains in FP32 on the GPU.  On n_eval held-out
+    sequences every step is solved to 1e-4 of ||b|| by four arms, each timed
+    with CUDA events around its whole call (set-up + loop, plus the start
+    guess for the learned arms): plain FP64 MAS-PCG from x0 = 0, plain BF16
+    MAS-PCG from x0 = 0, BF16 with the learned start (sgmas_mlp_warm_start:
+    Galerkin combination of previous step, lumped step, network step and
+    coarse term), and the same start with a zero network (previous step +
+    lumped step only: what the network adds).  The trajectory follows the
+    FP64 solution.  Each context solves the first system once untimed."""
+    import torch
+    import sgmas
+    from sgmas import learned
+    from sgmas.sequence import DropScene
+
+    def scene_ctx(sc, prec):
+        ctx = sgmas.Context(dev.index or 0, bank=16, precision=prec)
+        ctx.set_stream(stream.cuda_stream)
+        pm, rm = ctx.morton_partition(torch.as_tensor(sc.X, device=dev))
+        ctx.mas_init(sc.n, *sgmas.vert_neighbors(sc.tets, sc.n), pm, rm)
+        ctx.mas_set_contacts(sc.t_pairs, len(sc.pairs))
+        return ctx, pm
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    t0 = time.time()
+    ts = learned.TrainingSet(dev, keep=keep, seed=0)
+    n_solves = 0
+    for seed in range(n_train):
+        sc = DropScene(seed=seed, scale=scale, device=dev)
+        ctx, pm = scene_ctx(sc, "bf16")
+        sc.ctx = ctx
+        for _ in range(steps_per_seq):
+            vals, rows, cols, b = sc.system()
+            x = torch.zeros_like(b)
+            ctx.pcg_solve(vals, rows, cols, sc.n, b, x, rel_tol=1e-6, max_iter=MAX_ITER)
+            ts.add(ctx, vals, rows, cols, sc.n, b, x, prev=sc.prev, part_map=pm)
+            sc.advance(x)
+            n_solves += 1
+        ctx.close()
+    ts.finalize()
+    data_s = time.time() - t0
+    t0 = time.time()
+    trainer = sgmas.Context(dev.index or 0, bank=16, precision="bf16")
+    trainer.set_stream(stream.cuda_stream)
+    trainer.mlp_set_params(learned.init_params(0))
+    hist = learned.train(trainer, ts, epochs=epochs, batch_banks=batch_banks, lr=2e-3, lr_final=2e-4, seed=0,
+                         log_every=10 ** 9)
+    torch.cuda.synchronize()
+    train_s = time.time() - t0
+    P = trainer.mlp_get_params()
+    trainer.close()
+    arms = ("plain_fp64", "plain_bf16", "learned_bf16", "zero_net_bf16")
+    rec = {a: {"ms": [], "it": []} for a in arms}
+    rejected = 0
+    coefs = []
+    for seed in range(1000, 1000 + n_eval):
+        sc = DropScene(seed=seed, scale=scale, device=dev)
+        c64, _ = scene_ctx(sc, "fp64")
+        c16, _ = scene_ctx(sc, "bf16")
+        cl, _ = scene_ctx(sc, "bf16")
+        cz, _ = scene_ctx(sc, "bf16")
+        sc.ctx = c64
+        cl.mlp_set_params(P)
+        cz.mlp_set_params(np.zeros(len(P), np.float32))
+        for k in range(steps_per_seq):
+            vals, rows, cols, b = sc.system()
+            args_ = (vals, rows, cols, sc.n, b)
+            kw = dict(rel_tol=REL_TOL, max_iter=MAX_ITER)
+            reps = 2 if k == 0 else 1  # first system: one untimed call per context
+            for rep_i in range(reps):
+                x64 = torch.zeros_like(b)
+                r64, ms64 = timed(lambda: c64.pcg_solve(*args_, x64, **kw))
+                x16 = torch.zeros_like(b)
+                r16, ms16 = timed(lambda: c16.pcg_solve(*args_, x16, **kw))
+                res = {}
+                for name, cc in (("learned_bf16", cl), ("zero_net_bf16", cz)):
+                    x0 = torch.zeros_like(b)
+
+                    def go(cc=cc, x0=x0):
+                        cc.mlp_warm_start(*args_, x0, prev=sc.prev)
+                        return cc.pcg_solve(*args_, x0, initial_guess=True, **kw)
+                    res[name] = timed(go)
+            rec["plain_fp64"]["ms"].append(ms64); rec["plain_fp64"]["it"].append(r64["iterations"])
+            rec["plain_bf16"]["ms"].append(ms16); rec["plain_bf16"]["it"].append(r16["iterations"])
+            for name, (r, ms) in res.items():
+                rec[name]["ms"].append(ms); rec[name]["it"].append(r["iterations"])
+                if name == "learned_bf16":
+                    rejected += r["x0_rejected"]
+            coefs.append(cl.mlp_warm_start(*args_, torch.zeros_like(b), prev=sc.prev, coef=True).tolist())
+            sc.advance(x64)
+        for cc in (c64, c16, cl, cz):
+            cc.close()
+    mean = lambda v: round(float(np.mean(v)), 3)
+    summ = {a: {"ms": mean(rec[a]["ms"]), "iterations": mean(rec[a]["it"])} for a in arms}
+    n = len(rec["plain_fp64"]["ms"])
+    return {"workload": f"config 4: drop sequences at scale {scale} ({sc.n} vertices), "
+                        f"{n_train} x {steps_per_seq} training solves, {n_eval} x {steps_per_seq} held-out steps",
+            "metric": "mean solve ms per held-out step to 1e-4 of ||b||", "arms": summ, "steps": n,
+            "speedup_learned_bf16_vs_plain_fp64": round(summ["plain_fp64"]["ms"] / summ["learned_bf16"]["ms"], 3),
+            "speedup_plain_bf16_vs_plain_fp64": round(summ["plain_fp64"]["ms"] / summ["plain_bf16"]["ms"], 3),
+            "network_gain_vs_zero_net": round(summ["zero_net_bf16"]["ms"] / summ["learned_bf16"]["ms"], 3),
+            "learned_rejected": rejected, "mean_coef_prev_lumped_step_coarse": np.round(np.mean(coefs, 0), 4).tolist(),
+            "training": {"solves": n_solves, "rows": int(ts.X.shape[0]), "epochs": epochs, "data_s": round(data_s, 1),
+                         "train_s": round(train_s, 1), "loss_first": round(hist[0][1], 5) if hist else None,
+                         "loss_last": round(hist[-1][1], 5) if hist else None}}
+
+
+def run_c4(args):
+    """--workload c4: config 4 at its stated size (one GPU)."""
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    scale = args.c4_scale if args.c4_scale is not None else 1.0
+    ntr = args.c4_train if args.c4_train is not None else 100
+    nev = args.c4_eval if args.c4_eval is not None else 10
+    r = learned_c4(dev, stream, scale=scale, n_train=ntr, n_eval=nev, epochs=8 if scale >= 1.0 else 40,
+                   keep=0.5 if scale >= 1.0 else 1.0, batch_banks=512)
+    out = {"metric": "MAS-PCG solve ms to 1e-4 rel. residual: learned/mixed vs plain, same B200",
+           "value": r["arms"]["learned_bf16"]["ms"], "unit": "ms", "higher_is_better": False, "n_gpus": 1,
+           "dtype": "bf16 MAS / fp64 CG", "data": "synthetic", "vs_baseline": None, "config": r}
+    print(json.dumps(out))
 
 
 def run_e2e(args, ctx, s, dev, stream, head):
@@ -643,6 +784,8 @@ def main():
         run_reference(args)
     elif args.workload == "c5":
         run_c5(args)
+    elif args.workload == "c4":
+        run_c4(args)
     else:
         run_sgmas(args)
 

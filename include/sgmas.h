@@ -244,6 +244,60 @@ int sgmas_morton_codes_noalloc(const double* d_pos, int n, const double* aabb, u
 int sgmas_morton_partition(sgmas_context* ctx, const double* d_pos, int n, int* part_map,
                            int part_map_cap, int* part_map_size, int* real_map);
 
+/* ---- learned start guess (no reference counterpart) ----------------------
+ * A per-vertex MLP, 16 -> 128 -> 128 -> 6 with GELU, over features of the
+ * Newton system.  For vertex v (row = fem_offset + v), with D its diagonal
+ * 3x3 block, S_v = sum_j A_vj its 3x3 block row sum, u_v = S_v^-1 b_v (the
+ * lumped step, exact for a rigid translation; D^-1 b_v where S_v has no
+ * positive trace and determinant), t = trace(D) / 3 and s, s_b the RMS over
+ * the MAS vertices of |u_v| and |b_v|, the features are: u_v / s (3), the
+ * previous Newton step / s (3), D^-1 b_v / s (3), D_ii / t - 1 (3), D_01,
+ * D_02, D_12 / t (3), min(contacts of v, 32) / 8 (1).  The network predicts
+ * the correction (dx - u) / s: outputs 0-2 per vertex, outputs 3-5 a coarse
+ * term averaged over the vertex's 16-slot MAS subdomain.  Rows are in the
+ * MAS slot order of sgmas_mas_init (16 per subdomain, padding slots masked).
+ * Parameters (FP32, SGMAS_MLP_PARAMS floats): W1 [16][128] (input-major),
+ * b1 [128], W2 [128][128], b2 [128], W3 [128][6], b3 [6].  Training is FP32
+ * (forward, backward, Adam with beta 0.9 / 0.999, eps 1e-8); the start guess
+ * runs the network in BF16 with FP32 accumulation on the tensor cores. */
+#define SGMAS_MLP_PARAMS 19462
+/* set the FP32 parameters (host array) and reset the Adam state */
+int sgmas_mlp_set_params(sgmas_context* ctx, const float* params, int n);
+int sgmas_mlp_get_params(sgmas_context* ctx, float* params, int n);
+/* features in slot order: d_X [Mm][16], d_mask [Mm] (1 = vertex, 0 = padding);
+ * with d_dx (a solved step, 3 * n_block_rows doubles) also the training
+ * target d_T [Mm][3] = (dx - u) / s.  d_prev: the previous Newton step or
+ * NULL.  scales (host, may be NULL) receives (s, s_b).  Needs sgmas_mas_init and,
+ * for the contact counts, sgmas_mas_set_contacts. */
+int sgmas_mlp_features(sgmas_context* ctx, const sgmas_bcoo* A, const double* d_b, const double* d_prev,
+                       const double* d_dx, int fem_offset, float* d_X, float* d_mask, float* d_T,
+                       double* scales);
+/* Loss on n_rows slot rows (a multiple of 16): inv_n * sum over valid rows of
+ * |step + subdomain mean of the coarse term - T|^2.  sgmas_mlp_gradient writes
+ * the gradient (SGMAS_MLP_PARAMS floats, device) without changing the
+ * parameters; sgmas_mlp_train_step takes one Adam step with learning rate lr.
+ * *loss (host, may be NULL) receives the loss before the step. */
+int sgmas_mlp_gradient(sgmas_context* ctx, const float* d_X, const float* d_T, const float* d_mask, int n_rows,
+                       float inv_n, float* d_grad, float* loss);
+int sgmas_mlp_train_step(sgmas_context* ctx, const float* d_X, const float* d_T, const float* d_mask, int n_rows,
+                         float inv_n, float lr, float* loss);
+/* raw network outputs d_Y [n_rows][6]: bf16 = 0 the FP32 training network,
+ * bf16 = 1 the BF16 tensor-core inference */
+int sgmas_mlp_forward(sgmas_context* ctx, const float* d_X, int n_rows, int bf16, float* d_Y);
+/* The start guess of system (A, b), written to d_x0 (3 * n_block_rows
+ * doubles): features + BF16 inference give the candidates v1 = u (the lumped
+ * step S^-1 b, S = 3x3 block row sums of A), v2 = s * network step, v3 = s *
+ * subdomain mean of the network's coarse term (MAS rows only), and v0 =
+ * d_prev (the previous Newton step, when given); x0 = sum c_k v_k with
+ * (V^T A V) c = V^T b, the A-norm-best combination (a candidate that is zero
+ * or linearly dependent on earlier ones gets c_k = 0).  coef (host, may be
+ * NULL) receives c_0..c_3.  Pass d_x0 as d_x of sgmas_pcg_solve with
+ * initial_guess = 1, which rejects it if it raises the residual.  The block
+ * CSR of A built here is reused by the next sgmas_pcg_solve on the same
+ * arrays (they must not change in between). */
+int sgmas_mlp_warm_start(sgmas_context* ctx, const sgmas_bcoo* A, const double* d_b, const double* d_prev,
+                         int fem_offset, double* d_x0, double* coef);
+
 #ifdef __cplusplus
 }
 #endif

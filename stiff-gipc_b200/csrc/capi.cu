@@ -131,6 +131,7 @@ void sgmas_destroy(sgmas_context* c) {
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->ev2) cudaEventDestroy(c->ev2);
     free_all(c);
+    mlp_free(c);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     if (c->rec_stream) cudaStreamDestroy(c->rec_stream);
     delete c;

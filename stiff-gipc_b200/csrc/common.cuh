@@ -65,6 +65,28 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* e
     return false;
 }
 
+// Vertices of one contact in the reference's int4 encoding (the decoding of
+// _buildCollisionConnection_new, SG/MASPreconditioner.cu:1140-1537): point-
+// triangle / edge-edge and their degenerate point-point / point-edge forms,
+// told apart by the signs of the entries.  Returns the vertex count (2-4).
+__device__ __forceinline__ int decode_contact(int4 P, int v[4]) {
+    int nv = 4;
+    if (P.x >= 0) {
+        if (P.w < 0) P.w = -P.w - 1;
+        v[0] = P.x; v[1] = P.y; v[2] = P.z; v[3] = P.w;
+    } else {
+        const int x = -P.x - 1;
+        if (P.z < 0) {
+            if (P.y < 0) { v[0] = x; v[1] = -P.y - 1; v[2] = -P.z - 1; v[3] = -P.w - 1; }
+            else { v[0] = x; v[1] = P.y; nv = 2; }
+        } else if (P.w < 0) {
+            if (P.y < 0) { v[0] = x; v[1] = -P.y - 1; v[2] = P.z; v[3] = -P.w - 1; }
+            else { v[0] = x; v[1] = P.y; v[2] = P.z; nv = 3; }
+        } else { v[0] = x; v[1] = P.y; v[2] = P.z; v[3] = P.w; }
+    }
+    return nv;
+}
+
 // ---- precision helpers ---------------------------------------------------
 template <typename T> struct Store;
 template <> struct Store<float> {

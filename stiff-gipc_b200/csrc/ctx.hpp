@@ -5,6 +5,7 @@
 
 #include <string>
 
+#include "../../include/sgmas.h"
 #include "common.cuh"
 
 struct PcgState {
@@ -145,10 +146,18 @@ struct sgmas_context {
     // converter scratch
     void* d_sort_scratch = nullptr;
     size_t sort_scratch_bytes = 0;
+    // learned start guess (csrc/mlp.cu)
+    struct MlpState* mlp = nullptr;
+    // the block CSR was built for these arrays by the learned start guess and
+    // not used since: the next solve on the same arrays reuses it
+    const void* bsr_src[3] = {nullptr, nullptr, nullptr};
+    int bsr_src_nb = 0, bsr_src_nrows = 0;
+    bool bsr_fresh = false;
 };
 
 // error helpers
 int ctx_fail(sgmas_context* c, int code, const char* fmt, ...);
+void mlp_free(sgmas_context* c);  // the learned start guess's buffers
 #define SG_CUDA(c, expr)                                                                      \
     do {                                                                                      \
         cudaError_t _e = (expr);                                                              \
@@ -187,6 +196,8 @@ int mas_launch_apply(sgmas_context* c, const double* r, double* z, int mode, con
 ExtraRows extra_rows_of(const sgmas_context* c, const PcgRunCfg& cfg);
 int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* cols, int nblocks,
               int nrows);
+void bsr_mark_fresh(sgmas_context* c, const sgmas_bcoo* A);  // the CSR just built is A's
+bool bsr_reuse(sgmas_context* c, const sgmas_bcoo* A);       // true (once) when the fresh CSR is A's
 int bsr_spmv_plain(sgmas_context* c, double a, const double* x, double b, double* y);
 int bcoo_spmv_ref(sgmas_context* c, double a, const double* vals, const int* rows, const int* cols,
                   int nblocks, int nrows, const double* x, double b, double* y);

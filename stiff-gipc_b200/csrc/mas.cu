@@ -75,21 +75,8 @@ __global__ void k_collision(int cp, const int4* __restrict__ pairs, int level, i
                            unsigned* mask) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= cp) return;
-    int4 P = pairs[q];
-    int v[4], id[4], nv = 4;
-    if (P.x >= 0) {
-        if (P.w < 0) P.w = -P.w - 1;
-        v[0] = P.x; v[1] = P.y; v[2] = P.z; v[3] = P.w;
-    } else {
-        const int x = -P.x - 1;
-        if (P.z < 0) {
-            if (P.y < 0) { v[0] = x; v[1] = -P.y - 1; v[2] = -P.z - 1; v[3] = -P.w - 1; }
-            else { v[0] = x; v[1] = P.y; nv = 2; }
-        } else if (P.w < 0) {
-            if (P.y < 0) { v[0] = x; v[1] = -P.y - 1; v[2] = P.z; v[3] = -P.w - 1; }
-            else { v[0] = x; v[1] = P.y; v[2] = P.z; nv = 3; }
-        } else { v[0] = x; v[1] = P.y; v[2] = P.z; v[3] = P.w; }
-    }
+    int v[4], id[4];
+    const int nv = decode_contact(pairs[q], v);
     unsigned cm[4] = {0u, 0u, 0u, 0u};
     for (int i = 0; i < nv; ++i) {
         v[i] -= node_offset;

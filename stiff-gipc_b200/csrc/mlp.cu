@@ -1,0 +1,991 @@
+// mlp.cu -- the learned start guess of the Newton-step solve.
+//
+// The lumped step u_v = S_v^-1 b_v, with S_v = sum_j A_vj the 3x3 block row sum
+// of A, is exact for a rigid translation (elastic and barrier terms are
+// translation invariant, so their row sums vanish and S_v is the vertex mass
+// plus any anchoring terms).  A per-vertex MLP (16 -> 128 -> 128 -> 6, GELU)
+// reads local features of the system A x = b and predicts the correction
+// dx - u: per vertex a step (outputs 0-2) and a coarse term (outputs 3-5)
+// averaged over the vertex's level-0 MAS subdomain (16 slots of the
+// partition).  x0 = u + s (step + subdomain mean of the coarse term); the PCG
+// solve then scales x0 and keeps it only when it lowers the residual
+// (sgmas_pcg_solve with initial_guess = 1).  The reference has no learned
+// component; plain MAS-PCG stays the fallback.
+//
+// Features of vertex v (row = fem_offset + v), D = its diagonal 3x3 block,
+// t = trace(D) / 3, s = RMS over the MAS vertices of |u|:
+//   f0-2  u / s            f3-5  previous Newton step / s     f6-8  D^-1 b_v / s
+//   f9-11 D_ii / t - 1     f12-14 D_01, D_02, D_12 / t        f15   min(contacts of v, 32) / 8
+// Rows are in MAS slot order (slot = 16 * subdomain + lane; padding slots
+// have mask 0), so a subdomain is 16 consecutive rows.
+//
+// Kernels: features (k_diag_index, k_row_sums over the row-owned block CSR,
+// k_contact_count, k_feat_scales, k_feat_scales_final, k_features); FP32 training (k_mlp_tile: forward and
+// backward of 64 rows per CTA with all weights and activations in shared
+// memory, per-tile gradient partials; k_mlp_reduce: partials summed in tile
+// order, then Adam); BF16 inference (k_mlp_pack, k_mlp_infer: one warp per
+// subdomain, mma.sync m16n8k16 BF16 with FP32 accumulation, activations kept
+// in registers between the layers, x0 composed in the same kernel).
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/sgmas.h"
+#include "ctx.hpp"
+
+using namespace sgmas;
+
+namespace {
+
+constexpr int kIn = 16, kHid = 128, kOut = 6;
+constexpr int oW1 = 0, oB1 = oW1 + kIn * kHid, oW2 = oB1 + kHid, oB2 = oW2 + kHid * kHid, oW3 = oB2 + kHid,
+              oB3 = oW3 + kHid * kOut, kParams = oB3 + kOut;
+static_assert(kParams == SGMAS_MLP_PARAMS, "parameter count");
+
+constexpr int kTileRows = 64;  // training rows per CTA (4 subdomains)
+constexpr int kTT = 256;       // training threads per CTA
+constexpr int kW2S = kHid + 1; // padded shared-memory row stride of W2
+// packed BF16 inference weights: transposed (output-major), rows padded
+constexpr int kS1 = 24, kS2 = 136;  // row strides (bf16 elements) of W1t and W2t / W3t
+constexpr int kP1 = kHid * kS1, kP2 = kHid * kS2, kP3 = 8 * kS2, kPackBf16 = kP1 + kP2 + kP3;
+constexpr int kPackBias = kHid + kHid + 8;
+
+constexpr double kAdamB1 = 0.9, kAdamB2 = 0.999, kAdamEps = 1e-8;
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_d(float z) {
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+// ---- features ---------------------------------------------------------------
+__global__ void k_diag_index(int nb, const int* __restrict__ rows, const int* __restrict__ cols, int* dindex) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nb && rows[k] == cols[k]) dindex[rows[k]] = k;
+}
+
+// vertices of each contact (the decoding of _buildCollisionConnection_new,
+// SG/MASPreconditioner.cu:1140-1537), counted per MAS vertex
+__global__ void k_contact_count(int cp, const int4* __restrict__ pairs, int node_offset, int N, int* cnt) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= cp) return;
+    int v[4];
+    const int nv = decode_contact(pairs[q], v);
+    for (int i = 0; i < nv; ++i) {
+        const int u = v[i] - node_offset;
+        if (u >= 0 && u < N) atomicAdd(cnt + u, 1);
+    }
+}
+
+// y = D^-1 b by the cofactor inverse (D column-major); false when D is singular
+__device__ __forceinline__ bool solve3(const double* D, const double* bv, double y[3]) {
+    const double a = D[0], b = D[3], c = D[6], d = D[1], e = D[4], f = D[7], g = D[2], h = D[5], i = D[8];
+    const double A = e * i - f * h, B = f * g - d * i, C = d * h - e * g;
+    const double det = a * A + b * B + c * C;
+    if (!(det > 0.0) && !(det < 0.0)) { y[0] = y[1] = y[2] = 0.0; return false; }
+    const double inv = 1.0 / det;
+    const double m00 = A, m01 = c * h - b * i, m02 = b * f - c * e;
+    const double m10 = B, m11 = a * i - c * g, m12 = c * d - a * f;
+    const double m20 = C, m21 = b * g - a * h, m22 = a * e - b * d;
+    y[0] = inv * (m00 * bv[0] + m01 * bv[1] + m02 * bv[2]);
+    y[1] = inv * (m10 * bv[0] + m11 * bv[1] + m12 * bv[2]);
+    y[2] = inv * (m20 * bv[0] + m21 * bv[1] + m22 * bv[2]);
+    return true;
+}
+
+__device__ __forceinline__ const double* diag_of(const double* vals, const int* dindex, int row, const double* eye) {
+    const int k = dindex[row];
+    return k >= 0 ? vals + 9 * (size_t)k : eye;
+}
+
+// Block row sums of the full matrix from the row-owned block CSR (both
+// triangles, value planes vals[q * cap + p] with q = 3 a + c): one thread per
+// row, entries in CSR order; written column-major (S[a + 3 c]) for solve3.
+__global__ void k_row_sums(int nrows, const int* __restrict__ row_ptr, const double* __restrict__ bvals,
+                           long long cap, double* S) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrows) return;
+    double acc[9];
+    #pragma unroll
+    for (int q = 0; q < 9; ++q) acc[q] = 0.0;
+    for (int p = row_ptr[r]; p < row_ptr[r + 1]; ++p)
+        #pragma unroll
+        for (int q = 0; q < 9; ++q) acc[q] += bvals[q * cap + p];
+    #pragma unroll
+    for (int a = 0; a < 3; ++a)
+        #pragma unroll
+        for (int c = 0; c < 3; ++c) S[9 * (size_t)r + a + 3 * c] = acc[3 * a + c];
+}
+
+// u = S^-1 b when S is a usable lumped block (positive trace and
+// determinant), else D^-1 b
+__device__ __forceinline__ void lumped_step(const double* S, const double* D, const double* bv, double u[3]) {
+    const double tr = S[0] + S[4] + S[8];
+    const double det = S[0] * (S[4] * S[8] - S[7] * S[5]) - S[3] * (S[1] * S[8] - S[7] * S[2]) +
+                       S[6] * (S[1] * S[5] - S[4] * S[2]);
+    if (tr > 0.0 && det > 0.0) solve3(S, bv, u);
+    else solve3(D, bv, u);
+}
+
+// partial sums of |u|^2 per CTA
+__global__ void __launch_bounds__(256) k_feat_scales(int N, int fem_off, const double* __restrict__ vals,
+                                                     const int* __restrict__ dindex, const double* __restrict__ S,
+                                                     const double* __restrict__ b, double* partials) {
+    __shared__ double sh[32];
+    const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    double su = 0.0, sb = 0.0;
+    for (int v = blockIdx.x * 256 + threadIdx.x; v < N; v += gridDim.x * 256) {
+        const int row = fem_off + v;
+        const double* bv = b + 3 * (size_t)row;
+        double u[3];
+        lumped_step(S + 9 * (size_t)row, diag_of(vals, dindex, row, eye), bv, u);
+        su += u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        sb += bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2];
+    }
+    su = block_sum<256>(su, sh);
+    sb = block_sum<256>(sb, sh);
+    if (threadIdx.x == 0) { partials[blockIdx.x] = su; partials[gridDim.x + blockIdx.x] = sb; }
+}
+// scales[0] = s (RMS of |u|), scales[1] = RMS of |b_v| (per vertex; 1 when zero)
+__global__ void k_feat_scales_final(int grid, int N, const double* __restrict__ partials, double* scales) {
+    __shared__ double sh[32];
+    double sy = 0.0, sb = 0.0;
+    for (int i = threadIdx.x; i < grid; i += 256) { sy += partials[i]; sb += partials[grid + i]; }
+    sy = block_sum<256>(sy, sh);
+    sb = block_sum<256>(sb, sh);
+    if (threadIdx.x == 0) {
+        const double n = N > 0 ? (double)N : 1.0;
+        const double a = sqrt(sy / n), c = sqrt(sb / n);
+        scales[0] = a > 0.0 ? a : 1.0;
+        scales[1] = c > 0.0 ? c : 1.0;
+    }
+}
+
+// one thread per slot: X [Mm][16], mask [Mm], and T [Mm][3] = (dx - u) / s when dx is given
+__global__ void __launch_bounds__(256) k_features(int Mm, int N, int fem_off, const int* __restrict__ part_map,
+                                                  const double* __restrict__ vals, const int* __restrict__ dindex,
+                                                  const double* __restrict__ S, const double* __restrict__ b,
+                                                  const double* __restrict__ prev, const double* __restrict__ dx,
+                                                  const int* __restrict__ ccount, const double* __restrict__ scales,
+                                                  float* X, float* mask, float* T) {
+    const int s = blockIdx.x * 256 + threadIdx.x;
+    if (s >= Mm) return;
+    const int v = part_map[s];
+    float f[16];
+    #pragma unroll
+    for (int k = 0; k < 16; ++k) f[k] = 0.f;
+    float m = 0.f, t3[3] = {0.f, 0.f, 0.f};
+    if (v >= 0 && v < N) {
+        const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        const int row = fem_off + v;
+        const double* D = diag_of(vals, dindex, row, eye);
+        const double* bv = b + 3 * (size_t)row;
+        const double sc = scales[0];
+        double u[3], y[3];
+        lumped_step(S + 9 * (size_t)row, D, bv, u);
+        solve3(D, bv, y);
+        double t = (D[0] + D[4] + D[8]) / 3.0;
+        if (!(t > 0.0)) t = 1.0;
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            f[d] = (float)(u[d] / sc);
+            f[3 + d] = prev ? (float)(prev[3 * (size_t)row + d] / sc) : 0.f;
+            f[6 + d] = (float)(y[d] / sc);
+            if (dx) t3[d] = (float)((dx[3 * (size_t)row + d] - u[d]) / sc);
+        }
+        f[9] = (float)(D[0] / t - 1.0);
+        f[10] = (float)(D[4] / t - 1.0);
+        f[11] = (float)(D[8] / t - 1.0);
+        f[12] = (float)(D[3] / t);
+        f[13] = (float)(D[6] / t);
+        f[14] = (float)(D[7] / t);
+        f[15] = (float)min(ccount ? ccount[v] : 0, 32) * 0.125f;
+        m = 1.f;
+    }
+    float4* xo = reinterpret_cast<float4*>(X + 16 * (size_t)s);
+    xo[0] = make_float4(f[0], f[1], f[2], f[3]);
+    xo[1] = make_float4(f[4], f[5], f[6], f[7]);
+    xo[2] = make_float4(f[8], f[9], f[10], f[11]);
+    xo[3] = make_float4(f[12], f[13], f[14], f[15]);
+    mask[s] = m;
+    if (T) { T[3 * (size_t)s] = t3[0]; T[3 * (size_t)s + 1] = t3[1]; T[3 * (size_t)s + 2] = t3[2]; }
+}
+
+// ---- FP32 training: forward + backward of one 64-row tile per CTA -------------
+// shared memory (floats): w1 [16][128] | w2 [128][129] | w3 [128][6] | b1 [128] |
+// b2 [128] | b3 [8] | xs [64][16] | h1, g1, h2, g2 [64][128] | ys, dys [64][8] |
+// ts [64][3] | ms [64] | red [64]
+constexpr int kSmW1 = 0, kSmW2 = kSmW1 + kIn * kHid, kSmW3 = kSmW2 + kHid * kW2S, kSmB1 = kSmW3 + kHid * kOut,
+              kSmB2 = kSmB1 + kHid, kSmB3 = kSmB2 + kHid, kSmX = kSmB3 + 8, kSmH1 = kSmX + kTileRows * kIn,
+              kSmG1 = kSmH1 + kTileRows * kHid, kSmH2 = kSmG1 + kTileRows * kHid, kSmG2 = kSmH2 + kTileRows * kHid,
+              kSmY = kSmG2 + kTileRows * kHid, kSmDY = kSmY + kTileRows * 8, kSmT = kSmDY + kTileRows * 8,
+              kSmM = kSmT + kTileRows * 3, kSmRed = kSmM + kTileRows, kSmFloats = kSmRed + kTileRows;
+constexpr size_t kTrainSmem = sizeof(float) * kSmFloats;
+
+// mode 0: forward only, Y [rows][6] out; mode 1: loss + gradient partials
+__global__ void __launch_bounds__(kTT, 1) k_mlp_tile(const float* __restrict__ P, const float* __restrict__ X,
+                                                     const float* __restrict__ T, const float* __restrict__ mask,
+                                                     int n_rows, float inv_n, int mode, float* Y, float* gpart,
+                                                     float* lpart) {
+    extern __shared__ __align__(16) float sm[];
+    float *w1 = sm + kSmW1, *w2 = sm + kSmW2, *w3 = sm + kSmW3, *b1 = sm + kSmB1, *b2 = sm + kSmB2, *b3 = sm + kSmB3;
+    float *xs = sm + kSmX, *h1 = sm + kSmH1, *g1 = sm + kSmG1, *h2 = sm + kSmH2, *g2 = sm + kSmG2;
+    float *ys = sm + kSmY, *dys = sm + kSmDY, *ts = sm + kSmT, *ms = sm + kSmM, *red = sm + kSmRed;
+    const int tid = threadIdx.x;
+    const int r0 = blockIdx.x * kTileRows;
+    for (int i = tid; i < kIn * kHid; i += kTT) w1[i] = P[oW1 + i];
+    for (int i = tid; i < kHid * kHid; i += kTT) w2[(i / kHid) * kW2S + i % kHid] = P[oW2 + i];
+    for (int i = tid; i < kHid * kOut; i += kTT) w3[i] = P[oW3 + i];
+    for (int i = tid; i < kHid; i += kTT) { b1[i] = P[oB1 + i]; b2[i] = P[oB2 + i]; }
+    if (tid < 8) b3[tid] = tid < kOut ? P[oB3 + tid] : 0.f;
+    for (int i = tid; i < kTileRows * kIn; i += kTT) {
+        const int r = r0 + i / kIn;
+        xs[i] = r < n_rows ? X[(size_t)r0 * kIn + i] : 0.f;
+    }
+    if (mode == 1) {
+        for (int i = tid; i < kTileRows * 3; i += kTT) {
+            const int r = r0 + i / 3;
+            ts[i] = r < n_rows ? T[(size_t)r0 * 3 + i] : 0.f;
+        }
+        if (tid < kTileRows) ms[tid] = r0 + tid < n_rows ? mask[r0 + tid] : 0.f;
+    }
+    __syncthreads();
+    // thread (ty, tx): rows 4 ty .. 4 ty + 3, columns tx + 16 c (c < 8)
+    const int ty = tid / 16, tx = tid % 16;
+    {  // layer 1
+        float acc[4][8];
+        #pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const float bb = b1[tx + 16 * c];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i][c] = bb;
+        }
+        #pragma unroll 4
+        for (int k = 0; k < kIn; ++k) {
+            float a[4], w[8];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = xs[(4 * ty + i) * kIn + k];
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) w[c] = w1[k * kHid + tx + 16 * c];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i)
+                #pragma unroll
+                for (int c = 0; c < 8; ++c) acc[i][c] = fmaf(a[i], w[c], acc[i][c]);
+        }
+        #pragma unroll
+        for (int i = 0; i < 4; ++i)
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int o = (4 * ty + i) * kHid + tx + 16 * c;
+                h1[o] = gelu(acc[i][c]);
+                g1[o] = gelu_d(acc[i][c]);
+            }
+    }
+    __syncthreads();
+    {  // layer 2
+        float acc[4][8];
+        #pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const float bb = b2[tx + 16 * c];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i) acc[i][c] = bb;
+        }
+        #pragma unroll 4
+        for (int k = 0; k < kHid; ++k) {
+            float a[4], w[8];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = h1[(4 * ty + i) * kHid + k];
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) w[c] = w2[k * kW2S + tx + 16 * c];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i)
+                #pragma unroll
+                for (int c = 0; c < 8; ++c) acc[i][c] = fmaf(a[i], w[c], acc[i][c]);
+        }
+        #pragma unroll
+        for (int i = 0; i < 4; ++i)
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int o = (4 * ty + i) * kHid + tx + 16 * c;
+                h2[o] = gelu(acc[i][c]);
+                g2[o] = gelu_d(acc[i][c]);
+            }
+    }
+    __syncthreads();
+    for (int q = tid; q < kTileRows * kOut; q += kTT) {  // layer 3
+        const int r = q / kOut, o = q % kOut;
+        float s = b3[o];
+        for (int k = 0; k < kHid; ++k) s = fmaf(h2[r * kHid + k], w3[k * kOut + o], s);
+        ys[r * 8 + o] = s;
+    }
+    __syncthreads();
+    if (mode == 0) {
+        for (int q = tid; q < kTileRows * kOut; q += kTT) {
+            const int r = q / kOut;
+            if (r0 + r < n_rows) Y[(size_t)(r0 + r) * kOut + q % kOut] = ys[r * 8 + q % kOut];
+        }
+        return;
+    }
+    // prediction = step + subdomain mean of the coarse term; squared error on valid rows
+    if (tid < kTileRows) {
+        const int r = tid, sb = r & ~15;
+        float cnt = 0.f, cm[3] = {0.f, 0.f, 0.f};
+        for (int u = 0; u < 16; ++u) {
+            const float mu = ms[sb + u];
+            cnt += mu;
+            #pragma unroll
+            for (int d = 0; d < 3; ++d) cm[d] += mu * ys[(sb + u) * 8 + 3 + d];
+        }
+        const float ic = cnt > 0.f ? 1.f / cnt : 0.f;
+        float l = 0.f;
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const float e = (ys[r * 8 + d] + cm[d] * ic - ts[r * 3 + d]) * ms[r];
+            l += e * e;
+            dys[r * 8 + d] = 2.f * e * inv_n;
+        }
+        red[r] = l * inv_n;
+    }
+    __syncthreads();
+    if (tid < kTileRows) {  // d(coarse_u) = mask_u * (sum of the subdomain's d(prediction)) / count
+        const int r = tid, sb = r & ~15;
+        float cnt = 0.f, s[3] = {0.f, 0.f, 0.f};
+        for (int u = 0; u < 16; ++u) {
+            cnt += ms[sb + u];
+            #pragma unroll
+            for (int d = 0; d < 3; ++d) s[d] += dys[(sb + u) * 8 + d];
+        }
+        const float ic = cnt > 0.f ? ms[r] / cnt : 0.f;
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) dys[r * 8 + 3 + d] = s[d] * ic;
+    }
+    if (tid == 0) {
+        float l = 0.f;
+        for (int r = 0; r < kTileRows; ++r) l += red[r];
+        lpart[blockIdx.x] = l;
+    }
+    __syncthreads();
+    float* gp = gpart + (size_t)blockIdx.x * kParams;
+    for (int q = tid; q < kHid * kOut; q += kTT) {  // dW3 = h2^T dY
+        const int k = q / kOut, o = q % kOut;
+        float s = 0.f;
+        for (int r = 0; r < kTileRows; ++r) s = fmaf(h2[r * kHid + k], dys[r * 8 + o], s);
+        gp[oW3 + q] = s;
+    }
+    if (tid < kOut) {
+        float s = 0.f;
+        for (int r = 0; r < kTileRows; ++r) s += dys[r * 8 + tid];
+        gp[oB3 + tid] = s;
+    }
+    // dZ2 = (dY W3^T) * gelu'(Z2), in place of g2
+    #pragma unroll
+    for (int i = 0; i < 4; ++i)
+        #pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int r = 4 * ty + i, j = tx + 16 * c;
+            float s = 0.f;
+            #pragma unroll
+            for (int o = 0; o < kOut; ++o) s = fmaf(dys[r * 8 + o], w3[j * kOut + o], s);
+            g2[r * kHid + j] *= s;
+        }
+    __syncthreads();
+    {  // dW2 = h1^T dZ2: rows 8 ty .. 8 ty + 7 of W2, columns tx + 16 c
+        float acc[8][8];
+        #pragma unroll
+        for (int i = 0; i < 8; ++i)
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) acc[i][c] = 0.f;
+        #pragma unroll 2
+        for (int r = 0; r < kTileRows; ++r) {
+            float a[8], d[8];
+            #pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = h1[r * kHid + 8 * ty + i];
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) d[c] = g2[r * kHid + tx + 16 * c];
+            #pragma unroll
+            for (int i = 0; i < 8; ++i)
+                #pragma unroll
+                for (int c = 0; c < 8; ++c) acc[i][c] = fmaf(a[i], d[c], acc[i][c]);
+        }
+        #pragma unroll
+        for (int i = 0; i < 8; ++i)
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) gp[oW2 + (8 * ty + i) * kHid + tx + 16 * c] = acc[i][c];
+    }
+    if (tid < kHid) {
+        float s = 0.f;
+        for (int r = 0; r < kTileRows; ++r) s += g2[r * kHid + tid];
+        gp[oB2 + tid] = s;
+    }
+    // dZ1 = (dZ2 W2^T) * gelu'(Z1), in place of g1
+    {
+        float acc[4][8];
+        #pragma unroll
+        for (int i = 0; i < 4; ++i)
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) acc[i][c] = 0.f;
+        #pragma unroll 4
+        for (int j = 0; j < kHid; ++j) {
+            float a[4], w[8];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = g2[(4 * ty + i) * kHid + j];
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) w[c] = w2[(tx + 16 * c) * kW2S + j];
+            #pragma unroll
+            for (int i = 0; i < 4; ++i)
+                #pragma unroll
+                for (int c = 0; c < 8; ++c) acc[i][c] = fmaf(a[i], w[c], acc[i][c]);
+        }
+        #pragma unroll
+        for (int i = 0; i < 4; ++i)
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) g1[(4 * ty + i) * kHid + tx + 16 * c] *= acc[i][c];
+    }
+    __syncthreads();
+    {  // dW1 = xs^T dZ1: row tid / 16 of W1, columns tx + 16 c
+        const int i = tid / 16;
+        float acc[8];
+        #pragma unroll
+        for (int c = 0; c < 8; ++c) acc[c] = 0.f;
+        for (int r = 0; r < kTileRows; ++r) {
+            const float a = xs[r * kIn + i];
+            #pragma unroll
+            for (int c = 0; c < 8; ++c) acc[c] = fmaf(a, g1[r * kHid + tx + 16 * c], acc[c]);
+        }
+        #pragma unroll
+        for (int c = 0; c < 8; ++c) gp[oW1 + i * kHid + tx + 16 * c] = acc[c];
+    }
+    if (tid < kHid) {
+        float s = 0.f;
+        for (int r = 0; r < kTileRows; ++r) s += g1[r * kHid + tid];
+        gp[oB1 + tid] = s;
+    }
+}
+
+// gradient = partials summed in tile order (deterministic); then Adam
+// (mode 1) or the gradient itself to out (mode 0).  Thread 0 also sums the loss.
+__global__ void k_mlp_reduce(int ntiles, const float* __restrict__ gpart, const float* __restrict__ lpart, int mode,
+                             float lr, float c1, float c2, float* P, float* M, float* V, float* out, float* loss) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0) {
+        float l = 0.f;
+        for (int t = 0; t < ntiles; ++t) l += lpart[t];
+        *loss = l;
+    }
+    if (p >= kParams) return;
+    float g = 0.f;
+    for (int t = 0; t < ntiles; ++t) g += gpart[(size_t)t * kParams + p];
+    if (mode == 0) { out[p] = g; return; }
+    const float m = (float)kAdamB1 * M[p] + (float)(1.0 - kAdamB1) * g;
+    const float v = (float)kAdamB2 * V[p] + (float)(1.0 - kAdamB2) * g * g;
+    M[p] = m;
+    V[p] = v;
+    P[p] -= lr * (m / c1) / (sqrtf(v / c2) + (float)kAdamEps);
+}
+
+// ---- BF16 inference --------------------------------------------------------------
+// FP32 parameters -> W1t [128][24], W2t [128][136], W3t [8][136] (output-major,
+// BF16, zero padding) + FP32 biases b1 [128], b2 [128], b3 [8]
+__global__ void k_mlp_pack(const float* __restrict__ P, __nv_bfloat16* W, float* bias) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kP1) {
+        const int n = i / kS1, k = i % kS1;
+        W[i] = __float2bfloat16_rn(k < kIn ? P[oW1 + k * kHid + n] : 0.f);
+    } else if (i < kP1 + kP2) {
+        const int j = i - kP1, n = j / kS2, k = j % kS2;
+        W[i] = __float2bfloat16_rn(k < kHid ? P[oW2 + k * kHid + n] : 0.f);
+    } else if (i < kPackBf16) {
+        const int j = i - kP1 - kP2, n = j / kS2, k = j % kS2;
+        W[i] = __float2bfloat16_rn(k < kHid && n < kOut ? P[oW3 + k * kOut + n] : 0.f);
+    }
+    if (i < kPackBias) bias[i] = i < kHid ? P[oB1 + i] : i < 2 * kHid ? P[oB2 + i - kHid]
+                                                        : (i - 2 * kHid < kOut ? P[oB3 + i - 2 * kHid] : 0.f);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+constexpr int kIT = 256;  // inference threads per CTA (8 warps, one subdomain each at a time)
+
+// One warp per 16-row subdomain.  compose = 1: the three start-guess
+// candidates of each valid slot's vertex (row = fem_off + v), x0 holding
+// [3][3 nrows]: the lumped step u, s * network step, s * subdomain mean of the
+// coarse term; compose = 0: raw outputs Y [rows][6].
+__global__ void __launch_bounds__(kIT) k_mlp_infer(int n_rows, const float* __restrict__ X,
+                                                   const __nv_bfloat16* __restrict__ Wg, const float* __restrict__ bg,
+                                                   int compose, const int* __restrict__ part_map, int N, int fem_off,
+                                                   const double* __restrict__ scales, const double* __restrict__ vals,
+                                                   const int* __restrict__ dindex, const double* __restrict__ S,
+                                                   const double* __restrict__ b, int nrows, double* x0, float* Y) {
+    __shared__ __align__(16) __nv_bfloat16 W[kPackBf16];
+    __shared__ float bs[kPackBias];
+    __shared__ float ys[kIT / 32][16][8];
+    for (int i = threadIdx.x; i < kPackBf16 / 8; i += kIT)
+        reinterpret_cast<uint4*>(W)[i] = reinterpret_cast<const uint4*>(Wg)[i];
+    for (int i = threadIdx.x; i < kPackBias; i += kIT) bs[i] = bg[i];
+    __syncthreads();
+    const __nv_bfloat16 *W1 = W, *W2 = W + kP1, *W3 = W + kP1 + kP2;
+    const float *bb1 = bs, *bb2 = bs + kHid, *bb3 = bs + 2 * kHid;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, g = lane / 4, t = lane % 4;
+    const int nsub = n_rows / 16;
+    for (int sd = blockIdx.x * (kIT / 32) + warp; sd < nsub; sd += gridDim.x * (kIT / 32)) {
+        const float* x = X + (size_t)sd * 16 * kIn;
+        uint32_t a[4];
+        a[0] = pack_bf16(x[g * kIn + 2 * t], x[g * kIn + 2 * t + 1]);
+        a[1] = pack_bf16(x[(g + 8) * kIn + 2 * t], x[(g + 8) * kIn + 2 * t + 1]);
+        a[2] = pack_bf16(x[g * kIn + 2 * t + 8], x[g * kIn + 2 * t + 9]);
+        a[3] = pack_bf16(x[(g + 8) * kIn + 2 * t + 8], x[(g + 8) * kIn + 2 * t + 9]);
+        uint32_t h[8][4];  // layer output as the next layer's A fragments (8 k-steps of 16)
+        {
+            float acc[16][4];
+            #pragma unroll
+            for (int nt = 0; nt < 16; ++nt) {
+                const float c0 = bb1[nt * 8 + 2 * t], c1 = bb1[nt * 8 + 2 * t + 1];
+                acc[nt][0] = c0; acc[nt][1] = c1; acc[nt][2] = c0; acc[nt][3] = c1;
+                const __nv_bfloat16* wr = W1 + (nt * 8 + g) * kS1 + 2 * t;
+                mma_bf16(acc[nt], a, *reinterpret_cast<const uint32_t*>(wr), *reinterpret_cast<const uint32_t*>(wr + 8));
+            }
+            #pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                h[j][0] = pack_bf16(gelu(acc[2 * j][0]), gelu(acc[2 * j][1]));
+                h[j][1] = pack_bf16(gelu(acc[2 * j][2]), gelu(acc[2 * j][3]));
+                h[j][2] = pack_bf16(gelu(acc[2 * j + 1][0]), gelu(acc[2 * j + 1][1]));
+                h[j][3] = pack_bf16(gelu(acc[2 * j + 1][2]), gelu(acc[2 * j + 1][3]));
+            }
+        }
+        {
+            float acc[16][4];
+            #pragma unroll
+            for (int nt = 0; nt < 16; ++nt) {
+                const float c0 = bb2[nt * 8 + 2 * t], c1 = bb2[nt * 8 + 2 * t + 1];
+                acc[nt][0] = c0; acc[nt][1] = c1; acc[nt][2] = c0; acc[nt][3] = c1;
+            }
+            #pragma unroll
+            for (int j = 0; j < 8; ++j)
+                #pragma unroll
+                for (int nt = 0; nt < 16; ++nt) {
+                    const __nv_bfloat16* wr = W2 + (nt * 8 + g) * kS2 + 16 * j + 2 * t;
+                    mma_bf16(acc[nt], h[j], *reinterpret_cast<const uint32_t*>(wr),
+                             *reinterpret_cast<const uint32_t*>(wr + 8));
+                }
+            #pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                h[j][0] = pack_bf16(gelu(acc[2 * j][0]), gelu(acc[2 * j][1]));
+                h[j][1] = pack_bf16(gelu(acc[2 * j][2]), gelu(acc[2 * j][3]));
+                h[j][2] = pack_bf16(gelu(acc[2 * j + 1][0]), gelu(acc[2 * j + 1][1]));
+                h[j][3] = pack_bf16(gelu(acc[2 * j + 1][2]), gelu(acc[2 * j + 1][3]));
+            }
+        }
+        float o[4] = {bb3[2 * t], bb3[2 * t + 1], bb3[2 * t], bb3[2 * t + 1]};
+        #pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const __nv_bfloat16* wr = W3 + g * kS2 + 16 * j + 2 * t;
+            mma_bf16(o, h[j], *reinterpret_cast<const uint32_t*>(wr), *reinterpret_cast<const uint32_t*>(wr + 8));
+        }
+        ys[warp][g][2 * t] = o[0];
+        ys[warp][g][2 * t + 1] = o[1];
+        ys[warp][g + 8][2 * t] = o[2];
+        ys[warp][g + 8][2 * t + 1] = o[3];
+        __syncwarp();
+        if (!compose) {
+            if (lane < 16)
+                for (int d = 0; d < kOut; ++d) Y[((size_t)sd * 16 + lane) * kOut + d] = ys[warp][lane][d];
+        } else if (lane < 16) {
+            const int v = part_map[sd * 16 + lane];
+            float cnt = 0.f, cm[3] = {0.f, 0.f, 0.f};
+            for (int u = 0; u < 16; ++u) {
+                const int vu = part_map[sd * 16 + u];
+                if (vu < 0 || vu >= N) continue;
+                cnt += 1.f;
+                #pragma unroll
+                for (int d = 0; d < 3; ++d) cm[d] += ys[warp][u][3 + d];
+            }
+            if (v >= 0 && v < N) {
+                const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+                const int row = fem_off + v;
+                double u[3];
+                lumped_step(S + 9 * (size_t)row, diag_of(vals, dindex, row, eye), b + 3 * (size_t)row, u);
+                const double sc = scales[0];
+                const size_t n3 = 3 * (size_t)nrows;
+                #pragma unroll
+                for (int d = 0; d < 3; ++d) {  // candidates: lumped step, network step, subdomain coarse term
+                    x0[3 * (size_t)row + d] = u[d];
+                    x0[n3 + 3 * (size_t)row + d] = sc * (double)ys[warp][lane][d];
+                    x0[2 * n3 + 3 * (size_t)row + d] = sc * (double)(cm[d] / cnt);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---- Galerkin combination of the candidates ------------------------------------
+// x0 = sum_i c_i v_i with (V^T A V) c = V^T b: the A-norm-best start in the span
+// of v0 = previous step (when given), v1 = lumped step, v2 = network step,
+// v3 = network coarse term.  Partials: 10 entries of V^T A V (upper) + 4 of V^T b.
+constexpr int kCand = 4, kGram = kCand * (kCand + 1) / 2 + kCand;
+
+__global__ void __launch_bounds__(256) k_gram_partials(int n3, const double* __restrict__ prev,
+                                                       const double* __restrict__ V, const double* __restrict__ AV,
+                                                       const double* __restrict__ b, double* partials) {
+    __shared__ double sh[32];
+    double acc[kGram];
+    #pragma unroll
+    for (int q = 0; q < kGram; ++q) acc[q] = 0.0;
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < n3; i += gridDim.x * 256) {
+        double v[kCand], av[kCand];
+        v[0] = prev ? prev[i] : 0.0;
+        av[0] = prev ? AV[i] : 0.0;
+        #pragma unroll
+        for (int k = 1; k < kCand; ++k) { v[k] = V[(size_t)(k - 1) * n3 + i]; av[k] = AV[(size_t)k * n3 + i]; }
+        int q = 0;
+        #pragma unroll
+        for (int r = 0; r < kCand; ++r)
+            #pragma unroll
+            for (int c = r; c < kCand; ++c) acc[q++] += v[r] * av[c];
+        const double bi = b[i];
+        #pragma unroll
+        for (int k = 0; k < kCand; ++k) acc[q + k] += v[k] * bi;
+    }
+    #pragma unroll
+    for (int q = 0; q < kGram; ++q) {
+        const double t = block_sum<256>(acc[q], sh);
+        if (threadIdx.x == 0) partials[(size_t)q * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// sums the partials in CTA order and solves the small system by Cholesky in
+// candidate order, skipping a candidate that is zero or (to 1e-10 relative)
+// dependent on the earlier ones; coef[k] = 0 for skipped or non-finite cases
+__global__ void k_gram_solve(int grid, const double* __restrict__ partials, double* coef) {
+    __shared__ double sh[32];
+    __shared__ double tot[kGram];
+    for (int q = 0; q < kGram; ++q) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < grid; i += 256) s += partials[(size_t)q * grid + i];
+        s = block_sum<256>(s, sh);
+        if (threadIdx.x == 0) tot[q] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double G[kCand][kCand], r[kCand], L[kCand][kCand], y[kCand], c[kCand];
+    bool act[kCand];
+    int q = 0;
+    for (int i = 0; i < kCand; ++i)
+        for (int j = i; j < kCand; ++j) { G[i][j] = G[j][i] = tot[q++]; }
+    for (int k = 0; k < kCand; ++k) { r[k] = tot[q + k]; c[k] = 0.0; y[k] = 0.0; }
+    for (int i = 0; i < kCand; ++i)
+        for (int j = 0; j < kCand; ++j) L[i][j] = 0.0;
+    bool finite = true;
+    for (int i = 0; i < kCand; ++i) {
+        act[i] = false;
+        if (!(G[i][i] > 0.0)) continue;
+        double d = G[i][i];
+        for (int j = 0; j < i; ++j) if (act[j]) d -= L[i][j] * L[i][j];
+        if (!(d > 1e-10 * G[i][i])) continue;
+        act[i] = true;
+        L[i][i] = sqrt(d);
+        for (int m = i + 1; m < kCand; ++m) {
+            double t = G[m][i];
+            for (int j = 0; j < i; ++j) if (act[j]) t -= L[m][j] * L[i][j];
+            L[m][i] = t / L[i][i];
+        }
+    }
+    for (int i = 0; i < kCand; ++i) {
+        if (!act[i]) continue;
+        double t = r[i];
+        for (int j = 0; j < i; ++j) if (act[j]) t -= L[i][j] * y[j];
+        y[i] = t / L[i][i];
+    }
+    for (int i = kCand - 1; i >= 0; --i) {
+        if (!act[i]) continue;
+        double t = y[i];
+        for (int j = i + 1; j < kCand; ++j) if (act[j]) t -= L[j][i] * c[j];
+        c[i] = t / L[i][i];
+        finite = finite && (c[i] == c[i]) && c[i] < 1e300 && c[i] > -1e300;
+    }
+    for (int k = 0; k < kCand; ++k) coef[k] = finite ? c[k] : 0.0;
+}
+
+__global__ void k_combine(int n3, const double* __restrict__ prev, const double* __restrict__ V,
+                          const double* __restrict__ coef, double* x0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n3) return;
+    double s = prev ? coef[0] * prev[i] : 0.0;
+    #pragma unroll
+    for (int k = 1; k < kCand; ++k) s += coef[k] * V[(size_t)(k - 1) * n3 + i];
+    x0[i] = s;
+}
+
+}  // namespace
+
+// ---- state of the learned start guess (one per context) ---------------------------
+struct MlpState {
+    float *P = nullptr, *M = nullptr, *V = nullptr;  // FP32 parameters and Adam moments
+    __nv_bfloat16* W = nullptr;                      // packed BF16 inference weights
+    float* bias = nullptr;
+    int step = 0;                                    // Adam steps taken
+    bool ready = false;                              // parameters set
+    float *gpart = nullptr, *lpart = nullptr, *loss = nullptr;
+    int gcap = 0, lcap = 0;
+    // features scratch
+    int *dindex = nullptr, *ccount = nullptr;
+    int dcap = 0, ccap = 0, scap = 0;
+    double* S = nullptr;  // 3x3 block row sums, column-major
+    double *spart = nullptr, *scales = nullptr;
+    float *X = nullptr, *mask = nullptr;
+    int xcap = 0, mcap = 0;
+    double *cand = nullptr, *Acand = nullptr, *gpartial = nullptr, *coef = nullptr;  // Galerkin combination
+    int vcap = 0;
+};
+
+void mlp_free(sgmas_context* c) {
+    MlpState* m = c->mlp;
+    if (!m) return;
+    void* ptrs[] = {m->P, m->M, m->V, m->W, m->bias, m->gpart, m->lpart, m->loss, m->dindex, m->ccount,
+                    m->spart, m->scales, m->X, m->mask, m->S, m->cand, m->Acand, m->gpartial, m->coef};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete m;
+    c->mlp = nullptr;
+}
+
+static int mlp_state(sgmas_context* c, MlpState** out) {
+    if (!c->mlp) {
+        MlpState* m = new MlpState();
+        c->mlp = m;
+        if (ctx_alloc(c, &m->P, kParams) || ctx_alloc(c, &m->M, kParams) || ctx_alloc(c, &m->V, kParams) ||
+            ctx_alloc(c, &m->W, kPackBf16) || ctx_alloc(c, &m->bias, kPackBias) || ctx_alloc(c, &m->loss, 1) ||
+            ctx_alloc(c, &m->spart, 2 * 1024) || ctx_alloc(c, &m->scales, 2))
+            return SGMAS_ERR_CUDA;
+    }
+    *out = c->mlp;
+    return 0;
+}
+
+static int mlp_ready(sgmas_context* c, MlpState** out) {
+    int rc = mlp_state(c, out);
+    if (rc) return rc;
+    if (!(*out)->ready) return ctx_fail(c, SGMAS_ERR_STATE, "learned start guess used before sgmas_mlp_set_params");
+    return 0;
+}
+
+// features of the system in MAS slot order into X / mask (and T when dx is given)
+static int mlp_features(sgmas_context* c, MlpState* m, const sgmas_bcoo* A, const double* b, const double* prev,
+                        const double* dx, int fem_off, float* X, float* mask, float* T) {
+    const int N = c->N, Mm = c->Mm, nrows = A->n_block_rows;
+    cudaStream_t s = c->stream;
+    if (ctx_alloc_grow(c, &m->dindex, &m->dcap, nrows) || ctx_alloc_grow(c, &m->ccount, &m->ccap, N) ||
+        ctx_alloc_grow(c, &m->S, &m->scap, 9 * nrows))
+        return SGMAS_ERR_CUDA;
+    // the row-owned block CSR of A (kept for the solve that follows, see bsr_reuse)
+    int rc = bsr_build(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows);
+    if (rc) return rc;
+    bsr_mark_fresh(c, A);
+    k_row_sums<<<(nrows + 255) / 256, 256, 0, s>>>(nrows, c->bsr.row_ptr, c->bsr.vals, c->bsr.cap, m->S);
+    SG_CUDA(c, cudaMemsetAsync(m->dindex, 0xff, sizeof(int) * nrows, s));
+    SG_CUDA(c, cudaMemsetAsync(m->ccount, 0, sizeof(int) * N, s));
+    if (A->n_blocks > 0)
+        k_diag_index<<<(A->n_blocks + 255) / 256, 256, 0, s>>>(A->n_blocks, A->d_rows, A->d_cols, m->dindex);
+    if (c->cp_num > 0 && c->d_pairs)
+        k_contact_count<<<(c->cp_num + 255) / 256, 256, 0, s>>>(c->cp_num, (const int4*)c->d_pairs, c->node_offset,
+                                                                  N, m->ccount);
+    const int gs = std::max(1, std::min(1024, (N + 255) / 256));
+    k_feat_scales<<<gs, 256, 0, s>>>(N, fem_off, A->d_values, m->dindex, m->S, b, m->spart);
+    k_feat_scales_final<<<1, 256, 0, s>>>(gs, N, m->spart, m->scales);
+    k_features<<<(Mm + 255) / 256, 256, 0, s>>>(Mm, N, fem_off, c->d_part_map, A->d_values, m->dindex, m->S, b, prev,
+                                                dx, m->ccount, m->scales, X, mask, T);
+    SG_CUDA(c, cudaGetLastError());
+    c->build_launches += 6 + (c->cp_num > 0 ? 1 : 0);
+    return 0;
+}
+
+static int check_system(sgmas_context* c, const sgmas_bcoo* A, const double* b, int fem_off) {
+    if (!A || !b || A->n_block_rows < 1 || A->n_blocks < 0 || (A->n_blocks > 0 && (!A->d_values || !A->d_rows || !A->d_cols)))
+        return ctx_fail(c, SGMAS_ERR_ARG, "learned start guess: bad system");
+    if (!c->mas_init) return ctx_fail(c, SGMAS_ERR_STATE, "learned start guess needs the MAS partition (sgmas_mas_init)");
+    if (fem_off < 0 || fem_off + c->N > A->n_block_rows)
+        return ctx_fail(c, SGMAS_ERR_ARG, "MAS range [fem_offset, fem_offset + N) outside the system");
+    return 0;
+}
+
+extern "C" {
+
+int sgmas_mlp_set_params(sgmas_context* c, const float* params, int n) {
+    if (!c || !params || n != kParams) return c ? ctx_fail(c, SGMAS_ERR_ARG, "sgmas_mlp_set_params: need %d parameters", kParams) : SGMAS_ERR_ARG;
+    SG_CUDA(c, cudaSetDevice(c->device));
+    MlpState* m = nullptr;
+    int rc = mlp_state(c, &m);
+    if (rc) return rc;
+    SG_CUDA(c, cudaMemcpyAsync(m->P, params, sizeof(float) * kParams, cudaMemcpyHostToDevice, c->stream));
+    SG_CUDA(c, cudaMemsetAsync(m->M, 0, sizeof(float) * kParams, c->stream));
+    SG_CUDA(c, cudaMemsetAsync(m->V, 0, sizeof(float) * kParams, c->stream));
+    k_mlp_pack<<<(kPackBf16 + 255) / 256, 256, 0, c->stream>>>(m->P, m->W, m->bias);
+    SG_CUDA(c, cudaGetLastError());
+    SG_CUDA(c, cudaStreamSynchronize(c->stream));
+    m->step = 0;
+    m->ready = true;
+    return SGMAS_OK;
+}
+
+int sgmas_mlp_get_params(sgmas_context* c, float* params, int n) {
+    if (!c || !params || n != kParams) return SGMAS_ERR_ARG;
+    MlpState* m = nullptr;
+    int rc = mlp_ready(c, &m);
+    if (rc) return rc;
+    SG_CUDA(c, cudaMemcpyAsync(params, m->P, sizeof(float) * kParams, cudaMemcpyDeviceToHost, c->stream));
+    SG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return SGMAS_OK;
+}
+
+int sgmas_mlp_features(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, const double* d_prev,
+                       const double* d_dx, int fem_offset, float* d_X, float* d_mask, float* d_T, double* scales) {
+    if (!c || !d_X || !d_mask || (d_dx && !d_T)) return SGMAS_ERR_ARG;
+    int rc = check_system(c, A, d_b, fem_offset);
+    if (rc) return rc;
+    SG_CUDA(c, cudaSetDevice(c->device));
+    MlpState* m = nullptr;
+    rc = mlp_state(c, &m);
+    if (rc) return rc;
+    rc = mlp_features(c, m, A, d_b, d_prev, d_dx, fem_offset, d_X, d_mask, d_dx ? d_T : nullptr);
+    if (rc) return rc;
+    if (scales) {
+        SG_CUDA(c, cudaMemcpyAsync(scales, m->scales, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
+        SG_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return SGMAS_OK;
+}
+
+static int mlp_tiles(sgmas_context* c, MlpState* m, const float* X, const float* T, const float* mask, int n_rows,
+                     float inv_n) {
+    const int ntiles = (n_rows + kTileRows - 1) / kTileRows;
+    if (ctx_alloc_grow(c, &m->gpart, &m->gcap, ntiles * kParams) || ctx_alloc_grow(c, &m->lpart, &m->lcap, ntiles))
+        return SGMAS_ERR_CUDA;
+    SG_CUDA(c, cudaFuncSetAttribute(k_mlp_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem));
+    k_mlp_tile<<<ntiles, kTT, kTrainSmem, c->stream>>>(m->P, X, T, mask, n_rows, inv_n, 1, nullptr, m->gpart, m->lpart);
+    SG_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+static int check_rows(sgmas_context* c, int n_rows) {
+    if (n_rows < 16 || n_rows % 16 != 0)
+        return ctx_fail(c, SGMAS_ERR_ARG, "rows must be whole subdomains (a positive multiple of 16), got %d", n_rows);
+    return 0;
+}
+
+int sgmas_mlp_gradient(sgmas_context* c, const float* d_X, const float* d_T, const float* d_mask, int n_rows,
+                       float inv_n, float* d_grad, float* loss) {
+    if (!c || !d_X || !d_T || !d_mask || !d_grad) return SGMAS_ERR_ARG;
+    int rc = check_rows(c, n_rows);
+    if (rc) return rc;
+    SG_CUDA(c, cudaSetDevice(c->device));
+    MlpState* m = nullptr;
+    if ((rc = mlp_ready(c, &m)) || (rc = mlp_tiles(c, m, d_X, d_T, d_mask, n_rows, inv_n))) return rc;
+    const int ntiles = (n_rows + kTileRows - 1) / kTileRows;
+    k_mlp_reduce<<<(kParams + 255) / 256, 256, 0, c->stream>>>(ntiles, m->gpart, m->lpart, 0, 0.f, 1.f, 1.f, m->P,
+                                                                m->M, m->V, d_grad, m->loss);
+    SG_CUDA(c, cudaGetLastError());
+    if (loss) {
+        SG_CUDA(c, cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        SG_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return SGMAS_OK;
+}
+
+int sgmas_mlp_train_step(sgmas_context* c, const float* d_X, const float* d_T, const float* d_mask, int n_rows,
+                         float inv_n, float lr, float* loss) {
+    if (!c || !d_X || !d_T || !d_mask || !(lr > 0.f)) return SGMAS_ERR_ARG;
+    int rc = check_rows(c, n_rows);
+    if (rc) return rc;
+    SG_CUDA(c, cudaSetDevice(c->device));
+    MlpState* m = nullptr;
+    if ((rc = mlp_ready(c, &m)) || (rc = mlp_tiles(c, m, d_X, d_T, d_mask, n_rows, inv_n))) return rc;
+    const int ntiles = (n_rows + kTileRows - 1) / kTileRows;
+    m->step += 1;
+    const float c1 = (float)(1.0 - pow(kAdamB1, m->step)), c2 = (float)(1.0 - pow(kAdamB2, m->step));
+    k_mlp_reduce<<<(kParams + 255) / 256, 256, 0, c->stream>>>(ntiles, m->gpart, m->lpart, 1, lr, c1, c2, m->P, m->M,
+                                                                m->V, nullptr, m->loss);
+    k_mlp_pack<<<(kPackBf16 + 255) / 256, 256, 0, c->stream>>>(m->P, m->W, m->bias);
+    SG_CUDA(c, cudaGetLastError());
+    if (loss) {
+        SG_CUDA(c, cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        SG_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return SGMAS_OK;
+}
+
+int sgmas_mlp_forward(sgmas_context* c, const float* d_X, int n_rows, int bf16, float* d_Y) {
+    if (!c || !d_X || !d_Y) return SGMAS_ERR_ARG;
+    int rc = check_rows(c, n_rows);
+    if (rc) return rc;
+    SG_CUDA(c, cudaSetDevice(c->device));
+    MlpState* m = nullptr;
+    if ((rc = mlp_ready(c, &m))) return rc;
+    if (bf16) {
+        const int grid = std::min((n_rows / 16 + kIT / 32 - 1) / (kIT / 32), 4 * 148);
+        k_mlp_infer<<<grid, kIT, 0, c->stream>>>(n_rows, d_X, m->W, m->bias, 0, nullptr, 0, 0, nullptr, nullptr, nullptr,
+                                                 nullptr, nullptr, 0, nullptr, d_Y);
+    } else {
+        SG_CUDA(c, cudaFuncSetAttribute(k_mlp_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem));
+        k_mlp_tile<<<(n_rows + kTileRows - 1) / kTileRows, kTT, kTrainSmem, c->stream>>>(
+            m->P, d_X, nullptr, nullptr, n_rows, 0.f, 0, d_Y, nullptr, nullptr);
+    }
+    SG_CUDA(c, cudaGetLastError());
+    return SGMAS_OK;
+}
+
+int sgmas_mlp_warm_start(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, const double* d_prev,
+                         int fem_offset, double* d_x0, double* coef) {
+    if (!c || !d_x0) return SGMAS_ERR_ARG;
+    int rc = check_system(c, A, d_b, fem_offset);
+    if (rc) return rc;
+    SG_CUDA(c, cudaSetDevice(c->device));
+    MlpState* m = nullptr;
+    if ((rc = mlp_ready(c, &m))) return rc;
+    const int nrows = A->n_block_rows, n3 = 3 * nrows;
+    if (ctx_alloc_grow(c, &m->X, &m->xcap, 16 * c->Mm) || ctx_alloc_grow(c, &m->mask, &m->mcap, c->Mm))
+        return SGMAS_ERR_CUDA;
+    if (n3 > m->vcap) {
+        if (ctx_alloc(c, &m->cand, 3 * (size_t)n3) || ctx_alloc(c, &m->Acand, 4 * (size_t)n3) ||
+            ctx_alloc(c, &m->gpartial, (size_t)kGram * 1024) || ctx_alloc(c, &m->coef, kCand))
+            return SGMAS_ERR_CUDA;
+        m->vcap = n3;
+    }
+    c->build_launches = 0;
+    rc = mlp_features(c, m, A, d_b, d_prev, nullptr, fem_offset, m->X, m->mask, nullptr);
+    if (rc) return rc;
+    cudaStream_t s = c->stream;
+    SG_CUDA(c, cudaMemsetAsync(m->cand, 0, sizeof(double) * 3 * (size_t)n3, s));
+    const int grid = std::min((c->Mm / 16 + kIT / 32 - 1) / (kIT / 32), 4 * 148);
+    k_mlp_infer<<<grid, kIT, 0, s>>>(c->Mm, m->X, m->W, m->bias, 1, c->d_part_map, c->N, fem_offset, m->scales,
+                                     A->d_values, m->dindex, m->S, d_b, nrows, m->cand, nullptr);
+    SG_CUDA(c, cudaGetLastError());
+    // A v_k on the block CSR built for the features (row-owned, deterministic)
+    if (d_prev && (rc = bsr_spmv_plain(c, 1.0, d_prev, 0.0, m->Acand))) return rc;
+    for (int k = 1; k < kCand; ++k)
+        if ((rc = bsr_spmv_plain(c, 1.0, m->cand + (size_t)(k - 1) * n3, 0.0, m->Acand + (size_t)k * n3))) return rc;
+    const int gg = std::max(1, std::min(1024, (n3 + 255) / 256));
+    k_gram_partials<<<gg, 256, 0, s>>>(n3, d_prev, m->cand, m->Acand, d_b, m->gpartial);
+    k_gram_solve<<<1, 256, 0, s>>>(gg, m->gpartial, m->coef);
+    k_combine<<<(n3 + 255) / 256, 256, 0, s>>>(n3, d_prev, m->cand, m->coef, d_x0);
+    SG_CUDA(c, cudaGetLastError());
+    c->build_launches += 4 + (kCand - 1) + (d_prev ? 1 : 0);
+    if (coef) {
+        SG_CUDA(c, cudaMemcpyAsync(coef, m->coef, sizeof(double) * kCand, cudaMemcpyDeviceToHost, s));
+        SG_CUDA(c, cudaStreamSynchronize(s));
+    }
+    return SGMAS_OK;
+}
+
+}  // extern "C"

@@ -478,9 +478,27 @@ int ensure_partials(sgmas_context* c, int n) {
 
 }  // namespace
 
+void bsr_mark_fresh(sgmas_context* c, const sgmas_bcoo* A) {
+    c->bsr_src[0] = A->d_values;
+    c->bsr_src[1] = A->d_rows;
+    c->bsr_src[2] = A->d_cols;
+    c->bsr_src_nb = A->n_blocks;
+    c->bsr_src_nrows = A->n_block_rows;
+    c->bsr_fresh = true;
+}
+
+bool bsr_reuse(sgmas_context* c, const sgmas_bcoo* A) {
+    const bool same = c->bsr_fresh && c->bsr_src[0] == A->d_values && c->bsr_src[1] == A->d_rows &&
+                      c->bsr_src[2] == A->d_cols && c->bsr_src_nb == A->n_blocks &&
+                      c->bsr_src_nrows == A->n_block_rows;
+    c->bsr_fresh = false;
+    return same;
+}
+
 int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* cols, int nb, int nrows) {
     BsrMatrix& B = c->bsr;
     cudaStream_t s = c->stream;
+    c->bsr_fresh = false;
     if (nrows > B.rows_cap) {
         if (ctx_alloc(c, &B.row_ptr, (size_t)nrows + 1) || ctx_alloc(c, &B.cnt, nrows) ||
             ctx_alloc(c, &B.cnt_lower, nrows) || ctx_alloc(c, &B.fill, nrows) || ctx_alloc(c, &B.first, nrows) ||
@@ -881,7 +899,7 @@ int pcg_profile(sgmas_context* c, int reps, float* ms, int n_ms) {
 int pcg_prepare(sgmas_context* c, const sgmas_bcoo* A, const PcgRunCfg& cfg) {
     const int nrows = A->n_block_rows;
     if (ensure_vec(c, nrows)) return SGMAS_ERR_CUDA;
-    int rc = bsr_build(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows);
+    int rc = bsr_reuse(c, A) ? 0 : bsr_build(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows);
     if (rc) return rc;
     if (cfg.precond == 0) return jacobi_setup(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows, cfg.abd_bodies);
     if (cfg.abd_bodies > 0)  // MAS on the FEM range + 12x12 block-Jacobi on the bodies

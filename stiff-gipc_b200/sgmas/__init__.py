@@ -58,8 +58,10 @@ EXPORTS = [
     "sgmas_pcg_solve", "sgmas_pcg_solve_host", "sgmas_spmv", "sgmas_convert", "sgmas_write_upper_blocks",
     "sgmas_morton_codes", "sgmas_morton_partition", "sgmas_pcg_profile", "sgmas_vert_neighbors",
     "sgmas_part_maps", "sgmas_morton_codes_noalloc", "sgmas_set_pcg_mode", "sgmas_pcg_last_vectors",
-    "sgmas_mtx_write", "sgmas_mtx_read",
+    "sgmas_mtx_write", "sgmas_mtx_read", "sgmas_mlp_set_params", "sgmas_mlp_get_params", "sgmas_mlp_features",
+    "sgmas_mlp_gradient", "sgmas_mlp_train_step", "sgmas_mlp_forward", "sgmas_mlp_warm_start",
 ]
+MLP_PARAMS = 19462  # SGMAS_MLP_PARAMS in include/sgmas.h
 
 MORTON_NOALLOC_MAX_VERTS = 2097152  # SGMAS_MORTON_NOALLOC_MAX_VERTS in include/sgmas.h
 
@@ -105,6 +107,14 @@ def lib(build_if_missing: bool = False):
     L.sgmas_pcg_last_vectors.argtypes = [vp, vp, vp]
     L.sgmas_mtx_write.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, i, vp]
     L.sgmas_mtx_read.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, vp, i, C.POINTER(i), C.POINTER(i)]
+    f = C.c_float
+    L.sgmas_mlp_set_params.argtypes = [vp, vp, i]
+    L.sgmas_mlp_get_params.argtypes = [vp, vp, i]
+    L.sgmas_mlp_features.argtypes = [vp, C.POINTER(Bcoo), vp, vp, vp, i, vp, vp, vp, vp]
+    L.sgmas_mlp_gradient.argtypes = [vp, vp, vp, vp, i, f, vp, C.POINTER(f)]
+    L.sgmas_mlp_train_step.argtypes = [vp, vp, vp, vp, i, f, f, C.POINTER(f)]
+    L.sgmas_mlp_forward.argtypes = [vp, vp, i, i, vp]
+    L.sgmas_mlp_warm_start.argtypes = [vp, C.POINTER(Bcoo), vp, vp, i, vp, vp]
     _lib = L
     return L
 
@@ -325,6 +335,48 @@ class Context:
         self._check(self.L.sgmas_pcg_solve_host(self.h, _ptr(vals), _ptr(rows), _ptr(cols), len(rows),
                                                 n_block_rows, _ptr(b), _ptr(x), C.byref(c), C.byref(rep)))
         return x, {k: getattr(rep, k) for k, _ in PcgReport._fields_}
+
+    # ---- learned start guess ----
+    def mlp_set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        self._check(self.L.sgmas_mlp_set_params(self.h, _ptr(p), len(p)))
+
+    def mlp_get_params(self):
+        p = np.zeros(MLP_PARAMS, np.float32)
+        self._check(self.L.sgmas_mlp_get_params(self.h, _ptr(p), MLP_PARAMS))
+        return p
+
+    def mlp_features(self, vals, rows, cols, n_block_rows, b, X, mask, prev=None, dx=None, T=None, fem_offset=0):
+        """Slot-ordered features into device arrays X [Mm*16], mask [Mm] (+ T [Mm*3] from dx); returns (s_y, s_b)."""
+        A = self.bcoo(vals, rows, cols, n_block_rows)
+        sc = np.zeros(2)
+        self._check(self.L.sgmas_mlp_features(self.h, C.byref(A), _ptr(b), _ptr(prev), _ptr(dx), fem_offset, _ptr(X),
+                                              _ptr(mask), _ptr(T), _ptr(sc)))
+        return float(sc[0]), float(sc[1])
+
+    def mlp_gradient(self, X, T, mask, n_rows, inv_n, grad):
+        loss = C.c_float()
+        self._check(self.L.sgmas_mlp_gradient(self.h, _ptr(X), _ptr(T), _ptr(mask), n_rows, inv_n, _ptr(grad),
+                                              C.byref(loss)))
+        return loss.value
+
+    def mlp_train_step(self, X, T, mask, n_rows, inv_n, lr, want_loss=True):
+        loss = C.c_float()
+        self._check(self.L.sgmas_mlp_train_step(self.h, _ptr(X), _ptr(T), _ptr(mask), n_rows, inv_n, lr,
+                                                C.byref(loss) if want_loss else None))
+        return loss.value if want_loss else None
+
+    def mlp_forward(self, X, n_rows, Y, bf16=True):
+        self._check(self.L.sgmas_mlp_forward(self.h, _ptr(X), n_rows, int(bool(bf16)), _ptr(Y)))
+
+    def mlp_warm_start(self, vals, rows, cols, n_block_rows, b, x0, prev=None, fem_offset=0, coef=False):
+        """x0 <- the learned start guess; with coef=True also returns the Galerkin
+        coefficients of (previous step, lumped step, network step, network coarse term)."""
+        A = self.bcoo(vals, rows, cols, n_block_rows)
+        c = np.zeros(4) if coef else None
+        self._check(self.L.sgmas_mlp_warm_start(self.h, C.byref(A), _ptr(b), _ptr(prev), fem_offset, _ptr(x0),
+                                                _ptr(c)))
+        return c
 
     def pcg_profile(self, reps=20):
         """Per-phase device ms of one iteration of the last solve (sgmas_pcg_profile)."""
