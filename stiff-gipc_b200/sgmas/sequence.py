@@ -169,8 +169,12 @@ class DropScene:
                         torch.cat([-hat(f1), hat(f0), z3], 2)], 1)
         HF = mu * torch.eye(9, dtype=F.dtype, device=F.device)[None] + lam * g[:, :, None] * g[:, None, :] + \
             (lam * (J - alpha))[:, None, None] * HJ
-        w, V = torch.linalg.eigh(HF)
-        HF = (V * torch.clamp(w, min=0.0)[:, None, :]) @ V.transpose(1, 2)
+        # PSD projection, in chunks (the batched eigensolver limits the batch size)
+        parts = []
+        for i0 in range(0, len(HF), 16384):
+            w, V = torch.linalg.eigh(HF[i0:i0 + 16384])
+            parts.append((V * torch.clamp(w, min=0.0)[:, None, :]) @ V.transpose(1, 2))
+        HF = torch.cat(parts)
         He = self.t_vol[:, None, None] * (self.t_dFdx.transpose(1, 2) @ HF @ self.t_dFdx)
         ge = self.t_vol[:, None] * (self.t_dFdx.transpose(1, 2) @ P[:, :, None])[:, :, 0]
         return He, ge
