@@ -863,13 +863,15 @@ static void chol_factor(const double* packed, int b, double* out_packed)
     }
     for(int j = 0; j < n; j++)
         dW[j] = 1.0 / A[(size_t)j * n + j];
+    /* W_ij (i > j) = acc / L_ii with acc = +0 then acc = fma(-L_ik, W_kj, acc)
+       for k = j .. i-1 ascending (W_jj = 1 / L_jj) */
     for(int j = 0; j < n; j++)
         for(int i = j + 1; i < n; i++)
         {
-            double sum = 0.0;
+            double acc = 0.0;
             for(int k = j; k < i; k++)
-                sum = fma(A[(size_t)i * n + k], k == j ? dW[j] : A[(size_t)j * n + k], sum);
-            A[(size_t)j * n + i] = -sum / A[(size_t)i * n + i];
+                acc = fma(-A[(size_t)i * n + k], k == j ? dW[j] : A[(size_t)j * n + k], acc);
+            A[(size_t)j * n + i] = acc / A[(size_t)i * n + i];
         }
     for(int rb = 0; rb < b; rb++)
         for(int cb = rb; cb < b; cb++)

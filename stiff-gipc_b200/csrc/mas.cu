@@ -515,58 +515,76 @@ __global__ void __launch_bounds__(32 * inv_warps<B>()) k_invert(int nblk, const 
 
 // Factored inverse of one subdomain matrix per warp (storage Fact<T>): lower
 // Cholesky M = L L^T in FP64 (right-looking; a pivot that is not positive
-// becomes 1), then W = L^-1 column by column (one lane per column); the tile
-// slot (rb, cb), rb <= cb, receives block (cb, rb) of W.  Every element's
-// operations run in one fixed order (fma for each update), restated by the
-// oracle.  The padding rows of a bank (zero diagonal) become identity, as
-// the reference's inverse does (:628-724).
+// becomes 1), then W = L^-1; the tile slot (rb, cb), rb <= cb, receives block
+// (cb, rb) of W.  Every element's operations run in one fixed order (fma for
+// each update; W_ij = acc / L_ii with acc = fma(-L_ik, W_kj, acc) over
+// k = j .. i-1 ascending), restated by the oracle.  The padding rows of a bank
+// (zero diagonal) become identity, as the reference's inverse does
+// (:628-724).  The matrix sits in shared memory with a padded row stride
+// (n + 1 doubles) so that lanes walking down a column hit distinct banks;
+// W = L^-1 is formed row by row (step k finishes row k of W, then every later
+// row takes its term k: independent updates across lanes), L in the lower
+// triangle, W^T accumulating in the upper.
+template <int B>
+__host__ __device__ constexpr int chol_ld() { return 3 * B + 1; }
+// shared memory per warp (doubles) of k_chol_inv / k_invert
+template <int B>
+constexpr size_t inv_smem_doubles(bool fact) {
+    return fact ? (size_t)3 * B * chol_ld<B>() + 3 * B : (size_t)9 * B * B + 3 * B;
+}
+
 template <int B, typename S>
 __global__ void __launch_bounds__(32 * inv_warps<B>()) k_chol_inv(int nblk, const double* __restrict__ hess, S* inv,
                                                                  double* inv64, const int* __restrict__ level_size,
                                                                  int L) {
     constexpr int n = 3 * B;
+    constexpr int ld = chol_ld<B>();
     constexpr int bs = bsym_of(B);
     extern __shared__ double smem_inv[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mat = blockIdx.x * inv_warps<B>() + w;
     const int limit = level_size ? level_size[2 * L + 1] / B : nblk;
     if (mat >= nblk || mat >= limit) return;
-    double* A = smem_inv + (size_t)w * (n * n + n);  // row-major; L in the lower triangle, W^T in the upper
-    double* dW = A + n * n;                         // diagonal of W
+    double* A = smem_inv + (size_t)w * (n * ld + n);  // row-major, stride ld; L lower, W^T upper
+    double* dW = A + n * ld;                         // diagonal of W
     const double* P = hess + (size_t)mat * bs * 9;
-    for (int e = lane; e < n * n; e += 32) {  // lower triangle of M
+    for (int e = lane; e < n * n; e += 32) {  // lower triangle of M; the upper accumulates W^T from 0
         const int i = e / n, j = e % n;
-        if (j > i) continue;
+        if (j > i) { A[i * ld + j] = 0.0; continue; }
         const int rb = j / 3, cb = i / 3;
         double v = rb == cb ? P[sym_index(B, rb, rb) * 9 + (i % 3) + 3 * (j % 3)]
                             : P[sym_index(B, rb, cb) * 9 + (j % 3) + 3 * (i % 3)];
         if (i == j && v == 0.0) v = 1.0;
-        A[e] = v;
+        A[i * ld + j] = v;
     }
     __syncwarp();
     for (int k = 0; k < n; ++k) {
-        double d = A[k * n + k];
+        double d = A[k * ld + k];
         if (!(d > 0.0)) d = 1.0;
         const double lkk = sqrt(d);
-        for (int i = k + 1 + lane; i < n; i += 32) A[i * n + k] = A[i * n + k] / lkk;
+        for (int i = k + 1 + lane; i < n; i += 32) A[i * ld + k] = A[i * ld + k] / lkk;
         __syncwarp();
-        if (lane == 0) A[k * n + k] = lkk;
+        if (lane == 0) A[k * ld + k] = lkk;
         for (int i = k + 1 + lane; i < n; i += 32) {
-            const double lik = A[i * n + k];
-            for (int j = k + 1; j <= i; ++j) A[i * n + j] = __fma_rn(-lik, A[j * n + k], A[i * n + j]);
+            const double lik = A[i * ld + k];
+            for (int j = k + 1; j <= i; ++j) A[i * ld + j] = __fma_rn(-lik, A[j * ld + k], A[i * ld + j]);
         }
         __syncwarp();
     }
-    for (int j = lane; j < n; j += 32) dW[j] = 1.0 / A[j * n + j];
+    for (int j = lane; j < n; j += 32) dW[j] = 1.0 / A[j * ld + j];
     __syncwarp();
-    for (int j = lane; j < n; j += 32) {
-        for (int i = j + 1; i < n; ++i) {
-            double sum = 0.0;
-            for (int k = j; k < i; ++k) sum = __fma_rn(A[i * n + k], k == j ? dW[j] : A[j * n + k], sum);
-            A[j * n + i] = -sum / A[i * n + i];
+    for (int k = 0; k < n; ++k) {
+        // row k of W is complete: W_kj = acc_kj / L_kk (stored at A[j][k])
+        for (int j = lane; j < k; j += 32) A[j * ld + k] = A[j * ld + k] / A[k * ld + k];
+        __syncwarp();
+        // every later row i takes its term k: acc_ij = fma(-L_ik, W_kj, acc_ij), j <= k
+        for (int i = k + 1 + lane; i < n; i += 32) {
+            const double lik = A[i * ld + k];
+            for (int j = 0; j < k; ++j) A[j * ld + i] = __fma_rn(-lik, A[j * ld + k], A[j * ld + i]);
+            A[k * ld + i] = __fma_rn(-lik, dW[k], A[k * ld + i]);
         }
+        __syncwarp();
     }
-    __syncwarp();
     S* out = inv + (size_t)mat * bs * 9;
     for (int e = lane; e < bs * 9; e += 32) {
         const int b = e / 9, q = e % 9;
@@ -574,7 +592,7 @@ __global__ void __launch_bounds__(32 * inv_warps<B>()) k_chol_inv(int nblk, cons
         while (off + (B - rb) <= b) { off += B - rb; ++rb; }
         const int cb = rb + (b - off);
         const int i = 3 * cb + q % 3, j = 3 * rb + q / 3;  // element (i, j) of W
-        const double v = i > j ? A[j * n + i] : (i == j ? dW[i] : 0.0);
+        const double v = i > j ? A[j * ld + i] : (i == j ? dW[i] : 0.0);
         out[e] = Store<S>::from_double(v);
         if (inv64) inv64[(size_t)mat * bs * 9 + e] = v;
     }
@@ -918,7 +936,7 @@ int scatter_invert_t(sgmas_context* c, const double* vals, const int* rows, cons
                                                      c->d_hess);
     }
     constexpr int W = inv_warps<B>();
-    const size_t smem = (size_t)W * (9 * B * B + 3 * B) * sizeof(double);
+    const size_t smem = (size_t)W * inv_smem_doubles<B>(is_fact<S>::value) * sizeof(double);
     auto kern = is_fact<S>::value ? k_chol_inv<B, S> : k_invert<B, S>;
     SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<(nblk + W - 1) / W, 32 * W, smem, s>>>(nblk, c->d_hess, (S*)c->d_inv, nullptr, c->d_level_size, c->L);
@@ -1023,12 +1041,12 @@ int mas_invert_blocks_dev(sgmas_context* c, const double* hess, int nblk, double
     SG_CUDA(c, cudaMallocAsync((void**)&tmp, sizeof(float) * nblk * bs * 9, s));
     const bool fact = c->precision == SGMAS_MAS_BF16 || c->precision == SGMAS_MAS_FP32_FACTORED;
     if (c->bank == 16) {
-        const size_t smem = (size_t)inv_warps<16>() * (9 * 16 * 16 + 48) * sizeof(double);
+        const size_t smem = (size_t)inv_warps<16>() * inv_smem_doubles<16>(fact) * sizeof(double);
         auto kern = fact ? k_chol_inv<16, float> : k_invert<16, float>;
         SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<(nblk + 3) / 4, 128, smem, s>>>(nblk, hess, tmp, out64, nullptr, 0);
     } else {
-        const size_t smem = (size_t)(9 * 32 * 32 + 96) * sizeof(double);
+        const size_t smem = inv_smem_doubles<32>(fact) * sizeof(double);
         auto kern = fact ? k_chol_inv<32, float> : k_invert<32, float>;
         SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<nblk, 32, smem, s>>>(nblk, hess, tmp, out64, nullptr, 0);
