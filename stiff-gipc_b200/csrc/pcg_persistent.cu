@@ -384,6 +384,10 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     // ---- ownership, per-thread constants, cached tiles ----------------------
     Own o = {0, 0, 0, 0};
     int v = -1, n1loc = -1, par1 = -1;
+    // level-1 bank of this half-warp: the level-1 banks go to the CTA's last
+    // warps (hw1 = hw - base1), which have no level-0 bank unless the CTA has
+    // nearly 32 of them, so the level-1 products run beside the level-0 ones
+    int hw1 = -1;
     int vo = 0;  // 3 * (global row of vertex v)
     unsigned msk = 0u;
     bool own = false;
@@ -459,22 +463,28 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                 own = true;
             }
         }
-        if (a.L > 2 && hw < o.nbk1) {
-            const int i1 = (o.j0 + hw) * B + lane;
+        hw1 = TG ? hw : hw - (kPT / B - ((o.nbk1 + HPW - 1) / HPW) * HPW);
+        if (a.L > 2 && hw1 >= 0 && hw1 < o.nbk1) {
+            const int i1 = (o.j0 + hw1) * B + lane;
             if (i1 < a.lvl_count[1]) par1 = a.going_next[a.lvl_begin[1] + i1] - a.lvl_begin[2];
         }
         ok = mbar_wait(&mbar, mphase, a.err);
         mphase ^= 1u;
     }
     const bool act0 = (hw / HPW) * HPW < o.nbk0;  // this warp has level-0 work
-    const bool act1 = (hw / HPW) * HPW < o.nbk1;  // this warp has level-1 work
+    // level-1 work: the last warps, or (tiles in global memory, where the
+    // level-0 products are memory-bound) the first warps after the level-0 products
+    const bool act1 = TG ? (hw / HPW) * HPW < o.nbk1
+                         : o.nbk1 > 0 && (hw / HPW) * HPW >= kPT / B - ((o.nbk1 + HPW - 1) / HPW) * HPW;
 
     // ---- MAS pieces on the registers of this thread's slot ----------------
     double x0 = 0.0, x1 = 0.0, x2 = 0.0, r0 = 0.0, r1 = 0.0, r2 = 0.0;
     Acc zl0 = 0, zl1 = 0, zl2 = 0;  // level-0 Schwarz of the slot
     // level-0 (+ level-1) part of the apply on r (registers)
     auto apply_b = [&]() {
-        if (act0) {
+        // level-0 tiles: shared memory, or global memory when they did not fit
+        const S* t0 = TG && a.t0g ? (const S*)a.inv + (size_t)o.lo * tb : tiles0;
+        if (act0) {  // the slot's r into the bank exchange, level-0 component sums -> level-1 residuals
             Acc* xb = bank_slot<B>(xch);
             xch_put(xb, lane, (Acc)r0, (Acc)r1, (Acc)r2);
             Acc s0, s1, s2;
@@ -482,15 +492,17 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             if (own && a.L >= 2 && __popc(msk & lanemask_lt(lane)) == 0) {
                 R1s[3 * n1loc] = s0; R1s[3 * n1loc + 1] = s1; R1s[3 * n1loc + 2] = s2;
             }
-            // level-0 tiles: shared memory, or global memory when they did not fit
-            const S* t0 = TG && a.t0g ? (const S*)a.inv + (size_t)o.lo * tb : tiles0;
-            schwarz_rows<B, S, Acc>(t0 + (size_t)(hw < o.nbk0 ? hw : 0) * tb, lane, xb, zl0, zl1, zl2);
         }
-        if (a.L < 2) return;
-        __syncthreads();
+        if (TG || a.L < 2) {
+            if (act0) schwarz_rows<B, S, Acc>(t0 + (size_t)(hw < o.nbk0 ? hw : 0) * tb, lane, bank_slot<B>(xch), zl0, zl1, zl2);
+            if (a.L < 2) return;
+        }
+        __syncthreads();  // level-1 residuals complete
+        if (!TG && act0)  // level-0 Schwarz on r (still in the bank exchange)
+            schwarz_rows<B, S, Acc>(t0 + (size_t)(hw < o.nbk0 ? hw : 0) * tb, lane, bank_slot<B>(xch), zl0, zl1, zl2);
         if (act1) {  // level-1 banks of this CTA: push to level 2, Schwarz
-            const bool valid = hw < o.nbk1;
-            const int i = hw * B + lane;
+            const bool valid = hw1 >= 0 && hw1 < o.nbk1;
+            const int i = (valid ? hw1 : 0) * B + lane;
             const Acc v0 = valid ? R1s[3 * i] : (Acc)0, v1 = valid ? R1s[3 * i + 1] : (Acc)0,
                       v2 = valid ? R1s[3 * i + 2] : (Acc)0;
             Acc* xb = bank_slot<B>(xch);
@@ -506,7 +518,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             }
             Acc z0, z1, z2;
             const S* t1 = TG && a.t1g ? (const S*)a.inv + (size_t)(a.lvl_begin[1] / B + o.j0) * tb : tiles1;
-            schwarz_rows<B, S, Acc>(t1 + (size_t)(valid ? hw : 0) * tb, lane, xb, z0, z1, z2);
+            schwarz_rows<B, S, Acc>(t1 + (size_t)(valid ? hw1 : 0) * tb, lane, xb, z0, z1, z2);
             if (valid) { Z1s[3 * i] = z0; Z1s[3 * i + 1] = z1; Z1s[3 * i + 2] = z2; }
         }
         __syncthreads();
