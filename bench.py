@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--workload", default="c2", choices=["c2", "c4", "c5"],
                     help="c2: the headline contact solve; c5: batched uneven scenes (throughput, p50/p99)")
     ap.add_argument("--c5-scenes", type=int, default=64)
+    ap.add_argument("--c5-big-alone", action="store_true",
+                    help="config 5: scenes that fill every SM run one at a time (lower latency, lower throughput)")
+    ap.add_argument("--c5-streams", type=int, default=8,
+                    help="config 5: concurrent solves (one host thread, context and stream each); 1 = one after another")
     ap.add_argument("--c5-precision", default="bf16", choices=["bf16", "fp32", "fp64"])
     ap.add_argument("--variants", default="bf16,fp32,fp32f,fp64,jacobi,fp32-graph",
                     help="MAS storage precision (or jacobi); suffix -graph = kernel-per-phase CUDA graph "
@@ -697,10 +701,17 @@ def reduce_batch_timings(total_ms, dofs, lat, dev):
 def run_c5(args):
     """Config 5, batched serving of uneven scenes: 64 tet-grid systems (N
     log-uniform in [2k, 200k] x scale, E log-uniform in [1e4, 1e8], barrier
-    pairs 0-20 % of N).  Scenes are sharded across ranks by cost (blocks);
-    each rank solves its scenes one after another (BF16-factored MAS-PCG,
-    persistent form where a scene fits, graph form otherwise).  Prints one
-    JSON line: p50 / p99 per-scene solve latency and throughput."""
+    pairs 0-20 % of N).  Scenes are sharded across ranks by cost (blocks).
+    On each rank, --c5-streams host threads take scenes from a queue (largest
+    first), each with its own context and stream, and solve them
+    (BF16-factored MAS-PCG, persistent form on a grid sized to the scene --
+    about 20 level-0 subdomains per CTA -- so that small scenes share the GPU;
+    graph form where a scene does not fit).  Inputs are uploaded before the
+    timed pass; one untimed pass first.  Prints one JSON line: p50 / p99
+    per-scene solve latency (CUDA events on the scene's stream) and the
+    throughput of the timed pass (CUDA events around it, max over ranks)."""
+    import queue
+    import threading
     import torch
     import sgmas
     from sgmas import synth
@@ -712,45 +723,98 @@ def run_c5(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream()
     t0 = time.time()
     scenes = synth.config5(seed=0, n_scenes=args.c5_scenes, scale=args.scale)
     gen_s = time.time() - t0
     mine = shard_by_cost([len(sc.rows) for sc in scenes], world)[rank]
+    order = sorted(mine, key=lambda k: -len(scenes[k].rows))
 
     def tdev(a):
         return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
 
-    lat, forms, iters, dofs = [], [], [], 0
-    total_ms = 0.0
-    for k in sorted(mine):
+    nstreams = max(1, args.c5_streams)
+    streams = [torch.cuda.Stream(device=dev) for _ in range(nstreams)]
+    data = {}
+    for k in order:
         s = scenes[k]
-        vals, rows, cols, b, pos = tdev(s.vals), tdev(s.rows), tdev(s.cols), tdev(s.b), tdev(s.pos)
-        pairs = tdev(s.pairs if len(s.pairs) else np.zeros((1, 4), np.int32))
-        ctx = sgmas.Context(local, bank=16, precision=args.c5_precision)
-        ctx.set_stream(stream.cuda_stream)
-        pm, rm = ctx.morton_partition(pos)
-        ctx.mas_init(s.n_verts, *sgmas.vert_neighbors(s.tets, s.n_verts), pm, rm)
-        ctx.mas_set_contacts(pairs, len(s.pairs))
-        x = torch.zeros_like(b)
-        kw = dict(rel_tol=REL_TOL, max_iter=MAX_ITER, preconditioner="mas")
-        for _ in range(max(1, args.warmup // 3)):
-            ctx.pcg_solve(vals, rows, cols, s.n_verts, b, x, **kw)
-        for _ in range(max(1, min(args.steps, 3))):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            rep = ctx.pcg_solve(vals, rows, cols, s.n_verts, b, x, **kw)
-            e1.record(stream)
-            e1.synchronize()
-            ms = e0.elapsed_time(e1)
-            lat.append(ms)
-            total_ms += ms
-            dofs += 3 * s.n_verts
-            forms.append("persistent" if rep["kernel_launches"] == 1 else "graph")
-            iters.append(rep["iterations"])
+        data[k] = dict(vals=tdev(s.vals), rows=tdev(s.rows), cols=tdev(s.cols), b=tdev(s.b), pos=tdev(s.pos),
+                       pairs=tdev(s.pairs if len(s.pairs) else np.zeros((1, 4), np.int32)),
+                       x=torch.zeros(3 * s.n_verts, dtype=torch.float64, device=dev))
+    torch.cuda.synchronize()
+    ctxs = {}
+    kw = dict(rel_tol=REL_TOL, max_iter=MAX_ITER, preconditioner="mas")
+    lock = threading.Lock()
+    q = queue.Queue()
+    lat, forms, iters, errs = [], [], [], []
+
+    def worker(w, timed):
+        st = streams[w]
+        while True:
+            try:
+                k = q.get_nowait()
+            except queue.Empty:
+                return
+            s, dd = scenes[k], data[k]
+            try:
+                with torch.cuda.stream(st):
+                    if k not in ctxs:
+                        ctx = sgmas.Context(local, bank=16, precision=args.c5_precision)
+                        ctx.set_stream(st.cuda_stream)
+                        pm, rm = ctx.morton_partition(dd["pos"])
+                        ctx.mas_init(s.n_verts, *sgmas.vert_neighbors(s.tets, s.n_verts), pm, rm)
+                        ctx.mas_set_contacts(dd["pairs"], len(s.pairs))
+                        ctx.set_pcg_ctas(0 if k in big else min(n_sm, max(1, -(-len(pm) // (16 * 20)))))
+                        ctxs[k] = ctx
+                    ctx = ctxs[k]
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(st)
+                    rep = ctx.pcg_solve(dd["vals"], dd["rows"], dd["cols"], s.n_verts, dd["b"], dd["x"], **kw)
+                    e1.record(st)
+                    e1.synchronize()
+                if timed:
+                    with lock:
+                        lat.append(e0.elapsed_time(e1))
+                        forms.append("persistent" if rep["kernel_launches"] == 1 else "graph")
+                        iters.append(rep["iterations"])
+            except Exception as e:  # reported below
+                errs.append(repr(e))
+
+    # with --c5-big-alone, scenes that fill every SM (>= 20 level-0 subdomains per CTA on all
+    # of them, or the graph form) run one at a time and only the smaller ones share the GPU
+    def cap(k):
+        return max(1, -(-scenes[k].n_verts // (16 * 20)))
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    big = [k for k in order if nstreams == 1 or (args.c5_big_alone and cap(k) >= n_sm)]
+    small = [k for k in order if k not in big]
+
+    def one_pass(timed):
+        for group, nw in ((big, 1), (small, nstreams)):
+            for k in group:
+                q.put(k)
+            th = [threading.Thread(target=worker, args=(w, timed)) for w in range(min(nw, max(1, len(group))))]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+
+    one_pass(False)                       # contexts + hierarchy set-up, first solves (untimed)
+    torch.cuda.synchronize()
+    reps_timed = max(1, min(args.steps, 3))
+    w0 = torch.cuda.Event(enable_timing=True)
+    w1 = torch.cuda.Event(enable_timing=True)
+    w0.record()
+    for _ in range(reps_timed):
+        one_pass(True)
+    torch.cuda.synchronize()
+    w1.record()
+    w1.synchronize()
+    if errs:
+        raise RuntimeError("config-5 solves failed: " + "; ".join(errs[:3]))
+    total_ms = w0.elapsed_time(w1)
+    dofs = reps_timed * sum(3 * scenes[k].n_verts for k in order)
+    for ctx in ctxs.values():
         ctx.close()
-        del vals, rows, cols, b, pos, pairs, x
     if world > 1:
         import torch.distributed as dist
         wall_ms, dofs, lat = reduce_batch_timings(total_ms, dofs, lat, dev)
@@ -774,7 +838,12 @@ def run_c5(args):
                                            "forms": {f: forms.count(f) for f in set(forms)},
                                            "iterations_p50": int(sorted(iters)[len(iters) // 2]) if iters else 0,
                                            "gen_s": round(gen_s, 1),
-                                           "note": "scenes solved one after another per rank (not one launch)"}}
+                                           "concurrent_solves": max(1, args.c5_streams),
+                                           "scenes_alone": len(big), "scenes_shared": len(small),
+                                           "note": "scenes solved concurrently from per-stream host threads, "
+                                                   "each persistent solve on a grid sized to its scene"
+                                                   + ("; scenes filling every SM one at a time" if args.c5_big_alone else "")
+                                                   if args.c5_streams > 1 else "scenes solved one after another per rank"}}
     print(json.dumps(out))
 
 

@@ -173,6 +173,12 @@ int sgmas_pcg_last_vectors(sgmas_context* ctx, double* d_r, double* d_z);
 #define SGMAS_PCG_GRAPH 0
 #define SGMAS_PCG_PERSISTENT 1
 int sgmas_set_pcg_mode(sgmas_context* ctx, int mode);
+/* At most max_ctas CTAs (one per SM) for the persistent form; 0 (default) =
+ * every SM.  A small system solved on a few SMs leaves the rest to solves of
+ * other contexts on other streams (batched serving of many scenes): the
+ * cooperative launches of such solves run side by side.  A system needing
+ * more than 32 level-0 subdomains per CTA falls back to the graph form. */
+int sgmas_set_pcg_ctas(sgmas_context* ctx, int max_ctas);
 /* the same with host arrays: uploads A and b, solves, downloads x */
 int sgmas_pcg_solve_host(sgmas_context* ctx, const double* values, const int* rows,
                          const int* cols, int n_blocks, int n_block_rows, const double* b,

@@ -509,6 +509,13 @@ int sgmas_set_pcg_mode(sgmas_context* c, int mode) {
     return SGMAS_OK;
 }
 
+int sgmas_set_pcg_ctas(sgmas_context* c, int max_ctas) {
+    if (!c) return SGMAS_ERR_ARG;
+    if (max_ctas < 0) return ctx_fail(c, SGMAS_ERR_ARG, "max_ctas must be >= 0 (0: one CTA per SM)");
+    c->pcg_ctas = max_ctas;
+    return SGMAS_OK;
+}
+
 int sgmas_pcg_profile(sgmas_context* c, int reps, float* ms, int n_ms) {
     if (!c || reps < 1 || !ms || n_ms < 1) return SGMAS_ERR_ARG;
     SG_CUDA(c, cudaSetDevice(c->device));

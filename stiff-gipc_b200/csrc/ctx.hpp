@@ -119,6 +119,7 @@ struct sgmas_context {
     unsigned* d_coarse_ticket = nullptr;  // last-CTA ticket of the coarse MAS kernel
     unsigned* d_psync = nullptr;          // grid barrier + ticket of the persistent PCG kernel
     bool persistent = true;               // solve with the persistent kernel when the system fits
+    int pcg_ctas = 0;                     // CTAs of the persistent kernel (0: one per SM)
     bool last_persistent = false;         // the last solve ran the persistent kernel
     PcgRunCfg last_run = {};
     unsigned long long* d_stamps = nullptr;  // phase clock stamps of a profiled persistent solve

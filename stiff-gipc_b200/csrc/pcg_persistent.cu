@@ -782,7 +782,7 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
     cudaFuncAttributes fa;  // both instantiations have the same static shared memory
     SG_CUDA(c, cudaFuncGetAttributes(&fa, k_pcg_persistent<B, S, Acc, false>));
     const size_t budget = (size_t)max_smem - fa.sharedSizeBytes - 256;  // minus the kernel's static shared memory
-    const int G = dev_sms;
+    const int G = c->pcg_ctas > 0 ? std::min(dev_sms, c->pcg_ctas) : dev_sms;  // CTAs of this solve
     size_t smem = 0;
     if (a.precond == 1) {
         a.nb0 = a.Mm / B;
@@ -873,7 +873,9 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
         smem += (size_t)a.upw * per_unit;
     }
     auto kern = (a.t0g || a.t1g) ? k_pcg_persistent<B, S, Acc, true> : k_pcg_persistent<B, S, Acc, false>;
-    SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 1)));
+    // the attribute is per function, shared by every context and host thread: always the full
+    // budget, so that a concurrent launch never finds it below its own request
+    SG_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
     int per_sm = 0;
     SG_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPT, smem));
     if (per_sm < 1) return 1;

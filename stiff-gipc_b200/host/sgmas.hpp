@@ -39,6 +39,8 @@ class Context {
     void set_stream(void* s) { check(ctx_, sgmas_set_stream(ctx_, s), "sgmas_set_stream"); }
     // SGMAS_PCG_PERSISTENT (default) or SGMAS_PCG_GRAPH
     void set_pcg_mode(int mode) { check(ctx_, sgmas_set_pcg_mode(ctx_, mode), "sgmas_set_pcg_mode"); }
+    // at most max_ctas CTAs for the persistent form (0: every SM); for solves of many contexts side by side
+    void set_pcg_ctas(int max_ctas) { check(ctx_, sgmas_set_pcg_ctas(ctx_, max_ctas), "sgmas_set_pcg_ctas"); }
 
   private:
     sgmas_context* ctx_ = nullptr;

@@ -58,7 +58,7 @@ EXPORTS = [
     "sgmas_pcg_solve", "sgmas_pcg_solve_host", "sgmas_spmv", "sgmas_convert", "sgmas_write_upper_blocks",
     "sgmas_morton_codes", "sgmas_morton_partition", "sgmas_pcg_profile", "sgmas_vert_neighbors",
     "sgmas_part_maps", "sgmas_morton_codes_noalloc", "sgmas_set_pcg_mode", "sgmas_pcg_last_vectors",
-    "sgmas_mtx_write", "sgmas_mtx_read", "sgmas_mlp_set_params", "sgmas_mlp_get_params", "sgmas_mlp_features",
+    "sgmas_mtx_write", "sgmas_mtx_read", "sgmas_set_pcg_ctas", "sgmas_mlp_set_params", "sgmas_mlp_get_params", "sgmas_mlp_features",
     "sgmas_mlp_gradient", "sgmas_mlp_train_step", "sgmas_mlp_forward", "sgmas_mlp_warm_start",
 ]
 MLP_PARAMS = 19462  # SGMAS_MLP_PARAMS in include/sgmas.h
@@ -104,6 +104,7 @@ def lib(build_if_missing: bool = False):
     L.sgmas_part_maps.argtypes = [vp, i, i, vp, i, C.POINTER(i), vp]
     L.sgmas_morton_codes_noalloc.argtypes = [vp, i, vp, vp, vp]
     L.sgmas_set_pcg_mode.argtypes = [vp, i]
+    L.sgmas_set_pcg_ctas.argtypes = [vp, i]
     L.sgmas_pcg_last_vectors.argtypes = [vp, vp, vp]
     L.sgmas_mtx_write.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, i, vp]
     L.sgmas_mtx_read.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, vp, i, C.POINTER(i), C.POINTER(i)]
@@ -251,6 +252,11 @@ class Context:
     def set_pcg_mode(self, mode):
         """'persistent' (one cooperative kernel, default) or 'graph' (a kernel per phase)."""
         self._check(self.L.sgmas_set_pcg_mode(self.h, {"graph": 0, "persistent": 1}[mode]))
+
+    def set_pcg_ctas(self, max_ctas):
+        """Cap the persistent kernel's CTAs (0 = one per SM): small systems on a
+        few SMs leave the rest to concurrent solves on other streams."""
+        self._check(self.L.sgmas_set_pcg_ctas(self.h, int(max_ctas)))
 
     def synchronize(self):
         self._check(self.L.sgmas_synchronize(self.h))
