@@ -288,7 +288,7 @@ int sgmas_mlp_gradient(sgmas_context* ctx, const float* d_X, const float* d_T, c
 int sgmas_mlp_train_step(sgmas_context* ctx, const float* d_X, const float* d_T, const float* d_mask, int n_rows,
                          float inv_n, float lr, float* loss);
 /* raw network outputs d_Y [n_rows][6]: bf16 = 0 the FP32 training network,
- * bf16 = 1 the BF16 tensor-core inference */
+ * bf16 = 1 the BF16 tensor-core inference (tcgen05; d_X 16-byte aligned) */
 int sgmas_mlp_forward(sgmas_context* ctx, const float* d_X, int n_rows, int bf16, float* d_Y);
 /* The start guess of system (A, b), written to d_x0 (3 * n_block_rows
  * doubles): features + BF16 inference give the candidates v1 = u (the lumped

@@ -23,9 +23,9 @@
 // k_contact_count, k_feat_scales, k_feat_scales_final, k_features); FP32 training (k_mlp_tile: forward and
 // backward of 64 rows per CTA with all weights and activations in shared
 // memory, per-tile gradient partials; k_mlp_reduce: partials summed in tile
-// order, then Adam); BF16 inference (k_mlp_pack, k_mlp_infer: one warp per
-// subdomain, mma.sync m16n8k16 BF16 with FP32 accumulation, activations kept
-// in registers between the layers, x0 composed in the same kernel).
+// order, then Adam); BF16 inference (k_mlp_pack: weights into the tensor-core
+// operand layout; k_mlp_infer_tc: 128-row tiles through tcgen05.mma with TMEM
+// accumulators, FP32 accumulation, x0 composed in the same kernel).
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -48,10 +48,6 @@ static_assert(kParams == SGMAS_MLP_PARAMS, "parameter count");
 constexpr int kTileRows = 64;  // training rows per CTA (4 subdomains)
 constexpr int kTT = 256;       // training threads per CTA
 constexpr int kW2S = kHid + 1; // padded shared-memory row stride of W2
-// packed BF16 inference weights: transposed (output-major), rows padded
-constexpr int kS1 = 24, kS2 = 136;  // row strides (bf16 elements) of W1t and W2t / W3t
-constexpr int kP1 = kHid * kS1, kP2 = kHid * kS2, kP3 = 8 * kS2, kPackBf16 = kP1 + kP2 + kP3;
-constexpr int kPackBias = kHid + kHid + 8;
 
 constexpr double kAdamB1 = 0.9, kAdamB2 = 0.999, kAdamEps = 1e-8;
 
@@ -485,20 +481,47 @@ __global__ void k_mlp_reduce(int ntiles, const float* __restrict__ gpart, const 
     P[p] -= lr * (m / c1) / (sqrtf(v / c2) + (float)kAdamEps);
 }
 
-// ---- BF16 inference --------------------------------------------------------------
-// FP32 parameters -> W1t [128][24], W2t [128][136], W3t [8][136] (output-major,
-// BF16, zero padding) + FP32 biases b1 [128], b2 [128], b3 [8]
+// ---- BF16 inference on the 5th-generation tensor cores (tcgen05 + TMEM) ---------
+// One CTA of 256 threads runs 128-row tiles (8 subdomains): layer l is one
+// tcgen05.mma chain (M = 128, N = 128 / 128 / 16, K = 16 / 128 / 128 in K16
+// steps) from shared-memory operands into a TMEM accumulator (columns
+// [0, 128); layer 3 reuses [0, 16) once layer 2's output has been read),
+// issued by one thread and completed on an mbarrier.  Warps w and w + 4 read
+// TMEM lanes 32 (w % 4) .. + 31 (one row per thread) with tcgen05.ld, each
+// half of the columns, add the bias, apply GELU and store BF16 activations as
+// the next layer's A operand.  Operands use the canonical no-swizzle K-major
+// layout: 8 x 16-byte core matrices (8 rows x 8 BF16), the K-chunks of a row
+// group 128 B apart (LBO), row groups (K / 8) x 128 B apart (SBO).
+// k_mlp_pack writes the weights in that layout (W^T of each layer, W3 padded to
+// 16 outputs) with the FP32 biases behind them; each CTA brings them in with
+// one bulk copy.  Two CTAs fit an SM (shared memory), 2 x 128 TMEM columns.
+constexpr int kTcRows = 128, kTcThreads = 256, kTcCols = 128, kTcN3 = 16;
+constexpr int kPackW1 = kHid * kIn, kPackW2 = kHid * kHid, kPackW3 = kTcN3 * kHid;
+constexpr int kPackBf16 = kPackW1 + kPackW2 + kPackW3;  // BF16 elements
+constexpr int kPackBias = kHid + kHid + kTcN3;          // FP32
+constexpr int oTcX = 0, oTcH = oTcX + kTcRows * kIn * 2, oTcW = oTcH + kTcRows * kHid * 2, oTcB = oTcW + kPackBf16 * 2,
+              oTcY = oTcB + kPackBias * 4, oTcBar = oTcY + kTcRows * 8 * 4, oTcTm = oTcBar + 16, kTcSmem = oTcTm + 16;
+static_assert(oTcW % 16 == 0 && oTcB % 16 == 0 && (kPackBf16 * 2) % 16 == 0 && (kPackBias * 4) % 16 == 0,
+              "bulk copies: 16-byte aligned, multiples of 16 bytes");
+
+// byte offset of element (row r, k) of a K-major operand with K columns
+__host__ __device__ constexpr uint32_t core_off(int r, int k, int K) {
+    return (uint32_t)(((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// FP32 parameters -> the packed BF16 operands W1t [128 x 16], W2t [128 x 128],
+// W3t [16 x 128] (core-matrix layout) + FP32 biases b1, b2, b3 (zero padded)
 __global__ void k_mlp_pack(const float* __restrict__ P, __nv_bfloat16* W, float* bias) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < kP1) {
-        const int n = i / kS1, k = i % kS1;
-        W[i] = __float2bfloat16_rn(k < kIn ? P[oW1 + k * kHid + n] : 0.f);
-    } else if (i < kP1 + kP2) {
-        const int j = i - kP1, n = j / kS2, k = j % kS2;
-        W[i] = __float2bfloat16_rn(k < kHid ? P[oW2 + k * kHid + n] : 0.f);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // source element, output index fastest
+    if (i < kPackW1) {
+        const int n = i % kHid, k = i / kHid;
+        W[core_off(n, k, kIn) / 2] = __float2bfloat16_rn(P[oW1 + i]);
+    } else if (i < kPackW1 + kPackW2) {
+        const int j = i - kPackW1, n = j % kHid, k = j / kHid;
+        W[kPackW1 + core_off(n, k, kHid) / 2] = __float2bfloat16_rn(P[oW2 + j]);
     } else if (i < kPackBf16) {
-        const int j = i - kP1 - kP2, n = j / kS2, k = j % kS2;
-        W[i] = __float2bfloat16_rn(k < kHid && n < kOut ? P[oW3 + k * kOut + n] : 0.f);
+        const int j = i - kPackW1 - kPackW2, n = j % kTcN3, k = j / kTcN3;
+        W[kPackW1 + kPackW2 + core_off(n, k, kHid) / 2] = __float2bfloat16_rn(n < kOut ? P[oW3 + k * kOut + n] : 0.f);
     }
     if (i < kPackBias) bias[i] = i < kHid ? P[oB1 + i] : i < 2 * kHid ? P[oB2 + i - kHid]
                                                         : (i - 2 * kHid < kOut ? P[oB3 + i - 2 * kHid] : 0.f);
@@ -508,125 +531,188 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<uint32_t*>(&v);
 }
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+// shared-memory matrix descriptor: start, LBO, SBO (bytes), version 1, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+// instruction descriptor, kind::f16: BF16 A and B (K-major), FP32 accumulator, M = 128
+__host__ __device__ constexpr uint32_t umma_idesc(int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
     asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :: "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void smem_to_async_proxy() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    #pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-constexpr int kIT = 256;  // inference threads per CTA (8 warps, one subdomain each at a time)
-
-// One warp per 16-row subdomain.  compose = 1: the three start-guess
-// candidates of each valid slot's vertex (row = fem_off + v), x0 holding
-// [3][3 nrows]: the lumped step u, s * network step, s * subdomain mean of the
-// coarse term; compose = 0: raw outputs Y [rows][6].
-__global__ void __launch_bounds__(kIT) k_mlp_infer(int n_rows, const float* __restrict__ X,
-                                                   const __nv_bfloat16* __restrict__ Wg, const float* __restrict__ bg,
-                                                   int compose, const int* __restrict__ part_map, int N, int fem_off,
-                                                   const double* __restrict__ scales, const double* __restrict__ vals,
-                                                   const int* __restrict__ dindex, const double* __restrict__ S,
-                                                   const double* __restrict__ b, int nrows, double* x0, float* Y) {
-    __shared__ __align__(16) __nv_bfloat16 W[kPackBf16];
-    __shared__ float bs[kPackBias];
-    __shared__ float ys[kIT / 32][16][8];
-    for (int i = threadIdx.x; i < kPackBf16 / 8; i += kIT)
-        reinterpret_cast<uint4*>(W)[i] = reinterpret_cast<const uint4*>(Wg)[i];
-    for (int i = threadIdx.x; i < kPackBias; i += kIT) bs[i] = bg[i];
+// compose = 1: the three start-guess candidates of each valid slot's vertex
+// (row = fem_off + v), x0 holding [3][3 nrows]: the lumped step u, s * network
+// step, s * subdomain mean of the coarse term; compose = 0: raw outputs Y [rows][6].
+__global__ void __launch_bounds__(kTcThreads) k_mlp_infer_tc(int n_rows, const float* __restrict__ X,
+                                                             const __nv_bfloat16* __restrict__ Wg,
+                                                             const float* __restrict__ bg, int compose,
+                                                             const int* __restrict__ part_map, int N, int fem_off,
+                                                             const double* __restrict__ scales,
+                                                             const double* __restrict__ vals,
+                                                             const int* __restrict__ dindex,
+                                                             const double* __restrict__ S,
+                                                             const double* __restrict__ b, int nrows, double* x0,
+                                                             float* Y, int* err) {
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    unsigned char* sX = tsm + oTcX;
+    unsigned char* sH = tsm + oTcH;
+    const float* bias = reinterpret_cast<const float*>(tsm + oTcB);
+    float* ys = reinterpret_cast<float*>(tsm + oTcY);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tsm + oTcBar);  // [0] MMA completion, [1] weights
+    uint32_t* tm = reinterpret_cast<uint32_t*>(tsm + oTcTm);
+    __shared__ int failed;
+    const int tid = threadIdx.x, warp = tid / 32, half = warp >> 2;
+    if (tid == 0) {
+        failed = 0;
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+        fence_mbar_init();
+        mbar_expect_tx(bar + 1, kPackBf16 * 2 + kPackBias * 4);
+        bulk_g2s(tsm + oTcW, Wg, kPackBf16 * 2, bar + 1);
+        bulk_g2s(tsm + oTcB, bg, kPackBias * 4, bar + 1);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smem_u32(tm)),
+                     "r"(kTcCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
     __syncthreads();
-    const __nv_bfloat16 *W1 = W, *W2 = W + kP1, *W3 = W + kP1 + kP2;
-    const float *bb1 = bs, *bb2 = bs + kHid, *bb3 = bs + 2 * kHid;
-    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, g = lane / 4, t = lane % 4;
-    const int nsub = n_rows / 16;
-    for (int sd = blockIdx.x * (kIT / 32) + warp; sd < nsub; sd += gridDim.x * (kIT / 32)) {
-        const float* x = X + (size_t)sd * 16 * kIn;
-        uint32_t a[4];
-        a[0] = pack_bf16(x[g * kIn + 2 * t], x[g * kIn + 2 * t + 1]);
-        a[1] = pack_bf16(x[(g + 8) * kIn + 2 * t], x[(g + 8) * kIn + 2 * t + 1]);
-        a[2] = pack_bf16(x[g * kIn + 2 * t + 8], x[g * kIn + 2 * t + 9]);
-        a[3] = pack_bf16(x[(g + 8) * kIn + 2 * t + 8], x[(g + 8) * kIn + 2 * t + 9]);
-        uint32_t h[8][4];  // layer output as the next layer's A fragments (8 k-steps of 16)
-        {
-            float acc[16][4];
-            #pragma unroll
-            for (int nt = 0; nt < 16; ++nt) {
-                const float c0 = bb1[nt * 8 + 2 * t], c1 = bb1[nt * 8 + 2 * t + 1];
-                acc[nt][0] = c0; acc[nt][1] = c1; acc[nt][2] = c0; acc[nt][3] = c1;
-                const __nv_bfloat16* wr = W1 + (nt * 8 + g) * kS1 + 2 * t;
-                mma_bf16(acc[nt], a, *reinterpret_cast<const uint32_t*>(wr), *reinterpret_cast<const uint32_t*>(wr + 8));
+    tc_fence_after();
+    const uint32_t taddr = *tm;
+    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
+    const uint32_t aX = smem_u32(sX), aH = smem_u32(sH), aW = smem_u32(tsm + oTcW);
+    const uint32_t a1 = aW, a2 = aW + kPackW1 * 2, a3 = aW + (kPackW1 + kPackW2) * 2;
+    if (!mbar_wait(bar + 1, 0u, err)) failed = 1;
+    unsigned phase = 0u;
+    const int ntiles = (n_rows + kTcRows - 1) / kTcRows;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int row0 = tile * kTcRows, r = tid & (kTcRows - 1);
+        {  // features -> A of layer 1 (BF16): thread (r, half) converts 8 of row r's 16
+            const int grow = row0 + r;
+            float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f), f1 = f0;
+            if (grow < n_rows) {
+                const float4* xr = reinterpret_cast<const float4*>(X + (size_t)grow * kIn) + 2 * half;
+                f0 = xr[0];
+                f1 = xr[1];
             }
-            #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                h[j][0] = pack_bf16(gelu(acc[2 * j][0]), gelu(acc[2 * j][1]));
-                h[j][1] = pack_bf16(gelu(acc[2 * j][2]), gelu(acc[2 * j][3]));
-                h[j][2] = pack_bf16(gelu(acc[2 * j + 1][0]), gelu(acc[2 * j + 1][1]));
-                h[j][3] = pack_bf16(gelu(acc[2 * j + 1][2]), gelu(acc[2 * j + 1][3]));
-            }
+            uint4 q;
+            q.x = pack_bf16(f0.x, f0.y); q.y = pack_bf16(f0.z, f0.w);
+            q.z = pack_bf16(f1.x, f1.y); q.w = pack_bf16(f1.z, f1.w);
+            *reinterpret_cast<uint4*>(sX + core_off(r, 8 * half, kIn)) = q;
         }
-        {
-            float acc[16][4];
-            #pragma unroll
-            for (int nt = 0; nt < 16; ++nt) {
-                const float c0 = bb2[nt * 8 + 2 * t], c1 = bb2[nt * 8 + 2 * t + 1];
-                acc[nt][0] = c0; acc[nt][1] = c1; acc[nt][2] = c0; acc[nt][3] = c1;
-            }
-            #pragma unroll
-            for (int j = 0; j < 8; ++j)
-                #pragma unroll
-                for (int nt = 0; nt < 16; ++nt) {
-                    const __nv_bfloat16* wr = W2 + (nt * 8 + g) * kS2 + 16 * j + 2 * t;
-                    mma_bf16(acc[nt], h[j], *reinterpret_cast<const uint32_t*>(wr),
-                             *reinterpret_cast<const uint32_t*>(wr + 8));
+        for (int layer = 0; layer < 3; ++layer) {
+            smem_to_async_proxy();
+            tc_fence_before();
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after();
+                if (layer == 0) {
+                    umma_bf16(taddr, umma_desc(aX, 128, 2 * 128), umma_desc(a1, 128, 2 * 128), umma_idesc(kHid), 0u);
+                } else {
+                    const uint32_t b_base = layer == 1 ? a2 : a3;
+                    const uint32_t id = umma_idesc(layer == 1 ? kHid : kTcN3);
+                    #pragma unroll 1
+                    for (int k = 0; k < kHid / 16; ++k)
+                        umma_bf16(taddr, umma_desc(aH + 256 * k, 128, 16 * 128),
+                                  umma_desc(b_base + 256 * k, 128, 16 * 128), id, k > 0 ? 1u : 0u);
                 }
-            #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                h[j][0] = pack_bf16(gelu(acc[2 * j][0]), gelu(acc[2 * j][1]));
-                h[j][1] = pack_bf16(gelu(acc[2 * j][2]), gelu(acc[2 * j][3]));
-                h[j][2] = pack_bf16(gelu(acc[2 * j + 1][0]), gelu(acc[2 * j + 1][1]));
-                h[j][3] = pack_bf16(gelu(acc[2 * j + 1][2]), gelu(acc[2 * j + 1][3]));
+                umma_commit(bar);
+            }
+            if (!mbar_wait(bar, phase, err)) failed = 1;
+            phase ^= 1u;
+            tc_fence_after();
+            if (layer < 2) {  // accumulator -> bias + GELU -> BF16 activations (A of the next layer)
+                const float* bb = bias + layer * kHid;
+                #pragma unroll 1
+                for (int j = 0; j < kHid / 32; ++j) {
+                    const int c0 = 64 * half + 16 * j;
+                    float v[16];
+                    tmem_ld16(taddr + lane_base + c0, v);
+                    #pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        uint4 q;
+                        const int k0 = c0 + 8 * c;
+                        q.x = pack_bf16(gelu(v[8 * c] + bb[k0]), gelu(v[8 * c + 1] + bb[k0 + 1]));
+                        q.y = pack_bf16(gelu(v[8 * c + 2] + bb[k0 + 2]), gelu(v[8 * c + 3] + bb[k0 + 3]));
+                        q.z = pack_bf16(gelu(v[8 * c + 4] + bb[k0 + 4]), gelu(v[8 * c + 5] + bb[k0 + 5]));
+                        q.w = pack_bf16(gelu(v[8 * c + 6] + bb[k0 + 6]), gelu(v[8 * c + 7] + bb[k0 + 7]));
+                        *reinterpret_cast<uint4*>(sH + core_off(r, k0, kHid)) = q;
+                    }
+                }
+            } else if (half == 0) {
+                float v[16];
+                tmem_ld16(taddr + lane_base, v);
+                #pragma unroll
+                for (int d = 0; d < 8; ++d) ys[r * 8 + d] = v[d] + bias[2 * kHid + d];
             }
         }
-        float o[4] = {bb3[2 * t], bb3[2 * t + 1], bb3[2 * t], bb3[2 * t + 1]};
-        #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const __nv_bfloat16* wr = W3 + g * kS2 + 16 * j + 2 * t;
-            mma_bf16(o, h[j], *reinterpret_cast<const uint32_t*>(wr), *reinterpret_cast<const uint32_t*>(wr + 8));
-        }
-        ys[warp][g][2 * t] = o[0];
-        ys[warp][g][2 * t + 1] = o[1];
-        ys[warp][g + 8][2 * t] = o[2];
-        ys[warp][g + 8][2 * t + 1] = o[3];
-        __syncwarp();
-        if (!compose) {
-            if (lane < 16)
-                for (int d = 0; d < kOut; ++d) Y[((size_t)sd * 16 + lane) * kOut + d] = ys[warp][lane][d];
-        } else if (lane < 16) {
-            const int v = part_map[sd * 16 + lane];
-            float cnt = 0.f, cm[3] = {0.f, 0.f, 0.f};
-            for (int u = 0; u < 16; ++u) {
-                const int vu = part_map[sd * 16 + u];
-                if (vu < 0 || vu >= N) continue;
-                cnt += 1.f;
-                #pragma unroll
-                for (int d = 0; d < 3; ++d) cm[d] += ys[warp][u][3 + d];
-            }
-            if (v >= 0 && v < N) {
-                const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-                const int row = fem_off + v;
-                double u[3];
-                lumped_step(S + 9 * (size_t)row, diag_of(vals, dindex, row, eye), b + 3 * (size_t)row, u);
-                const double sc = scales[0];
-                const size_t n3 = 3 * (size_t)nrows;
-                #pragma unroll
-                for (int d = 0; d < 3; ++d) {  // candidates: lumped step, network step, subdomain coarse term
-                    x0[3 * (size_t)row + d] = u[d];
-                    x0[n3 + 3 * (size_t)row + d] = sc * (double)ys[warp][lane][d];
-                    x0[2 * n3 + 3 * (size_t)row + d] = sc * (double)(cm[d] / cnt);
+        tc_fence_before();
+        __syncthreads();
+        if (failed) break;
+        const int grow = row0 + r;
+        if (half == 0 && grow < n_rows) {
+            if (!compose) {
+                for (int d = 0; d < kOut; ++d) Y[(size_t)grow * kOut + d] = ys[r * 8 + d];
+            } else {
+                const int v = part_map[grow], sb = r & ~15;
+                float cnt = 0.f, cm[3] = {0.f, 0.f, 0.f};
+                for (int u = 0; u < 16; ++u) {
+                    const int vu = part_map[row0 + sb + u];
+                    if (vu < 0 || vu >= N) continue;
+                    cnt += 1.f;
+                    #pragma unroll
+                    for (int d = 0; d < 3; ++d) cm[d] += ys[(sb + u) * 8 + 3 + d];
+                }
+                if (v >= 0 && v < N) {
+                    const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+                    const int row = fem_off + v;
+                    double u3[3];
+                    lumped_step(S + 9 * (size_t)row, diag_of(vals, dindex, row, eye), b + 3 * (size_t)row, u3);
+                    const double sc = scales[0];
+                    const size_t n3 = 3 * (size_t)nrows;
+                    #pragma unroll
+                    for (int d = 0; d < 3; ++d) {  // candidates: lumped step, network step, subdomain coarse term
+                        x0[3 * (size_t)row + d] = u3[d];
+                        x0[n3 + 3 * (size_t)row + d] = sc * (double)ys[r * 8 + d];
+                        x0[2 * n3 + 3 * (size_t)row + d] = sc * (double)(cm[d] / cnt);
+                    }
                 }
             }
         }
-        __syncwarp();
+        __syncthreads();  // ys and sX are rewritten by the next tile
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(kTcCols) : "memory");
     }
 }
 
@@ -737,6 +823,7 @@ struct MlpState {
     float* bias = nullptr;
     int step = 0;                                    // Adam steps taken
     bool ready = false;                              // parameters set
+    int infer_sms = 0;                               // SM count for the inference grid (0: not yet queried)
     float *gpart = nullptr, *lpart = nullptr, *loss = nullptr;
     int gcap = 0, lcap = 0;
     // features scratch
@@ -778,6 +865,24 @@ static int mlp_ready(sgmas_context* c, MlpState** out) {
     int rc = mlp_state(c, out);
     if (rc) return rc;
     if (!(*out)->ready) return ctx_fail(c, SGMAS_ERR_STATE, "learned start guess used before sgmas_mlp_set_params");
+    return 0;
+}
+
+// BF16 inference of n_rows feature rows on the tensor cores (k_mlp_infer_tc):
+// raw outputs into Y, or (compose) the three start-guess candidates into x0
+static int mlp_infer(sgmas_context* c, MlpState* m, int n_rows, const float* X, int compose, int fem_off,
+                     const double* vals, const double* b, const double* S, int nrows, double* x0, float* Y) {
+    if (n_rows <= 0) return 0;
+    if (!m->infer_sms) {  // once per context: SM count and the shared-memory opt-in (the same value every time)
+        SG_CUDA(c, cudaDeviceGetAttribute(&m->infer_sms, cudaDevAttrMultiProcessorCount, c->device));
+        SG_CUDA(c, cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    }
+    // two CTAs per SM at most (shared memory), so 2 x 128 TMEM columns always fit
+    const int grid = std::min((n_rows + kTcRows - 1) / kTcRows, 2 * m->infer_sms);
+    k_mlp_infer_tc<<<grid, kTcThreads, kTcSmem, c->stream>>>(n_rows, X, m->W, m->bias, compose, c->d_part_map, c->N,
+                                                             fem_off, m->scales, vals, m->dindex, S, b, nrows, x0, Y,
+                                                             c->d_err);
+    SG_CUDA(c, cudaGetLastError());
     return 0;
 }
 
@@ -933,9 +1038,9 @@ int sgmas_mlp_forward(sgmas_context* c, const float* d_X, int n_rows, int bf16, 
     MlpState* m = nullptr;
     if ((rc = mlp_ready(c, &m))) return rc;
     if (bf16) {
-        const int grid = std::min((n_rows / 16 + kIT / 32 - 1) / (kIT / 32), 4 * 148);
-        k_mlp_infer<<<grid, kIT, 0, c->stream>>>(n_rows, d_X, m->W, m->bias, 0, nullptr, 0, 0, nullptr, nullptr, nullptr,
-                                                 nullptr, nullptr, 0, nullptr, d_Y);
+        if (reinterpret_cast<uintptr_t>(d_X) % 16)
+            return ctx_fail(c, SGMAS_ERR_ARG, "sgmas_mlp_forward: d_X must be 16-byte aligned for BF16 inference");
+        if ((rc = mlp_infer(c, m, n_rows, d_X, 0, 0, nullptr, nullptr, nullptr, 0, nullptr, d_Y))) return rc;
     } else {
         SG_CUDA(c, cudaFuncSetAttribute(k_mlp_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem));
         k_mlp_tile<<<(n_rows + kTileRows - 1) / kTileRows, kTT, kTrainSmem, c->stream>>>(
@@ -967,10 +1072,7 @@ int sgmas_mlp_warm_start(sgmas_context* c, const sgmas_bcoo* A, const double* d_
     if (rc) return rc;
     cudaStream_t s = c->stream;
     SG_CUDA(c, cudaMemsetAsync(m->cand, 0, sizeof(double) * 3 * (size_t)n3, s));
-    const int grid = std::min((c->Mm / 16 + kIT / 32 - 1) / (kIT / 32), 4 * 148);
-    k_mlp_infer<<<grid, kIT, 0, s>>>(c->Mm, m->X, m->W, m->bias, 1, c->d_part_map, c->N, fem_offset, m->scales,
-                                     A->d_values, m->dindex, m->S, d_b, nrows, m->cand, nullptr);
-    SG_CUDA(c, cudaGetLastError());
+    if ((rc = mlp_infer(c, m, c->Mm, m->X, 1, fem_offset, A->d_values, d_b, m->S, nrows, m->cand, nullptr))) return rc;
     // A v_k on the block CSR built for the features (row-owned, deterministic)
     if (d_prev && (rc = bsr_spmv_plain(c, 1.0, d_prev, 0.0, m->Acand))) return rc;
     for (int k = 1; k < kCand; ++k)
