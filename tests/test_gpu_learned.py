@@ -120,6 +120,31 @@ def test_bf16_inference_matches_oracle(sgm):
     ctx.close()
 
 
+def test_bf16_inference_many_tiles(sgm):
+    """160,016 rows: 1,251 tiles of 128 rows on at most two CTAs per SM (each CTA
+    runs several tiles through the same TMEM accumulator and mbarrier phases),
+    the last tile holding 16 rows."""
+    case = cases.build("c1")
+    ctx = ctx_for(sgm, case)
+    P = params(5)
+    ctx.mlp_set_params(P)
+    rng = np.random.default_rng(6)
+    n = 16 * 10001
+    X = rng.normal(size=(n, 16)).astype(np.float32)
+    Y = torch.full((n * 6,), float("nan"), dtype=torch.float32, device="cuda")
+    ctx.mlp_forward(dev(X), n, Y, bf16=True)
+    Yg = Y.cpu().numpy().reshape(n, 6)
+    Yo = OM.infer_bf16(P, X)
+    scale = np.abs(Yo).max()
+    assert np.isfinite(Yg).all()
+    assert np.max(np.abs(Yg - Yo)) <= 2e-2 * scale, np.max(np.abs(Yg - Yo)) / scale
+    assert np.median(np.abs(Yg - Yo)) <= 2e-3 * scale
+    # every tile as accurate as the first (no stale accumulator or phase slip)
+    err = np.abs(Yg - Yo).max(axis=1).reshape(-1, 16).max(axis=1)
+    assert err[-1] <= 2e-2 * scale and np.percentile(err, 99) <= 1e-2 * scale
+    ctx.close()
+
+
 def test_warm_start_is_galerkin_optimal(sgm):
     """x0 is the A-norm-best combination of its candidates: with zero network
     parameters it equals the oracle's Galerkin combination of the previous
