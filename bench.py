@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--c5-streams", type=int, default=8,
                     help="config 5: concurrent solves (one host thread, context and stream each); 1 = one after another")
     ap.add_argument("--c5-precision", default="bf16", choices=["bf16", "fp32", "fp64"])
+    ap.add_argument("--c5-tune", default="throughput", choices=["throughput", "latency", "none"],
+                    help="config 5: launch shape per scene from the autotuner (sgmas_autotune_pcg, untimed, "
+                         "before the passes); none = about 20 level-0 subdomains per CTA")
     ap.add_argument("--variants", default="bf16,fp32,fp32f,fp64,jacobi,fp32-graph",
                     help="MAS storage precision (or jacobi); suffix -graph = kernel-per-phase CUDA graph "
                          "instead of the persistent cooperative kernel")
@@ -704,9 +707,11 @@ def run_c5(args):
     pairs 0-20 % of N).  Scenes are sharded across ranks by cost (blocks).
     On each rank, --c5-streams host threads take scenes from a queue (largest
     first), each with its own context and stream, and solve them
-    (BF16-factored MAS-PCG, persistent form on a grid sized to the scene --
-    about 20 level-0 subdomains per CTA -- so that small scenes share the GPU;
-    graph form where a scene does not fit).  Inputs are uploaded before the
+    (BF16-factored MAS-PCG).  Each scene's launch shape (persistent form on a
+    grid sized to the scene, so that small scenes share the GPU, or the graph
+    form) comes from the autotuner (--c5-tune, default: least SM-time per
+    iteration), run on each scene alone before the passes; --c5-tune none
+    uses about 20 level-0 subdomains per CTA.  Inputs are uploaded before the
     timed pass; one untimed pass first.  Prints one JSON line: p50 / p99
     per-scene solve latency (CUDA events on the scene's stream) and the
     throughput of the timed pass (CUDA events around it, max over ranks)."""
@@ -765,7 +770,10 @@ def run_c5(args):
                         ctx.mas_set_contacts(dd["pairs"], len(s.pairs))
                         ctx.set_pcg_ctas(0 if k in big else min(n_sm, max(1, -(-len(pm) // (16 * 20)))))
                         ctxs[k] = ctx
+                        if args.c5_tune != "none":  # tuned alone, before the passes (see below)
+                            raise RuntimeError("config-5 scene %d was not tuned" % k)
                     ctx = ctxs[k]
+                    ctx.set_stream(st.cuda_stream)  # this worker's stream (the tuner ran on another)
                     e0 = torch.cuda.Event(enable_timing=True)
                     e1 = torch.cuda.Event(enable_timing=True)
                     e0.record(st)
@@ -798,6 +806,28 @@ def run_c5(args):
             for t in th:
                 t.join()
 
+    tuned, tune_s = {}, 0.0
+    if args.c5_tune != "none":
+        # each scene alone on the GPU: trial solves of candidate launch shapes,
+        # the choice kept on the scene's context (untimed; a serving system does
+        # this once per scene and reuses it every Newton step)
+        t0 = time.time()
+        st = streams[0]
+        with torch.cuda.stream(st):
+            for k in order:
+                s, dd = scenes[k], data[k]
+                ctx = sgmas.Context(local, bank=16, precision=args.c5_precision)
+                ctx.set_stream(st.cuda_stream)
+                pm, rm = ctx.morton_partition(dd["pos"])
+                ctx.mas_init(s.n_verts, *sgmas.vert_neighbors(s.tets, s.n_verts), pm, rm)
+                ctx.mas_set_contacts(dd["pairs"], len(s.pairs))
+                t = ctx.autotune(dd["vals"], dd["rows"], dd["cols"], s.n_verts, dd["b"], objective=args.c5_tune,
+                                 concurrency=nstreams, trial_iters=20, reps=2, **kw)
+                ch = t["candidates"][t["chosen"]]
+                tuned[k] = ch["ctas"] if ch["persistent"] else "graph"
+                ctxs[k] = ctx
+        torch.cuda.synchronize()
+        tune_s = time.time() - t0
     one_pass(False)                       # contexts + hierarchy set-up, first solves (untimed)
     torch.cuda.synchronize()
     reps_timed = max(1, min(args.steps, 3))
@@ -839,9 +869,13 @@ def run_c5(args):
                                            "iterations_p50": int(sorted(iters)[len(iters) // 2]) if iters else 0,
                                            "gen_s": round(gen_s, 1),
                                            "concurrent_solves": max(1, args.c5_streams),
+                                           "launch_shape": ("autotuned (%s): %s" % (args.c5_tune, json.dumps(
+                                               {str(k): tuned[k] for k in sorted(tuned)})) if tuned else
+                                               "about 20 level-0 subdomains per CTA"),
+                                           "tune_s": round(tune_s, 2),
                                            "scenes_alone": len(big), "scenes_shared": len(small),
                                            "note": "scenes solved concurrently from per-stream host threads, "
-                                                   "each persistent solve on a grid sized to its scene"
+                                                   "each solve with its scene's launch shape"
                                                    + ("; scenes filling every SM one at a time" if args.c5_big_alone else "")
                                                    if args.c5_streams > 1 else "scenes solved one after another per rank"}}
     print(json.dumps(out))

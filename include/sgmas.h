@@ -179,6 +179,32 @@ int sgmas_set_pcg_mode(sgmas_context* ctx, int mode);
  * cooperative launches of such solves run side by side.  A system needing
  * more than 32 level-0 subdomains per CTA falls back to the graph form. */
 int sgmas_set_pcg_ctas(sgmas_context* ctx, int max_ctas);
+/* Autotuner of the loop's launch shape: the persistent form on candidate grid
+ * sizes (from the fewest CTAs the system fits on up to every SM, about x1.4
+ * apart; tried from the largest down, until one does not fit) and the
+ * graph form, each timed by `reps` trial solves of
+ * trial_iters iterations (cfg as given, x0 = 0, into a scratch vector;
+ * builds included, the loop's time per iteration compared).  Objective
+ * SGMAS_TUNE_LATENCY picks the least time per iteration, SGMAS_TUNE_THROUGHPUT
+ * the least SM-time per iteration for `concurrency` solves sharing the GPU
+ * (time x max(CTAs, SMs / concurrency); the graph form counts every SM): a
+ * grid below its share of the SMs gains nothing, the SMs it leaves idle.  The
+ * choice stays set on the context (sgmas_set_pcg_mode / sgmas_set_pcg_ctas).
+ * The project's own: the reference has no autotuner. */
+#define SGMAS_TUNE_LATENCY 0
+#define SGMAS_TUNE_THROUGHPUT 1
+#define SGMAS_TUNE_MAX_CANDIDATES 16
+typedef struct {
+    int n_candidates;
+    int ctas[SGMAS_TUNE_MAX_CANDIDATES];        /* grid tried (the graph form: 0) */
+    int persistent[SGMAS_TUNE_MAX_CANDIDATES];  /* 1: the trial ran the persistent form */
+    double us_per_iter[SGMAS_TUNE_MAX_CANDIDATES];  /* least over the reps */
+    double cost[SGMAS_TUNE_MAX_CANDIDATES];     /* the objective's figure (us, or SM-us) */
+    int chosen;                                 /* index of the choice */
+    int sms;                                    /* SMs of the device */
+} sgmas_tune_report;
+int sgmas_autotune_pcg(sgmas_context* ctx, const sgmas_bcoo* A, const double* d_b, const sgmas_pcg_config* cfg,
+                       int objective, int concurrency, int trial_iters, int reps, sgmas_tune_report* report);
 /* the same with host arrays: uploads A and b, solves, downloads x */
 int sgmas_pcg_solve_host(sgmas_context* ctx, const double* values, const int* rows,
                          const int* cols, int n_blocks, int n_block_rows, const double* b,

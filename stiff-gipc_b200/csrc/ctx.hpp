@@ -129,6 +129,8 @@ struct sgmas_context {
     int* d_own1 = nullptr;                // first level-1 bank of each CTA of the persistent kernel
     int own1_cap = 0;
     int partial_cap = 0;
+    double* d_tune_x = nullptr;           // scratch solution of the autotuner's trial solves
+    int tune_cap = 0;
     PcgState* d_state = nullptr;
     // uploaded host systems (sgmas_pcg_solve_host)
     double *d_hvals = nullptr, *d_hb = nullptr, *d_hx = nullptr;

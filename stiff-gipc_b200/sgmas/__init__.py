@@ -46,6 +46,15 @@ class PcgReport(C.Structure):
                 ("x0_scale", C.c_double), ("rr_x0", C.c_double), ("bb", C.c_double)]
 
 
+TUNE_MAX = 16  # SGMAS_TUNE_MAX_CANDIDATES in include/sgmas.h
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("n_candidates", C.c_int), ("ctas", C.c_int * TUNE_MAX), ("persistent", C.c_int * TUNE_MAX),
+                ("us_per_iter", C.c_double * TUNE_MAX), ("cost", C.c_double * TUNE_MAX), ("chosen", C.c_int),
+                ("sms", C.c_int)]
+
+
 class Bcoo(C.Structure):
     _fields_ = [("d_values", C.c_void_p), ("d_rows", C.c_void_p), ("d_cols", C.c_void_p),
                 ("n_blocks", C.c_int), ("n_block_rows", C.c_int)]
@@ -60,6 +69,7 @@ EXPORTS = [
     "sgmas_part_maps", "sgmas_morton_codes_noalloc", "sgmas_set_pcg_mode", "sgmas_pcg_last_vectors",
     "sgmas_mtx_write", "sgmas_mtx_read", "sgmas_set_pcg_ctas", "sgmas_mlp_set_params", "sgmas_mlp_get_params", "sgmas_mlp_features",
     "sgmas_mlp_gradient", "sgmas_mlp_train_step", "sgmas_mlp_forward", "sgmas_mlp_warm_start",
+    "sgmas_autotune_pcg",
 ]
 MLP_PARAMS = 19462  # SGMAS_MLP_PARAMS in include/sgmas.h
 
@@ -105,6 +115,7 @@ def lib(build_if_missing: bool = False):
     L.sgmas_morton_codes_noalloc.argtypes = [vp, i, vp, vp, vp]
     L.sgmas_set_pcg_mode.argtypes = [vp, i]
     L.sgmas_set_pcg_ctas.argtypes = [vp, i]
+    L.sgmas_autotune_pcg.argtypes = [vp, C.POINTER(Bcoo), vp, C.POINTER(PcgConfig), i, i, i, i, C.POINTER(TuneReport)]
     L.sgmas_pcg_last_vectors.argtypes = [vp, vp, vp]
     L.sgmas_mtx_write.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, i, vp]
     L.sgmas_mtx_read.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, vp, i, C.POINTER(i), C.POINTER(i)]
@@ -257,6 +268,24 @@ class Context:
         """Cap the persistent kernel's CTAs (0 = one per SM): small systems on a
         few SMs leave the rest to concurrent solves on other streams."""
         self._check(self.L.sgmas_set_pcg_ctas(self.h, int(max_ctas)))
+
+    def autotune(self, vals, rows, cols, n_block_rows, b, objective="throughput", concurrency=1, trial_iters=30,
+                 reps=2, **cfg):
+        """Time trial solves of the persistent form on candidate grids and of the
+        graph form; keep the best for `objective` ('latency': least time per
+        iteration; 'throughput': least SM-time per iteration with `concurrency`
+        solves sharing the GPU, each charged at least SMs / concurrency) on this context.
+        Returns the candidates: a list of dicts (ctas, persistent, us_per_iter,
+        cost) and the index of the choice."""
+        A = self.bcoo(vals, rows, cols, n_block_rows)
+        c = pcg_config(**cfg)
+        rep = TuneReport()
+        obj = {"latency": 0, "throughput": 1}[objective]
+        self._check(self.L.sgmas_autotune_pcg(self.h, C.byref(A), _ptr(b), C.byref(c), obj, int(concurrency),
+                                              int(trial_iters), int(reps), C.byref(rep)))
+        cands = [dict(ctas=rep.ctas[i], persistent=bool(rep.persistent[i]), us_per_iter=rep.us_per_iter[i],
+                      cost=rep.cost[i]) for i in range(rep.n_candidates)]
+        return {"candidates": cands, "chosen": rep.chosen, "sms": rep.sms}
 
     def synchronize(self):
         self._check(self.L.sgmas_synchronize(self.h))
