@@ -733,12 +733,17 @@ __device__ __forceinline__ bool schwarz_banks(const S* __restrict__ inv, Acc* R,
 // Coarse levels (_schwarzLocalXSym6 for levels >= 1).  Each CTA applies a
 // run of level-1 banks and sums their residuals into the level-2 nodes; the
 // CTA that finishes last (a ticket, nothing waits) then builds levels >= 3
-// the same way, bank by bank, and applies the banks of levels >= 2.
+// the same way, bank by bank, and applies the banks of levels >= 2 -- unless
+// k_apply_coarse_hi follows (hi_kernel = 1) and they are more than two rounds
+// of one CTA (large systems: a hundred or more banks), which it then spreads
+// over CTAs.  Both read the level sizes on the device, so a recorded graph
+// stays right when the hierarchy of a later solve changes size.
 template <int B, typename S, typename Acc>
 __global__ void __launch_bounds__(kCoarseThreads) k_apply_coarse(int L, const int* __restrict__ level_size,
                                                                  const int* __restrict__ going_next,
                                                                  const S* __restrict__ inv, Acc* R, Acc* Z,
-                                                                 const PcgState* st, unsigned* ticket, int* err) {
+                                                                 const PcgState* st, unsigned* ticket, int hi_kernel,
+                                                                 int* err) {
     if (st && st->done) return;
     if (L < 2) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -798,9 +803,37 @@ __global__ void __launch_bounds__(kCoarseThreads) k_apply_coarse(int L, const in
         }
         __syncthreads();
     }
-    schwarz_banks<B, S, Acc, false>(inv, R, Z, going_next, 0, b2, total / B - b2, chunk, tile, &bar, phase, err,
-                                    xch);
+    if (!(hi_kernel && total / B - b2 > 2 * BPC))
+        schwarz_banks<B, S, Acc, false>(inv, R, Z, going_next, 0, b2, total / B - b2, chunk, tile, &bar, phase, err,
+                                        xch);
     if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// The Schwarz products of the banks of levels >= 2 (residuals complete: the
+// previous kernel built them) when there are more than two rounds of one CTA
+// of them: coarse_bpc banks per CTA, grid-stride.
+template <int B, typename S, typename Acc>
+__global__ void __launch_bounds__(kCoarseThreads) k_apply_coarse_hi(int L, const int* __restrict__ level_size,
+                                                                    const int* __restrict__ going_next,
+                                                                    const S* __restrict__ inv, Acc* R, Acc* Z,
+                                                                    const PcgState* st, int* err) {
+    if (st && st->done) return;
+    if (L < 3) return;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ uint64_t bar;
+    __shared__ __align__(16) Acc xch[(kCoarseThreads / 32) * kXchPerWarp];
+    constexpr int bs = bsym_of(B);
+    constexpr int BPC = coarse_bpc<B>();
+    S* tile = reinterpret_cast<S*>(smem_raw);
+    const int chunk = max(1, min(BPC, (int)(kCoarseSmem / (bs * 9 * sizeof(S)))));
+    const int b2 = level_size[5] / B, bend = level_size[2 * L + 1] / B;
+    if (bend - b2 <= 2 * BPC || b2 + (int)blockIdx.x * BPC >= bend) return;  // k_apply_coarse took them
+    unsigned phase = 0u;
+    if (threadIdx.x == 0) { mbar_init(&bar, 1); fence_mbar_init(); }
+    for (int bank0 = b2 + blockIdx.x * BPC; bank0 < bend; bank0 += gridDim.x * BPC)
+        if (!schwarz_banks<B, S, Acc, false>(inv, R, Z, going_next, 0, bank0, min(BPC, bend - bank0), chunk, tile,
+                                             &bar, phase, err, xch))
+            return;
 }
 
 }  // namespace
@@ -969,10 +1002,21 @@ int apply_t(sgmas_context* c, const double* r, double* z, int mode, const PcgSta
             st, c->d_err);
     // level-1 banks are bounded by the vertex count (extra CTAs return at once)
     const int l1_cap = (c->N + B - 1) / B + 1;
-    if (parts & 2)
+    // banks of levels >= 2: more than two rounds of one CTA go to their own
+    // kernel (the kernels decide again from the device's level sizes)
+    const int nb_hi = c->L > 2 ? (c->h_level_size[2 * c->L + 1] - c->h_level_size[5]) / B : 0;
+    const int hi_apart = nb_hi > 2 * coarse_bpc<B>();
+    if (parts & 2) {
         k1<<<(l1_cap + coarse_bpc<B>() - 1) / coarse_bpc<B>(), kCoarseThreads, smem1, s>>>(
             c->L, c->d_level_size, c->d_going_next, (const S*)c->d_inv, (Acc*)c->d_R, (Acc*)c->d_Z, st,
-            c->d_coarse_ticket, c->d_err);
+            c->d_coarse_ticket, hi_apart, c->d_err);
+        if (hi_apart) {
+            auto k2 = k_apply_coarse_hi<B, S, Acc>;
+            SG_CUDA(c, cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
+            k2<<<(nb_hi + coarse_bpc<B>() - 1) / coarse_bpc<B>(), kCoarseThreads, smem1, s>>>(
+                c->L, c->d_level_size, c->d_going_next, (const S*)c->d_inv, (Acc*)c->d_R, (Acc*)c->d_Z, st, c->d_err);
+        }
+    }
     // threads past the MAS vertices (padded to a warp): 16 per body, then one per other row
     const int n_extra = kind >= 1 && ex.n_units > 0 ? 16 * ex.abd_bodies + (ex.n_units - ex.abd_bodies) : 0;
     const int gN = (((c->N + 31) & ~31) + n_extra + kCollectThreads - 1) / kCollectThreads;
@@ -981,7 +1025,7 @@ int apply_t(sgmas_context* c, const double* r, double* z, int mode, const PcgSta
             c->N, c->L, c->Mm, c->d_level_size, c->d_real_map, c->d_coarse_table, (const Acc*)c->d_Z, (Acc*)c->d_R,
             (double*)r, z, ex, mode, x, p, Ap, kind, (PcgState*)st, partials, ticket, cond != 0ull, cond);
     SG_CUDA(c, cudaGetLastError());
-    if (launches) *launches += 3;
+    if (launches) *launches += 3 + hi_apart;
     return 0;
 }
 

@@ -162,11 +162,13 @@ PREC = {"fp32": 0, "bf16": 1, "fp64": 2, "fp32f": 3}
 
 
 @pytest.mark.parametrize("precision", ["fp32", "bf16", "fp64", "fp32f"])
-@pytest.mark.parametrize("name", ["c1", "c2s", "bar", "bunny2"])
+@pytest.mark.parametrize("name", ["c1", "c2s", "bar", "bunny2", "g80k"])
 def test_apply(sgm, name, precision):
     """MAS apply on identical subdomain matrices (the oracle takes the
     device's assembled FP64 matrices): every sum of the apply has a defined
-    order on both sides, so the result is bit-identical."""
+    order on both sides, so the result is bit-identical.  g80k (82,944
+    vertices) has more than 32 subdomains at levels >= 2, which the coarse
+    apply spreads over CTAs in a kernel of their own."""
     case = cases.build(name)
     ctx = make_ctx(sgm, case, precision)
     d = upload(case)
@@ -174,6 +176,9 @@ def test_apply(sgm, name, precision):
     ctx.mas_set_contacts(d["pairs"], cp)
     ctx.mas_assemble(d["vals"], d["rows"], d["cols"])
     torch.cuda.synchronize()
+    if name == "g80k":
+        ls = ctx.mas_tables()["level_size"]
+        assert len(ls) > 3 and (ls[-1, 1] - ls[2, 1]) // 16 > 32, ls
     hess_g, _ = ctx.mas_matrices()
     m = case.oracle_mas(pairs=bool(cp), precision=PREC[precision])
     m.set_hess(hess_g, PREC[precision])
