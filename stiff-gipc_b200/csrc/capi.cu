@@ -85,7 +85,7 @@ void free_all(sgmas_context* c) {
                     c->d_z, c->d_p0, c->d_p1, c->d_Ap, c->d_diag_inv, c->d_abd_inv, c->d_partials, c->d_ticket,
                     c->d_state, c->d_hvals, c->d_hb, c->d_hx, c->d_hrows, c->d_hcols, c->d_sort_scratch,
                     c->d_coarse_ticket, c->bsr.row_list, c->bsr.d_nlong, c->bsr.tcols, c->bsr.tsrc,
-                    c->d_psync, c->d_stamps, c->d_l1_bank, c->d_own1, c->d_tune_x};
+                    c->d_psync, c->d_stamps, c->d_l1_bank, c->d_own1, c->d_tune_x, c->bsr.udesc};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

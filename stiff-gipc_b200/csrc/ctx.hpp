@@ -57,6 +57,7 @@ struct BsrMatrix {
     int* tcols = nullptr;             // [cap] lower entries in claim order (scratch)
     uint32_t* tsrc = nullptr;         // [cap]
     int* row_list = nullptr;          // [nrows] long rows first, then short rows (row order)
+    int4* udesc = nullptr;            // [nrows * 4] SpMV work-unit descriptors (unit, lane group)
     int* d_nlong = nullptr;           // [1]
     int n_long = 0;                   // rows handled by a whole warp
     int rows_cap = 0;
@@ -71,6 +72,7 @@ struct BsrView {
     const int* row_list;
     int nrows;
     int n_long;
+    const int4* udesc;  // precomputed unit descriptors (NULL: computed from row_list / row_ptr)
 };
 
 struct sgmas_context {
@@ -130,6 +132,7 @@ struct sgmas_context {
     int own1_cap = 0;
     int partial_cap = 0;
     double* d_tune_x = nullptr;           // scratch solution of the autotuner's trial solves
+    int spmv_resident = 0;                // resident CTAs of the graph-form SpMV (0: not yet queried)
     int tune_cap = 0;
     PcgState* d_state = nullptr;
     // uploaded host systems (sgmas_pcg_solve_host)

@@ -244,6 +244,30 @@ __global__ void k_abd_inverse(int bodies, int nb, const int* __restrict__ rows, 
 //   MODE 1: p_new = z + beta p_old (fused), Ap = A p_new, p.Ap -> alpha
 //   MODE 2: r = rhs - A x
 // ---------------------------------------------------------------------------
+// SpMV work-unit descriptors (unit_desc for every unit and lane group),
+// once per block CSR build: a warp then reads its next unit's rows with one
+// independent load instead of the row_list -> row_ptr chain.
+__global__ void k_unit_desc(int nrows, const int* __restrict__ row_ptr, const int* __restrict__ row_list,
+                            const int* __restrict__ d_nlong, int4* udesc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n_long = *d_nlong;
+    if (i >= spmv_units(n_long, nrows) * kRowGroups) return;
+    const int u = i / kRowGroups, g = i % kRowGroups;
+    int4 d = make_int4(-1, 0, 0, 0);
+    if (u < n_long) {
+        d.x = row_list[u];
+        d.w = 1;
+    } else {
+        const int k = (u - n_long) * kRowGroups + g;
+        if (k < nrows - n_long) d.x = row_list[n_long + k];
+    }
+    if (d.x >= 0) {
+        d.y = row_ptr[d.x];
+        d.z = row_ptr[d.x + 1];
+    }
+    udesc[i] = d;
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kT) k_bsr_spmv(BsrView A, const double* __restrict__ xin, const double* __restrict__ pold,
                                                  double* pnew, double* y, const double* __restrict__ rhs, double a,
@@ -251,8 +275,18 @@ __global__ void __launch_bounds__(kT) k_bsr_spmv(BsrView A, const double* __rest
     if (MODE != 0 && st->done) return;
     __shared__ double sh[32];
     const double beta = MODE == 1 ? st->beta : 0.0;
-    const int gw = blockIdx.x * (kT / 32) + (threadIdx.x >> 5);
-    const double dot = spmv_unit<MODE>(A, gw, threadIdx.x & 31, xin, pold, pnew, y, rhs, a, b, beta);
+    const int lane = threadIdx.x & 31, units = spmv_units(A.n_long, A.nrows), stride = gridDim.x * (kT / 32);
+    const int4 none = make_int4(-1, 0, 0, 0);
+    int gw = blockIdx.x * (kT / 32) + (threadIdx.x >> 5);  // warp-uniform
+    int4 d = gw < units ? __ldg(A.udesc + (size_t)gw * kRowGroups + lane / kRowLanes) : none;
+    double dot = 0.0;
+    while (gw < units) {
+        const int gn = gw + stride;
+        const int4 dn = gn < units ? __ldg(A.udesc + (size_t)gn * kRowGroups + lane / kRowLanes) : none;
+        dot += spmv_unit_d<MODE>(A, d, lane, xin, pold, pnew, y, rhs, a, b, beta);
+        d = dn;
+        gw = gn;
+    }
     if (MODE != 1) return;
     double total;
     if (grid_sum_last<kT>(block_sum<kT>(dot, sh), partials, ticket, sh, &total)) {
@@ -502,7 +536,8 @@ int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* 
     if (nrows > B.rows_cap) {
         if (ctx_alloc(c, &B.row_ptr, (size_t)nrows + 1) || ctx_alloc(c, &B.cnt, nrows) ||
             ctx_alloc(c, &B.cnt_lower, nrows) || ctx_alloc(c, &B.fill, nrows) || ctx_alloc(c, &B.first, nrows) ||
-            ctx_alloc(c, &B.row_list, nrows) || ctx_alloc(c, &B.d_nlong, 1))
+            ctx_alloc(c, &B.row_list, nrows) || ctx_alloc(c, &B.d_nlong, 1) ||
+            ctx_alloc(c, &B.udesc, (size_t)nrows * kRowGroups))
             return SGMAS_ERR_CUDA;
         B.rows_cap = nrows;
     }
@@ -530,7 +565,8 @@ int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* 
                                                              B.cols, B.src);
     k_bsr_values<<<(int)((B.cap + kT - 1) / kT), kT, 0, s>>>(B.cap, B.row_ptr, nrows, B.src, vals, B.vals);
     k_row_split<<<1, 1024, 0, s>>>(nrows, B.row_ptr, B.row_list, B.d_nlong);
-    c->build_launches += 4 + (nb > 0 ? 2 : 0);
+    k_unit_desc<<<(nrows * kRowGroups + kT - 1) / kT, kT, 0, s>>>(nrows, B.row_ptr, B.row_list, B.d_nlong, B.udesc);
+    c->build_launches += 5 + (nb > 0 ? 2 : 0);
     SG_CUDA(c, cudaGetLastError());
     // the long-row count sizes the SpMV grid (one 4-byte read per build)
     SG_CUDA(c, cudaMemcpyAsync(&B.n_long, B.d_nlong, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -539,16 +575,25 @@ int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* 
 }
 
 static BsrView bsr_view(const BsrMatrix& B) {
-    return BsrView{B.row_ptr, B.cols, B.vals, B.cap, B.row_list, B.nrows, B.n_long};
+    return BsrView{B.row_ptr, B.cols, B.vals, B.cap, B.row_list, B.nrows, B.n_long, B.udesc};
 }
-static int spmv_grid(const BsrMatrix& B) {
+// one warp per work unit, but no more CTAs than stay resident: the warps loop
+// over units (next descriptor in flight) and reduce once at the end
+static int spmv_grid(sgmas_context* c, const BsrMatrix& B) {
     const int warps = spmv_units(B.n_long, B.nrows);
-    return (warps + kT / 32 - 1) / (kT / 32);
+    const int need = (warps + kT / 32 - 1) / (kT / 32);
+    if (!c->spmv_resident) {
+        int sms = 0, occ = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bsr_spmv<1>, kT, 0);
+        c->spmv_resident = std::max(1, sms * std::max(1, occ));
+    }
+    return std::max(1, std::min(need, c->spmv_resident));
 }
 
 int bsr_spmv_plain(sgmas_context* c, double a, const double* x, double b, double* y) {
     const BsrMatrix& B = c->bsr;
-    k_bsr_spmv<0><<<spmv_grid(B), kT, 0, c->stream>>>(bsr_view(B), x, nullptr, nullptr, y, nullptr, a, b, nullptr,
+    k_bsr_spmv<0><<<spmv_grid(c, B), kT, 0, c->stream>>>(bsr_view(B), x, nullptr, nullptr, y, nullptr, a, b, nullptr,
                                                       nullptr, nullptr);
     SG_CUDA(c, cudaGetLastError());
     return 0;
@@ -601,7 +646,7 @@ static int record_prologue(sgmas_context* c, const double* b, double* x, const P
     if (cfg.warm) {
         const int gv = std::min((n + kT - 1) / kT, 4 * 148);
         k_warm_dots<<<gv, kT, 0, s>>>(n, x, b, c->d_state, c->d_partials, c->d_ticket);
-        k_bsr_spmv<1><<<spmv_grid(c->bsr), kT, 0, s>>>(bsr_view(c->bsr), x, x, c->d_p1, c->d_Ap, nullptr, 1.0, 0.0,
+        k_bsr_spmv<1><<<spmv_grid(c, c->bsr), kT, 0, s>>>(bsr_view(c->bsr), x, x, c->d_p1, c->d_Ap, nullptr, 1.0, 0.0,
                                                        c->d_state, c->d_partials, c->d_ticket);
         k_warm_residual<<<gv, kT, 0, s>>>(n, x, c->d_r, b, c->d_Ap, c->d_state, c->d_partials, c->d_ticket);
         k_warm_reject<<<gv, kT, 0, s>>>(n, x, c->d_r, b, c->d_state);
@@ -626,7 +671,7 @@ static int record_body(sgmas_context* c, cudaStream_t s, const double* b, double
                        unsigned long long cond, int* nk) {
     const int nrows = c->bsr.nrows, n = 3 * nrows;
     const BsrMatrix& B = c->bsr;
-    const int gs = spmv_grid(B);
+    const int gs = spmv_grid(c, B);
     const int gj = (nrows + kT - 1) / kT;
     cudaStream_t saved = c->stream;
     c->stream = s;
@@ -864,7 +909,7 @@ int pcg_profile(sgmas_context* c, int reps, float* ms, int n_ms) {
     if (!(h.rz == h.rz) || h.rz == 0.0) h.rz = 1.0;
     SG_CUDA(c, cudaMemcpyAsync(c->d_state, &h, sizeof(PcgState), cudaMemcpyHostToDevice, s));
     for (int i = 0; i < n_ms; ++i) ms[i] = 0.f;
-    const int gs = spmv_grid(B), gj = (nrows + kT - 1) / kT;
+    const int gs = spmv_grid(c, B), gj = (nrows + kT - 1) / kT;
     int rc = 0;
     for (int part = 0; part < 4 && part < n_ms && rc == 0; ++part) {
         if (c->last_cfg.precond == 0 && part >= 2) break;

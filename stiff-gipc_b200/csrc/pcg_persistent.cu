@@ -898,7 +898,7 @@ int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRu
     const BsrMatrix& M = c->bsr;
 
     PArgs a = {};
-    a.A = BsrView{M.row_ptr, M.cols, M.vals, M.cap, M.row_list, M.nrows, M.n_long};
+    a.A = BsrView{M.row_ptr, M.cols, M.vals, M.cap, M.row_list, M.nrows, M.n_long, nullptr};
     a.b = b; a.x = x; a.r = c->d_r; a.z = c->d_z; a.p0 = c->d_p0; a.p1 = c->d_p1; a.Ap = c->d_Ap;
     a.nrows = M.nrows;
     a.units = spmv_units(M.n_long, M.nrows);

@@ -48,6 +48,9 @@ def build(name, bank=16):
     elif name == "g80k":  # large enough for more than 32 subdomains at levels >= 2
         s = synth.stencil_grid_system(64, 36, 36, E=1e5, n_pairs=2000, seed=3)
         pm, rm = O.morton_partition(s.pos, bank)
+    elif name == "g221k":  # block CSR of both triangles about twice the 126 MB L2
+        s = synth.stencil_grid_system(96, 48, 48, E=1e5, n_pairs=4000, seed=4)
+        pm, rm = O.morton_partition(s.pos, bank)
     elif name in ("bar", "bunny2", "cube"):
         g = golden(name)
         s = synth.mesh_system(g["pos"], g["tets"], seed=2)
