@@ -603,9 +603,10 @@ __global__ void __launch_bounds__(32 * inv_warps<B>()) k_chol_inv(int nblk, cons
 // ---------------------------------------------------------------------------
 
 
-// Stage `nb` consecutive bank tiles into shared memory with one bulk copy.
+// Start staging `nb` consecutive bank tiles into shared memory with one bulk
+// copy; the caller waits on `bar` (phase 0) before it reads them.
 template <typename S>
-__device__ __forceinline__ bool stage_tiles(S* tile, const S* src, int nb, int bs, uint64_t* bar, int* err) {
+__device__ __forceinline__ void stage_tiles_issue(S* tile, const S* src, int nb, int bs, uint64_t* bar) {
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         fence_mbar_init();
@@ -616,7 +617,6 @@ __device__ __forceinline__ bool stage_tiles(S* tile, const S* src, int nb, int b
         mbar_expect_tx(bar, bytes);
         bulk_g2s(tile, src, bytes, bar);
     }
-    return mbar_wait(bar, 0, err);
 }
 
 constexpr int kL0Banks = 4;         // level-0 banks per CTA of the level-0 kernel
@@ -648,7 +648,8 @@ __global__ void __launch_bounds__(kL0Banks * B) k_apply_l0(int Mm, int L, const 
     S* tile = reinterpret_cast<S*>(smem_raw);
     const int bank0 = blockIdx.x * kL0Banks;
     const int nb = min(kL0Banks, Mm / B - bank0);
-    const bool ok = stage_tiles<S>(tile, inv + (size_t)bank0 * bs * 9, nb, bs, &bar, err);
+    // the tiles arrive while the slot's vectors are read and updated
+    stage_tiles_issue<S>(tile, inv + (size_t)bank0 * bs * 9, nb, bs, &bar);
 
     const int tdx = blockIdx.x * (kL0Banks * B) + threadIdx.x;
     const int lane = threadIdx.x % B;
@@ -677,7 +678,7 @@ __global__ void __launch_bounds__(kL0Banks * B) k_apply_l0(int Mm, int L, const 
         const int nx = going_next[idx];
         R[3 * (size_t)nx] = s0; R[3 * (size_t)nx + 1] = s1; R[3 * (size_t)nx + 2] = s2;
     }
-    if (!ok) return;
+    if (!mbar_wait(&bar, 0, err)) return;
     Acc z0, z1, z2;
     schwarz_rows<B, S, Acc>(tile + (size_t)(threadIdx.x / B) * bs * 9, lane, xb, z0, z1, z2);
     if (tdx < Mm) {
@@ -705,8 +706,7 @@ __device__ __forceinline__ bool schwarz_banks(const S* __restrict__ inv, Acc* R,
             mbar_expect_tx(bar, bytes);
             bulk_g2s(tile, inv + (size_t)(bank0 + c0) * bs * 9, bytes, bar);
         }
-        if (!mbar_wait(bar, phase, err)) return false;
-        phase ^= 1u;
+        bool staged = false;  // the first pass reads its residuals while the tiles arrive
         for (int q = threadIdx.x / B; q < ((nc + per_pass - 1) / per_pass) * per_pass; q += per_pass) {
             const bool valid = q < nc;
             const int node = (bank0 + c0 + q) * B + lane;
@@ -721,6 +721,11 @@ __device__ __forceinline__ bool schwarz_banks(const S* __restrict__ inv, Acc* R,
                 bool lead;
                 group_sum<B, Acc>(par, xb, lane, s0, s1, s2, lead);
                 if (lead) { R[3 * (size_t)par] = s0; R[3 * (size_t)par + 1] = s1; R[3 * (size_t)par + 2] = s2; }
+            }
+            if (!staged) {  // same trip count on every thread: all wait here once per chunk
+                if (!mbar_wait(bar, phase, err)) return false;
+                phase ^= 1u;
+                staged = true;
             }
             Acc z0, z1, z2;
             schwarz_rows<B, S, Acc>(tile + (size_t)(valid ? q : 0) * bs * 9, lane, xb, z0, z1, z2);
