@@ -246,6 +246,18 @@ int sgmas_spmv(sgmas_context* ctx, double a, const sgmas_bcoo* A, const double* 
  * (h_unique_key_number, global_matrix.h:197).  Outputs need n entries. */
 int sgmas_convert(sgmas_context* ctx, const double* d_values, const int* d_rows, const int* d_cols,
                   int n, double* d_out_values, int* d_out_rows, int* d_out_cols, int* n_unique);
+/* The same merge for a triplet structure that stays fixed across Newton steps
+ * (elastic terms of a mesh: same rows and cols in the same order every step).
+ * sgmas_assembly_plan sorts and merges d_rows / d_cols of n raw triplets once:
+ * the merged structure goes to d_out_rows / d_out_cols (*n_unique entries,
+ * room for n), the sorted order stays on the context.  sgmas_assemble then
+ * merges that step's n raw values (d_values [n][9]) into d_out_values
+ * [n_unique][9] with one kernel and no sort, bit-identical to what
+ * sgmas_convert returns for the same triplets.  The project's own: the
+ * reference sorts every step. */
+int sgmas_assembly_plan(sgmas_context* ctx, const int* d_rows, const int* d_cols, int n, int* d_out_rows,
+                        int* d_out_cols, int* n_unique);
+int sgmas_assemble(sgmas_context* ctx, const double* d_values, int n, double* d_out_values);
 /* write_triplet_fem / write_triplet<12,12> with SymGH (SG/femEnergy.cu:14-62,
  * SG/GIPC.cu:82-139): element matrices [n_elem][3k][3k] row-major with node
  * lists [n_elem][k] -> k(k+1)/2 upper triplets per element */

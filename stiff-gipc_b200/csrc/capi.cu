@@ -85,7 +85,8 @@ void free_all(sgmas_context* c) {
                     c->d_z, c->d_p0, c->d_p1, c->d_Ap, c->d_diag_inv, c->d_abd_inv, c->d_partials, c->d_ticket,
                     c->d_state, c->d_hvals, c->d_hb, c->d_hx, c->d_hrows, c->d_hcols, c->d_sort_scratch,
                     c->d_coarse_ticket, c->bsr.row_list, c->bsr.d_nlong, c->bsr.tcols, c->bsr.tsrc,
-                    c->d_psync, c->d_stamps, c->d_l1_bank, c->d_own1, c->d_tune_x, c->bsr.udesc};
+                    c->d_psync, c->d_stamps, c->d_l1_bank, c->d_own1, c->d_tune_x, c->bsr.udesc, c->d_plan_idx,
+                    c->d_plan_start};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -449,6 +450,22 @@ int sgmas_convert(sgmas_context* c, const double* d_values, const int* d_rows, c
     int rc = convert_triplets(c, d_values, d_rows, d_cols, n, d_out_values, d_out_rows, d_out_cols, n_unique);
     if (rc) return rc;
     return check_device_error(c, "sgmas_convert");
+}
+
+int sgmas_assembly_plan(sgmas_context* c, const int* d_rows, const int* d_cols, int n, int* d_out_rows,
+                        int* d_out_cols, int* n_unique) {
+    if (!c || n < 0 || !n_unique || (n > 0 && (!d_rows || !d_cols || !d_out_rows || !d_out_cols)))
+        return SGMAS_ERR_ARG;
+    SG_CUDA(c, cudaSetDevice(c->device));
+    int rc = assembly_plan(c, d_rows, d_cols, n, d_out_rows, d_out_cols, n_unique);
+    if (rc) return rc;
+    return check_device_error(c, "sgmas_assembly_plan");
+}
+
+int sgmas_assemble(sgmas_context* c, const double* d_values, int n, double* d_out_values) {
+    if (!c || n < 0 || (n > 0 && (!d_values || !d_out_values))) return SGMAS_ERR_ARG;
+    SG_CUDA(c, cudaSetDevice(c->device));
+    return assemble_planned(c, d_values, n, d_out_values);
 }
 
 int sgmas_write_upper_blocks(sgmas_context* c, const double* d_H, int n_elem, int k, const int* d_nodes,

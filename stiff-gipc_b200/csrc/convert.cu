@@ -146,23 +146,18 @@ __global__ void k_seg_starts(int n, const uint64_t* __restrict__ keys, const int
     out_rows[u] = (int)(keys[i] >> cb);
     out_cols[u] = (int)(keys[i] & ((1ull << cb) - 1ull));
 }
-// one thread per merged block: sum its run in sorted (stable) order
+// nine threads per merged block, one per component: each sums its component
+// over the block's run in sorted (stable) order -- the order, and so the
+// result, of a per-block sum -- while the nine read one block's 72 bytes together
 __global__ void k_seg_sum(int nu, int n, const int* __restrict__ start, const uint32_t* __restrict__ idx,
                           const double* __restrict__ vals, double* out) {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= nu) return;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 9LL * nu) return;
+    const int u = (int)(t / 9), q = (int)(t % 9);
     const int b = start[u], e = (u + 1 < nu) ? start[u + 1] : n;
-    double s[9];
-    const size_t k0 = idx[b];
-    #pragma unroll
-    for (int q = 0; q < 9; ++q) s[q] = vals[9 * k0 + q];
-    for (int i = b + 1; i < e; ++i) {
-        const size_t k = idx[i];
-        #pragma unroll
-        for (int q = 0; q < 9; ++q) s[q] += vals[9 * k + q];
-    }
-    #pragma unroll
-    for (int q = 0; q < 9; ++q) out[9 * (size_t)u + q] = s[q];
+    double s = vals[9 * (size_t)idx[b] + q];
+    for (int i = b + 1; i < e; ++i) s += vals[9 * (size_t)idx[i] + q];
+    out[9 * (size_t)u + q] = s;
 }
 
 // upper triplets of element matrices: one thread per (element, block pair)
@@ -367,9 +362,72 @@ int convert_triplets(sgmas_context* c, const double* vals, const int* rows, cons
     SG_CUDA(c, cudaStreamSynchronize(s));
     const int nu = h2[1];
     k_seg_starts<<<g, kT, 0, s>>>(n, keys, head, seg, cb, start, out_rows, out_cols);
-    k_seg_sum<<<(nu + kT - 1) / kT, kT, 0, s>>>(nu, n, start, idx, vals, out_vals);
+    k_seg_sum<<<(int)((9LL * nu + kT - 1) / kT), kT, 0, s>>>(nu, n, start, idx, vals, out_vals);
     SG_CUDA(c, cudaGetLastError());
     *n_unique = nu;
+    return 0;
+}
+
+// Assembly plan: the key sort and merge of convert_triplets for a fixed
+// triplet structure, once.  The stable sorted order (idx) and the segment
+// starts stay on the context; assemble_planned then runs only k_seg_sum, so
+// its sums are convert_triplets' to the bit.
+int assembly_plan(sgmas_context* c, const int* rows, const int* cols, int n, int* out_rows, int* out_cols,
+                  int* n_unique) {
+    *n_unique = 0;
+    c->plan_n = -1;
+    if (n == 0) {
+        c->plan_n = 0;
+        c->plan_nu = 0;
+        return 0;
+    }
+    if (ctx_alloc_grow(c, &c->d_plan_idx, &c->plan_idx_cap, n) || ctx_alloc_grow(c, &c->d_plan_start, &c->plan_start_cap, n))
+        return SGMAS_ERR_CUDA;
+    cudaStream_t s = c->stream;
+    const size_t need = (size_t)n * (8 + 4 + 4) + sort_scratch_size(n) + 8192;
+    if (ensure_scratch(c, need)) return SGMAS_ERR_CUDA;
+    Scratch S{(unsigned char*)c->d_sort_scratch, 0};
+    uint64_t* keys = S.take<uint64_t>(n);
+    int* head = S.take<int>(n);
+    int* seg = S.take<int>(n);
+    int* misc = S.take<int>(4);
+    int* sums = S.take<int>((n + 1023) / 1024 + 1);
+    uint32_t* idx = reinterpret_cast<uint32_t*>(c->d_plan_idx);
+    SG_CUDA(c, cudaMemsetAsync(misc, 0, sizeof(int) * 4, s));
+    k_max_index<<<min(1024, (n + kT - 1) / kT), kT, 0, s>>>(n, rows, cols, misc);
+    int mx = 0;
+    SG_CUDA(c, cudaMemcpyAsync(&mx, misc, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SG_CUDA(c, cudaStreamSynchronize(s));
+    int cb = 1;
+    while ((1ll << cb) <= (long long)mx) ++cb;
+    const int g = (n + kT - 1) / kT;
+    k_make_keys<<<g, kT, 0, s>>>(n, rows, cols, cb, keys, idx, c->d_err);
+    int rc = sort_pairs_impl(c, keys, idx, n, 2 * cb, S);
+    if (rc) return rc;
+    k_heads<<<g, kT, 0, s>>>(n, keys, head);
+    rc = scan_ints(c, head, seg, n, sums, misc + 1);
+    if (rc) return rc;
+    int h2[2];
+    SG_CUDA(c, cudaMemcpyAsync(h2, misc, sizeof(int) * 2, cudaMemcpyDeviceToHost, s));
+    SG_CUDA(c, cudaStreamSynchronize(s));
+    k_seg_starts<<<g, kT, 0, s>>>(n, keys, head, seg, cb, c->d_plan_start, out_rows, out_cols);
+    SG_CUDA(c, cudaGetLastError());
+    c->plan_n = n;
+    c->plan_nu = h2[1];
+    *n_unique = h2[1];
+    return 0;
+}
+
+int assemble_planned(sgmas_context* c, const double* vals, int n, double* out_vals) {
+    if (c->plan_n < 0) return ctx_fail(c, SGMAS_ERR_STATE, "sgmas_assemble before sgmas_assembly_plan");
+    if (n != c->plan_n)
+        return ctx_fail(c, SGMAS_ERR_ARG, "sgmas_assemble: %d triplets, the plan has %d", n, c->plan_n);
+    const int nu = c->plan_nu;
+    if (nu == 0) return 0;
+    k_seg_sum<<<(int)((9LL * nu + kT - 1) / kT), kT, 0, c->stream>>>(nu, n, c->d_plan_start,
+                                                        reinterpret_cast<const uint32_t*>(c->d_plan_idx), vals,
+                                                        out_vals);
+    SG_CUDA(c, cudaGetLastError());
     return 0;
 }
 

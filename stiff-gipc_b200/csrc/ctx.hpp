@@ -133,6 +133,11 @@ struct sgmas_context {
     int partial_cap = 0;
     double* d_tune_x = nullptr;           // scratch solution of the autotuner's trial solves
     int spmv_resident = 0;                // resident CTAs of the graph-form SpMV (0: not yet queried)
+    // assembly plan (sgmas_assembly_plan): stable sorted order of the raw triplets, segment starts
+    int* d_plan_idx = nullptr;
+    int* d_plan_start = nullptr;
+    int plan_idx_cap = 0, plan_start_cap = 0;
+    int plan_n = -1, plan_nu = 0;         // raw triplets and merged blocks of the plan (-1: none)
     int tune_cap = 0;
     PcgState* d_state = nullptr;
     // uploaded host systems (sgmas_pcg_solve_host)
@@ -202,6 +207,9 @@ int mas_launch_apply(sgmas_context* c, const double* r, double* z, int mode, con
 ExtraRows extra_rows_of(const sgmas_context* c, const PcgRunCfg& cfg);
 int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* cols, int nblocks,
               int nrows);
+int assembly_plan(sgmas_context* c, const int* rows, const int* cols, int n, int* out_rows, int* out_cols,
+                  int* n_unique);
+int assemble_planned(sgmas_context* c, const double* vals, int n, double* out_vals);
 void bsr_mark_fresh(sgmas_context* c, const sgmas_bcoo* A);  // the CSR just built is A's
 bool bsr_reuse(sgmas_context* c, const sgmas_bcoo* A);       // true (once) when the fresh CSR is A's
 int bsr_spmv_plain(sgmas_context* c, double a, const double* x, double b, double* y);

@@ -69,7 +69,7 @@ EXPORTS = [
     "sgmas_part_maps", "sgmas_morton_codes_noalloc", "sgmas_set_pcg_mode", "sgmas_pcg_last_vectors",
     "sgmas_mtx_write", "sgmas_mtx_read", "sgmas_set_pcg_ctas", "sgmas_mlp_set_params", "sgmas_mlp_get_params", "sgmas_mlp_features",
     "sgmas_mlp_gradient", "sgmas_mlp_train_step", "sgmas_mlp_forward", "sgmas_mlp_warm_start",
-    "sgmas_autotune_pcg",
+    "sgmas_autotune_pcg", "sgmas_assembly_plan", "sgmas_assemble",
 ]
 MLP_PARAMS = 19462  # SGMAS_MLP_PARAMS in include/sgmas.h
 
@@ -117,6 +117,8 @@ def lib(build_if_missing: bool = False):
     L.sgmas_set_pcg_ctas.argtypes = [vp, i]
     L.sgmas_autotune_pcg.argtypes = [vp, C.POINTER(Bcoo), vp, C.POINTER(PcgConfig), i, i, i, i, C.POINTER(TuneReport)]
     L.sgmas_pcg_last_vectors.argtypes = [vp, vp, vp]
+    L.sgmas_assembly_plan.argtypes = [vp, vp, vp, i, vp, vp, C.POINTER(i)]
+    L.sgmas_assemble.argtypes = [vp, vp, i, vp]
     L.sgmas_mtx_write.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, i, vp]
     L.sgmas_mtx_read.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, vp, i, C.POINTER(i), C.POINTER(i)]
     f = C.c_float
@@ -436,6 +438,17 @@ class Context:
         self._check(self.L.sgmas_convert(self.h, _ptr(vals), _ptr(rows), _ptr(cols), int(rows.shape[0]),
                                          _ptr(out_vals), _ptr(out_rows), _ptr(out_cols), C.byref(nu)))
         return nu.value
+
+    def assembly_plan(self, rows, cols, out_rows, out_cols):
+        """Sort and merge a fixed triplet structure once (sgmas_assembly_plan); returns the merged count."""
+        nu = C.c_int()
+        self._check(self.L.sgmas_assembly_plan(self.h, _ptr(rows), _ptr(cols), int(rows.shape[0]), _ptr(out_rows),
+                                               _ptr(out_cols), C.byref(nu)))
+        return nu.value
+
+    def assemble(self, vals, out_vals):
+        """Merge one step's raw values in the planned structure (sgmas_assemble)."""
+        self._check(self.L.sgmas_assemble(self.h, _ptr(vals), int(vals.shape[0]), _ptr(out_vals)))
 
     def write_upper_blocks(self, H, nodes, vals, rows, cols):
         n_elem, k = int(nodes.shape[0]), int(nodes.shape[1])

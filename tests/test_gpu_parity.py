@@ -462,6 +462,45 @@ def test_convert_bit_exact(sgm, name):
     ctx.close()
 
 
+@pytest.mark.parametrize("name", ["c1", "c2s"])
+def test_assembly_plan_matches_convert(sgm, name):
+    """Plan a triplet structure once, then assemble two steps' values: each
+    step equals sgmas_convert of the same triplets bit for bit (the same
+    stable order, the same sums), with no sort per step."""
+    s = synth.config1(seed=5, keep_raw=True) if name == "c1" else synth.config2(seed=5, scale=0.3, keep_raw=True)
+    ctx = sgm.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    n = len(s.raw_rows)
+    rng = np.random.default_rng(1)
+    perm = rng.permutation(n)
+    rr, rc = dev(s.raw_rows[perm]), dev(s.raw_cols[perm])
+    pr = torch.zeros(n, dtype=torch.int32, device="cuda")
+    pc = torch.zeros(n, dtype=torch.int32, device="cuda")
+    nu = ctx.assembly_plan(rr, rc, pr, pc)
+    for step in range(2):
+        rv = s.raw_vals[perm] * (1.0 + 0.25 * step) + rng.normal(size=s.raw_vals[perm].shape) * 1e-3 * step
+        out = torch.zeros((n, 9), dtype=torch.float64, device="cuda")
+        ctx.assemble(dev(rv), out)
+        cv = torch.zeros((n, 9), dtype=torch.float64, device="cuda")
+        cr = torch.zeros(n, dtype=torch.int32, device="cuda")
+        cc = torch.zeros(n, dtype=torch.int32, device="cuda")
+        assert ctx.convert(dev(rv), rr, rc, cv, cr, cc) == nu
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(pr.cpu().numpy()[:nu], cr.cpu().numpy()[:nu])
+        np.testing.assert_array_equal(pc.cpu().numpy()[:nu], cc.cpu().numpy()[:nu])
+        np.testing.assert_array_equal(out.cpu().numpy()[:nu].view(np.uint64), cv.cpu().numpy()[:nu].view(np.uint64))
+    with pytest.raises(sgm.SgmasError):  # another triplet count than planned
+        ctx.assemble(dev(np.zeros((n - 1, 9))), out)
+    ctx.close()
+
+
+def test_assemble_before_plan_refused(sgm):
+    ctx = sgm.Context(0)
+    with pytest.raises(sgm.SgmasError):
+        ctx.assemble(dev(np.zeros((4, 9))), torch.zeros((4, 9), dtype=torch.float64, device="cuda"))
+    ctx.close()
+
+
 def test_upper_blocks_bit_exact(sgm):
     rng = np.random.default_rng(1)
     m, k = 500, 4
