@@ -41,6 +41,24 @@ class Context {
     void set_pcg_mode(int mode) { check(ctx_, sgmas_set_pcg_mode(ctx_, mode), "sgmas_set_pcg_mode"); }
     // at most max_ctas CTAs for the persistent form (0: every SM); for solves of many contexts side by side
     void set_pcg_ctas(int max_ctas) { check(ctx_, sgmas_set_pcg_ctas(ctx_, max_ctas), "sgmas_set_pcg_ctas"); }
+    // launch shape by timed trial solves on A (kept on the context); see sgmas_autotune_pcg
+    sgmas_tune_report autotune(const sgmas_bcoo& A, const double* d_b, const sgmas_pcg_config& cfg,
+                               int objective = SGMAS_TUNE_THROUGHPUT, int concurrency = 1, int trial_iters = 30,
+                               int reps = 2) {
+        sgmas_tune_report r{};
+        check(ctx_, sgmas_autotune_pcg(ctx_, &A, d_b, &cfg, objective, concurrency, trial_iters, reps, &r),
+              "sgmas_autotune_pcg");
+        return r;
+    }
+    // fixed triplet structure: sort and merge once, then merge each step's values without a sort
+    int assembly_plan(const int* d_rows, const int* d_cols, int n, int* d_out_rows, int* d_out_cols) {
+        int nu = 0;
+        check(ctx_, sgmas_assembly_plan(ctx_, d_rows, d_cols, n, d_out_rows, d_out_cols, &nu), "sgmas_assembly_plan");
+        return nu;
+    }
+    void assemble(const double* d_values, int n, double* d_out_values) {
+        check(ctx_, sgmas_assemble(ctx_, d_values, n, d_out_values), "sgmas_assemble");
+    }
 
   private:
     sgmas_context* ctx_ = nullptr;
