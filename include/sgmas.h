@@ -258,6 +258,33 @@ int sgmas_convert(sgmas_context* ctx, const double* d_values, const int* d_rows,
 int sgmas_assembly_plan(sgmas_context* ctx, const int* d_rows, const int* d_cols, int n, int* d_out_rows,
                         int* d_out_cols, int* n_unique);
 int sgmas_assemble(sgmas_context* ctx, const double* d_values, int n, double* d_out_values);
+
+/* Affine-body coupling (ABDSystem::_setup_abd_system_hessian,
+ * SG/abd_system/abd_system_function/setup_abd_system_gradient_and_hessian.cu:419-601):
+ * vertex-level 3x3 blocks into the 3x3 triplets of the 12-DOF body rows (body b
+ * owns block rows 4b .. 4b + 3).  A body vertex moves as x = J(xb) q with
+ * J = [I | e1 xb^T | e2 xb^T | e3 xb^T] of its rest position xb (d_xbar [3 per
+ * vertex]); d_body_of gives each body vertex's body, d_fixed[b] != 0 marks a
+ * fixed body (BodyBoundaryType::Fixed).  Blocks are 9 doubles column-major.
+ * sgmas_abd_body_blocks: each body's 12x12 Hessian (144 doubles, column-major)
+ *   -> its 10 upper blocks (write_abd_body_hessian :127-136).
+ * sgmas_abd_pair_blocks: n merged body-body vertex-pair blocks (row, col =
+ *   vertex ids) -> 16 blocks each of J_i^T H J_j at [16 t, 16 t + 16), blocks
+ *   below the diagonal written as zero with swapped indices (write_barrier_hessian
+ *   :84-124); zero when either body is fixed.
+ * sgmas_abd_fem_blocks: n body-vertex / FEM-vertex blocks (col = global point
+ *   id, FEM point = col - fem_point_offset) -> 4 blocks each of J^T H at rows
+ *   4 body + k, column 4 n_bodies + FEM point (:505-560); zero when the FEM
+ *   point's boundary type (d_fem_boundary) is nonzero or the body is fixed. */
+int sgmas_abd_body_blocks(sgmas_context* ctx, const double* d_H12, int n_bodies, double* d_vals, int* d_rows,
+                          int* d_cols);
+int sgmas_abd_pair_blocks(sgmas_context* ctx, const double* d_in_vals, const int* d_in_rows, const int* d_in_cols,
+                          int n, const double* d_xbar, const int* d_body_of, const int* d_fixed, double* d_vals,
+                          int* d_rows, int* d_cols);
+int sgmas_abd_fem_blocks(sgmas_context* ctx, const double* d_in_vals, const int* d_in_rows, const int* d_in_cols,
+                         int n, const double* d_xbar, const int* d_body_of, const int* d_fixed,
+                         const int* d_fem_boundary, int fem_point_offset, int n_bodies, double* d_vals, int* d_rows,
+                         int* d_cols);
 /* write_triplet_fem / write_triplet<12,12> with SymGH (SG/femEnergy.cu:14-62,
  * SG/GIPC.cu:82-139): element matrices [n_elem][3k][3k] row-major with node
  * lists [n_elem][k] -> k(k+1)/2 upper triplets per element */

@@ -69,7 +69,8 @@ EXPORTS = [
     "sgmas_part_maps", "sgmas_morton_codes_noalloc", "sgmas_set_pcg_mode", "sgmas_pcg_last_vectors",
     "sgmas_mtx_write", "sgmas_mtx_read", "sgmas_set_pcg_ctas", "sgmas_mlp_set_params", "sgmas_mlp_get_params", "sgmas_mlp_features",
     "sgmas_mlp_gradient", "sgmas_mlp_train_step", "sgmas_mlp_forward", "sgmas_mlp_warm_start",
-    "sgmas_autotune_pcg", "sgmas_assembly_plan", "sgmas_assemble",
+    "sgmas_autotune_pcg", "sgmas_assembly_plan", "sgmas_assemble", "sgmas_abd_body_blocks",
+    "sgmas_abd_pair_blocks", "sgmas_abd_fem_blocks",
 ]
 MLP_PARAMS = 19462  # SGMAS_MLP_PARAMS in include/sgmas.h
 
@@ -119,6 +120,9 @@ def lib(build_if_missing: bool = False):
     L.sgmas_pcg_last_vectors.argtypes = [vp, vp, vp]
     L.sgmas_assembly_plan.argtypes = [vp, vp, vp, i, vp, vp, C.POINTER(i)]
     L.sgmas_assemble.argtypes = [vp, vp, i, vp]
+    L.sgmas_abd_body_blocks.argtypes = [vp, vp, i, vp, vp, vp]
+    L.sgmas_abd_pair_blocks.argtypes = [vp, vp, vp, vp, i, vp, vp, vp, vp, vp, vp]
+    L.sgmas_abd_fem_blocks.argtypes = [vp, vp, vp, vp, i, vp, vp, vp, vp, i, i, vp, vp, vp]
     L.sgmas_mtx_write.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, i, vp]
     L.sgmas_mtx_read.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, i, vp, i, C.POINTER(i), C.POINTER(i)]
     f = C.c_float
@@ -449,6 +453,26 @@ class Context:
     def assemble(self, vals, out_vals):
         """Merge one step's raw values in the planned structure (sgmas_assemble)."""
         self._check(self.L.sgmas_assemble(self.h, _ptr(vals), int(vals.shape[0]), _ptr(out_vals)))
+
+    # ---- affine-body coupling (vertex blocks -> 12-DOF body rows) ----
+    def abd_body_blocks(self, H12, vals, rows, cols):
+        """Each body's 12x12 Hessian (column-major) -> its 10 upper 3x3 blocks."""
+        self._check(self.L.sgmas_abd_body_blocks(self.h, _ptr(H12), int(H12.shape[0]), _ptr(vals), _ptr(rows),
+                                                 _ptr(cols)))
+
+    def abd_pair_blocks(self, in_vals, in_rows, in_cols, xbar, body_of, fixed, vals, rows, cols):
+        """Body-body vertex-pair blocks -> 16 blocks each of J_i^T H J_j."""
+        self._check(self.L.sgmas_abd_pair_blocks(self.h, _ptr(in_vals), _ptr(in_rows), _ptr(in_cols),
+                                                 int(in_rows.shape[0]), _ptr(xbar), _ptr(body_of), _ptr(fixed),
+                                                 _ptr(vals), _ptr(rows), _ptr(cols)))
+
+    def abd_fem_blocks(self, in_vals, in_rows, in_cols, xbar, body_of, fixed, fem_boundary, fem_point_offset,
+                       n_bodies, vals, rows, cols):
+        """Body-vertex / FEM-vertex blocks -> 4 blocks each of J^T H."""
+        self._check(self.L.sgmas_abd_fem_blocks(self.h, _ptr(in_vals), _ptr(in_rows), _ptr(in_cols),
+                                                int(in_rows.shape[0]), _ptr(xbar), _ptr(body_of), _ptr(fixed),
+                                                _ptr(fem_boundary), int(fem_point_offset), int(n_bodies), _ptr(vals),
+                                                _ptr(rows), _ptr(cols)))
 
     def write_upper_blocks(self, H, nodes, vals, rows, cols):
         n_elem, k = int(nodes.shape[0]), int(nodes.shape[1])
