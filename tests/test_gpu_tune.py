@@ -92,3 +92,20 @@ def test_bad_arguments(sgm):
     x = torch.zeros(3 * case.n, dtype=torch.float64, device="cuda")
     assert ctx.pcg_solve(d["vals"], d["rows"], d["cols"], case.n, d["b"], x)["converged"] == 1
     ctx.close()
+
+
+def test_system_beyond_every_persistent_grid(sgm):
+    """82,944 vertices need more than 32 level-0 subdomains per CTA on every
+    grid: no persistent candidate survives, the graph form is the choice, and
+    the solve with it converges."""
+    case, ctx, d = setup(sgm, "g80k")
+    t = ctx.autotune(d["vals"], d["rows"], d["cols"], case.n, d["b"], objective="latency", trial_iters=10, reps=1)
+    c = t["candidates"]
+    assert len(c) == 1 and not c[0]["persistent"] and t["chosen"] == 0
+    x = torch.zeros(3 * case.n, dtype=torch.float64, device="cuda")
+    rep = ctx.pcg_solve(d["vals"], d["rows"], d["cols"], case.n, d["b"], x, rel_tol=1e-4)
+    assert rep["converged"] == 1 and rep["kernel_launches"] > 1
+    A = synth.full_matrix(case.s)
+    res = np.linalg.norm(case.s.b - A @ x.cpu().numpy()) / np.linalg.norm(case.s.b)
+    assert res <= 1e-4 * 1.0001, res
+    ctx.close()
