@@ -7,7 +7,7 @@ definition (include/sgmas.h, "learned start guess") in numpy -- features,
 forward pass, loss, analytic backward pass, Adam, and the BF16 inference with
 its rounding points -- and is itself checked by finite differences
 (tests/test_learned_oracle.py).  Parity with the reference is therefore
-unpinned for this part; it is judged against plain MAS-PCG.
+unpinned for this part; it is measured against plain MAS-PCG.
 """
 from __future__ import annotations
 
