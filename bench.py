@@ -575,32 +575,34 @@ def run_c4(args):
 
 
 def run_e2e(args, ctx, s, dev, stream, head):
-    """Same solve through the public API with host inputs: H2D of the matrix,
-    right-hand side and contact pairs from pinned memory, the solve, D2H of x."""
+    """Same solve through the reference-facing host-buffer call
+    (sgmas_pcg_solve_host): H2D of the matrix and right-hand side from pinned
+    memory, the solve, D2H of x into pinned memory -- plus the H2D of the
+    contact pairs the MAS reads (sgmas_mas_set_contacts takes device pairs)."""
     import torch
     h = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
          for k, a in (("vals", s.vals), ("rows", s.rows), ("cols", s.cols), ("b", s.b), ("pairs", s.pairs))}
-    d = {k: torch.empty_like(t, device=dev) for k, t in h.items()}
+    hn = {k: t.numpy() for k, t in h.items()}  # the same pinned buffers, as host arrays
+    d_pairs = torch.empty_like(h["pairs"], device=dev)
     hx = torch.empty_like(h["b"]).pin_memory()
-    dx = torch.empty_like(d["b"])
-    ctx.mas_set_contacts(d["pairs"], len(s.pairs))
+    hxn = hx.numpy()
+    ctx.mas_set_contacts(d_pairs, len(s.pairs))
     precond = "jacobi" if head == "jacobi" else "mas"
     times = []
     for it in range(args.warmup + args.steps):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for k in d:
-            d[k].copy_(h[k], non_blocking=True)
-        ctx.pcg_solve(d["vals"], d["rows"], d["cols"], s.n_verts, d["b"], dx, rel_tol=REL_TOL, max_iter=MAX_ITER, preconditioner=precond)
-        hx.copy_(dx, non_blocking=True)
+        d_pairs.copy_(h["pairs"], non_blocking=True)
+        ctx.pcg_solve_host(hn["vals"], hn["rows"], hn["cols"], s.n_verts, hn["b"], out=hxn, rel_tol=REL_TOL,
+                           max_iter=MAX_ITER, preconditioner=precond)
         e1.record(stream)
         e1.synchronize()
         if it >= args.warmup:
             times.append(e0.elapsed_time(e1))
     h2d = sum(t.numel() * t.element_size() for t in h.values())
     return {"value": round(statistics.mean(times), 4), "unit": "ms", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(hx.numel() * hx.element_size())}
+            "d2h_bytes_per_step": int(hx.numel() * hx.element_size()), "api": "sgmas_pcg_solve_host"}
 
 
 def cpu_baseline(s, results):

@@ -366,9 +366,16 @@ class Context:
         self._check(self.L.sgmas_pcg_solve(self.h, C.byref(A), _ptr(b), _ptr(x), C.byref(c), C.byref(rep)))
         return {k: getattr(rep, k) for k, _ in PcgReport._fields_}
 
-    def pcg_solve_host(self, vals, rows, cols, n_block_rows, b, x0=None, **cfg):
+    def pcg_solve_host(self, vals, rows, cols, n_block_rows, b, x0=None, out=None, **cfg):
+        """Host arrays in, x out (sgmas_pcg_solve_host).  out: a host float64
+        array for x (e.g. pinned memory); x0: a start guess (copied into x)."""
         vals, rows, cols, b = _h(vals, np.float64), _h(rows, np.int32), _h(cols, np.int32), _h(b, np.float64)
-        x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64, copy=True)
+        if out is not None:
+            x = out
+            if x0 is not None:
+                x[...] = np.asarray(x0, np.float64)
+        else:
+            x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64, copy=True)
         if x0 is not None:
             cfg["initial_guess"] = True
         c = pcg_config(**cfg)
