@@ -38,6 +38,7 @@ METRIC = "MAS-PCG solve ms to 1e-4 rel. residual: learned/mixed vs plain, same B
 WORKLOAD = "two 40x20x20-vertex tet blocks 1e-4 m apart + 50k point-triangle barrier pairs (32,000 verts, 96,000 DOF)"
 REL_TOL = 1e-4
 MAX_ITER = 5000  # cap (the reference default is the DOF count); a variant that hits it reports converged=false
+TIGHT_TOL = 1e-10  # the untimed tight solve per variant whose distance to the direct solution is reported
 L2_FLUSH_BYTES = 512 << 20
 
 
@@ -49,6 +50,8 @@ def parse():
     ap.add_argument("--impl", default="sgmas", choices=["sgmas", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = benchmark size)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-direct", action="store_true",
+                    help="skip the FP64 direct solve (the per-variant solution errors)")
     ap.add_argument("--no-other", action="store_true", help="skip the brief config 1 / config 3 lines")
     ap.add_argument("--c4-scale", type=float, default=None, help="config-4 scene scale (default 1.0 for --workload c4)")
     ap.add_argument("--c4-train", type=int, default=None, help="config-4 training sequences (20 steps each)")
@@ -186,6 +189,41 @@ class Clocks:
                 "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
+class DirectSolve:
+    """FP64 direct solve of the benchmark system (sgmas.synth.direct_solve:
+    banded Cholesky in reverse Cuthill-McKee order), run in a child process
+    (spawned, not forked) while the GPU variants are timed; the per-variant
+    solution errors ||x - x*|| / ||x*|| are taken against it."""
+
+    def __init__(self, scale, seed):
+        self.path = tempfile.mktemp(suffix=".npy")
+        code = ("import sys, time, numpy as np; sys.path[:0] = [%r, %r]; from sgmas import synth; "
+                "t = time.time(); s = synth.config2(seed=%d, scale=%r); x = synth.direct_solve(s); "
+                "np.save(%r, x); print(round(time.time() - t, 1))"
+                % (ROOT, os.path.join(ROOT, "stiff-gipc_b200"), seed, scale, self.path))
+        self.t0 = time.time()
+        self.p = subprocess.Popen([sys.executable, "-c", code], stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                  text=True)
+        self.x = None
+        self.err = None
+        self.secs = None
+
+    def result(self):
+        out, err = self.p.communicate()
+        if self.p.returncode == 0 and os.path.exists(self.path):
+            self.x = np.load(self.path)
+            os.unlink(self.path)
+            self.secs = float(out.strip().splitlines()[-1]) if out.strip() else None
+        else:
+            self.err = (err or "").strip().splitlines()[-1:] or ["failed"]
+        return self.x
+
+    def info(self):
+        return {"method": "FP64 banded Cholesky (LAPACK dpbtrf) in reverse Cuthill-McKee order + one refinement "
+                          "step, scipy; child process beside the GPU legs", "seconds": self.secs,
+                "error": self.err}
+
+
 def build_problem(scale, seed=0):
     from sgmas import synth
     return synth.config2(seed=seed, scale=scale)
@@ -230,6 +268,7 @@ def run_sgmas(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
+    direct = DirectSolve(args.scale, rank) if rank == 0 and not args.no_direct else None
     t0 = time.time()
     s = build_problem(args.scale, seed=rank)
     gen_s = time.time() - t0
@@ -255,6 +294,7 @@ def run_sgmas(args):
 
     variants = [v for v in args.variants.split(",") if v]
     results = {}
+    sols = {}
     A_full = None
     clocks = Clocks(local)
     gpu_launches = None
@@ -298,6 +338,12 @@ def run_sgmas(args):
         ms = statistics.mean(times)
         if world > 1:
             ms = max_over_ranks(ms, dev)
+        # one tight solve (1e-10, untimed) of the same variant: its distance to the
+        # direct solution, beside that of the timed 1e-4 solution
+        xt = torch.zeros_like(b)
+        rt = ctx.pcg_solve(vals, rows, cols, s.n_verts, b, xt, rel_tol=TIGHT_TOL, max_iter=4 * MAX_ITER,
+                           preconditioner=precond)
+        sols[v] = (x.cpu().numpy(), xt.cpu().numpy(), int(rt["iterations"]), bool(rt["converged"]))
         results[v] = {"ms": ms, "ms_min": min(times), "ms_max": max(times), "iterations": int(statistics.median(iters)),
                       "rel_residual": res, "converged": bool(rep["converged"]),
                       "precond_build_ms": rep["precond_ms"], "pcg_loop_ms": rep["solve_ms"], "mode": mode,
@@ -355,10 +401,24 @@ def run_sgmas(args):
         traffic = tj.get(f"{dom}_{precision}")
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": f"{peak_kind} HBM copy",
+                "frac": round(achieved / hbm, 4), "traffic": traffic,
+                "traffic_source": ("stored, not measured in this run: ncu DRAM bytes (read + write) per "
+                                   "iteration of the same kernel on the same workload (profiles/traffic.json) "
+                                   "x this run's iterations"),
+                "peak_kind": f"{peak_kind} HBM copy",
                 "algorithmic_bytes": int(dom_bytes), "kernel_ms": dom_ms, "phase_ms": kms,
                 "phase_bytes": abytes, "graph_kernel_ms": gkms,
                 "note": "per-iteration working set < 126 MB L2: achieved can exceed the HBM copy peak"}
+    if direct is not None:
+        xs = direct.result()
+        for v, (x4, xt, it_t, conv_t) in sols.items():
+            if xs is None:
+                break
+            nx = float(np.linalg.norm(xs))
+            results[v]["x_err_vs_direct"] = float(np.linalg.norm(x4 - xs) / nx)
+            results[v]["tight"] = {"rel_tol": TIGHT_TOL, "iterations": it_t, "converged": conv_t,
+                                   "x_err_vs_direct": float(np.linalg.norm(xt - xs) / nx)}
+    ref_storage = results.get("fp32", {})
     out = {"metric": METRIC, "value": round(results[head]["ms"], 4), "unit": "ms", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(results[head]["ms"], 4),
            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -371,6 +431,12 @@ def run_sgmas(args):
            "variants": results,
            "speedup_vs_plain_fp64": (round(results["fp64"]["ms"] / results[head]["ms"], 3)
                                      if "ms" in results.get("fp64", {}) else None),
+           "reference_storage_fp32": ({"ms": round(ref_storage["ms"], 4), "iterations": ref_storage["iterations"],
+                                       "x_err_vs_direct": ref_storage.get("x_err_vs_direct"),
+                                       "note": "FP32 explicit subdomain inverses and FP32 apply, the "
+                                               "reference's own MAS storage"} if "ms" in ref_storage else None),
+           "x_err_vs_direct": results[head].get("x_err_vs_direct"),
+           "direct_solve": None if direct is None else direct.info(),
            "e2e": e2e, "gpu_launches": gpu_launches, "roofline": roofline, "clocks": clocks_rec}
     if not args.no_other:
         out["other_configs"] = other_configs(args, dev, stream)
@@ -606,11 +672,19 @@ def run_e2e(args, ctx, s, dev, stream, head):
 
 
 def cpu_baseline(s, results):
-    """The oracle port of the reference's MAS-PCG (FP64 CG, FP32 MAS, the
-    reference stopping rule) on this host's cores: one full solve of the same
-    system (preconditioner build + PCG)."""
+    """The reference's CPU path on this host's cores: the block-Jacobi CG
+    (PCGSolver::pcg, pcg_solver.cu:171-304, with DiagPreconditioner's 3x3
+    block-Jacobi, diag_preconditioner.cu:9-66: the preconditioner the
+    reference runs without MAS, and the "block-Jacobi CG" its solve is judged
+    against), the oracle port with OpenMP over all host threads: one full solve
+    of the same system to 1e-4 (D^-1 build + PCG).  Beside it, the port of the
+    reference's MAS-PCG (FP64 CG, FP32 MAS) on the same cores."""
     from oracle import oracle as O
     nthreads = O.lib().or_omp_max_threads()
+    t0 = time.perf_counter()
+    xj, repj = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=1, rel_tol=REL_TOL, nthreads=nthreads,
+                     max_iter=MAX_ITER)
+    tj = time.perf_counter() - t0
     pm, rm = O.morton_partition(s.pos)
     st, nn, nl = O.vert_neighbors(s.tets, s.n_verts)
     t0 = time.perf_counter()
@@ -618,51 +692,60 @@ def cpu_baseline(s, results):
     m.reorder(s.pairs)
     m.assemble(s.vals, s.rows, s.cols, precision=0)
     t1 = time.perf_counter()
-    x, rep = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=2, rel_tol=REL_TOL, mas=m, nthreads=nthreads, max_iter=MAX_ITER)
+    x, rep = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=2, rel_tol=REL_TOL, mas=m, nthreads=nthreads,
+                   max_iter=MAX_ITER)
     t2 = time.perf_counter()
-    tj = time.perf_counter()
-    xj, repj = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=1, rel_tol=REL_TOL, nthreads=nthreads, max_iter=MAX_ITER)
-    tj = time.perf_counter() - tj
-    return {"value": round((t2 - t0) * 1e3, 1), "unit": "ms", "cores": nthreads, "kind": "port",
-            "sample": "one full solve of the benchmark system: MAS build + FP64 PCG with FP32 MAS to 1e-4",
-            "iterations": rep["iterations"], "rel_residual": rep["rel_residual"],
-            "build_ms": round((t1 - t0) * 1e3, 1),
-            "jacobi_pcg": {"ms": round(tj * 1e3, 1), "iterations": repj["iterations"]}}
+    return {"value": round(tj * 1e3, 1), "unit": "ms", "cores": nthreads, "kind": "port",
+            "sample": "one full solve of the benchmark system: 3x3 block-Jacobi CG (FP64) to 1e-4, OpenMP",
+            "iterations": repj["iterations"], "rel_residual": repj["rel_residual"],
+            "mas_pcg_port": {"ms": round((t2 - t0) * 1e3, 1), "iterations": rep["iterations"],
+                             "build_ms": round((t1 - t0) * 1e3, 1), "rel_residual": rep["rel_residual"],
+                             "sample": "one full solve: MAS build + FP64 PCG with FP32 MAS to 1e-4, OpenMP"}}
 
 
 def run_reference(args):
-    """--impl reference: the reference's own algorithm on the host cores (the
-    reference cannot be built here -- its device code needs Eigen -- so this
-    is the oracle port of PCGSolver::pcg + MASPreconditioner, OpenMP)."""
+    """--impl reference: the reference's CPU path for this solve on the host
+    cores -- the block-Jacobi CG (PCGSolver::pcg + DiagPreconditioner, the
+    oracle port, OpenMP over all host threads; the reference's own code is
+    CUDA with Eigen in device code and cannot be built here).  Each step is
+    one full solve of the benchmark system to 1e-4 (D^-1 build + PCG).  One
+    MAS-PCG port solve is timed once beside it (mas_pcg_port)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     from oracle import oracle as O
     s = build_problem(args.scale, seed=0)
     nthreads = O.lib().or_omp_max_threads()
-    pm, rm = O.morton_partition(s.pos)
-    st, nn, nl = O.vert_neighbors(s.tets, s.n_verts)
     times, iters = [], []
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        m = O.MAS(s.n_verts, st, nn, nl, pm, rm)
-        m.reorder(s.pairs)
-        m.assemble(s.vals, s.rows, s.cols, precision=0)
-        x, rep = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=2, rel_tol=REL_TOL, mas=m, nthreads=nthreads, max_iter=MAX_ITER)
+        x, rep = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=1, rel_tol=REL_TOL, nthreads=nthreads,
+                       max_iter=MAX_ITER)
         dt = (time.perf_counter() - t0) * 1e3
         if it >= args.warmup:
             times.append(dt)
             iters.append(rep["iterations"])
     ms = statistics.mean(times)
-    sample = "full solves of the benchmark system (MAS build + FP64 PCG with FP32 MAS to 1e-4), OpenMP"
+    pm, rm = O.morton_partition(s.pos)
+    st, nn, nl = O.vert_neighbors(s.tets, s.n_verts)
+    t0 = time.perf_counter()
+    m = O.MAS(s.n_verts, st, nn, nl, pm, rm)
+    m.reorder(s.pairs)
+    m.assemble(s.vals, s.rows, s.cols, precision=0)
+    _, rm_rep = O.pcg(s.vals, s.rows, s.cols, s.n_verts, s.b, precond=2, rel_tol=REL_TOL, mas=m, nthreads=nthreads,
+                      max_iter=MAX_ITER)
+    mas_ms = (time.perf_counter() - t0) * 1e3
+    sample = "full solves of the benchmark system: 3x3 block-Jacobi CG (FP64) to 1e-4, OpenMP"
     print(json.dumps({"impl": "reference", "metric": METRIC, "value": round(ms, 2), "unit": "ms", "n_gpus": world,
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2),
-                      "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+                      "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                       "data": "synthetic",
                       "config": {"workload": WORKLOAD, "scale": args.scale, "rel_tol": REL_TOL},
                       "iterations": int(statistics.median(iters)),
                       "cpu_baseline": {"value": round(ms, 2), "unit": "ms", "cores": nthreads, "kind": "port",
                                        "sample": sample},
+                      "mas_pcg_port": {"ms": round(mas_ms, 2), "iterations": rm_rep["iterations"],
+                                       "sample": "one solve: MAS build + FP64 PCG with FP32 MAS to 1e-4, OpenMP"},
                       "e2e": {"value": round(ms, 2), "unit": "ms", "h2d_bytes_per_step": 0,
                               "d2h_bytes_per_step": 0}}))
 

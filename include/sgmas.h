@@ -179,6 +179,16 @@ int sgmas_set_pcg_mode(sgmas_context* ctx, int mode);
  * cooperative launches of such solves run side by side.  A system needing
  * more than 32 level-0 subdomains per CTA falls back to the graph form. */
 int sgmas_set_pcg_ctas(sgmas_context* ctx, int max_ctas);
+/* Bound on each device-side wait of the persistent form (the grid barriers
+ * between its phases and the waits for its bulk tile copies): at most
+ * spin_limit polls (0 = the default, 4,194,304), after which the kernel sets
+ * its error flag, leaves the loop and returns; sgmas_pcg_solve then reports
+ * SGMAS_ERR_DEVICE ("bounded wait expired") and the context stays usable.
+ * phantom_arrivals > 0 is fault injection for tests: every grid barrier then
+ * waits for that many arrivals beyond the grid's CTAs, which never come, so
+ * the first wait runs out (0 = normal operation).  No reference counterpart:
+ * the reference's loop is host-driven and has no device-side waits. */
+int sgmas_set_wait_limit(sgmas_context* ctx, int spin_limit, int phantom_arrivals);
 /* Autotuner of the loop's launch shape: the persistent form on candidate grid
  * sizes (from the fewest CTAs the system fits on up to every SM, about x1.4
  * apart; tried from the largest down, until one does not fit) and the
@@ -296,17 +306,22 @@ int sgmas_write_upper_blocks(sgmas_context* ctx, const double* d_H, int n_elem, 
 int sgmas_morton_codes(sgmas_context* ctx, const double* d_pos, int n, const double* aabb,
                        uint64_t* d_codes);
 /* Morton codes exactly as sgmas_morton_codes, for callers that cannot
- * allocate device memory: code running during CUDA graph capture, or hosts
- * whose device memory comes from their own pool.  No reference counterpart:
- * this entry point exists only in this library.  It needs no context and
- * calls no allocating routine; the bounding-box reduction uses a fixed
- * 49,216-byte static device array that every GPU loading the library holds
- * until exit.  n must not exceed SGMAS_MORTON_NOALLOC_MAX_VERTS
- * (SGMAS_ERR_CAPACITY otherwise, before any work is queued).  Runs on the
- * current device and `stream` (NULL = legacy default stream).  The first
- * call on a device looks the array up (cudaGetSymbolAddress): make that first
- * call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race, so order them (same stream or synchronised). */
+ * allocate device memory: hosts whose device memory comes from their own pool
+ * or is fixed at start-up, and loops that must not allocate once they run.
+ * No reference counterpart: this entry point exists only in this library.
+ * It needs no context and calls no allocating routine; the bounding-box
+ * reduction uses a fixed 49,216-byte static device array that every GPU
+ * loading the library holds until exit.  n must not exceed
+ * SGMAS_MORTON_NOALLOC_MAX_VERTS (SGMAS_ERR_CAPACITY otherwise, before any
+ * work is queued).  Runs on the current device and `stream` (NULL = legacy
+ * default stream).  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and loads the kernels: make that first call before
+ * any stream capture.  The address is kept for the life of the process, so
+ * the device's primary context must not be reset while the library is loaded.
+ * An error already pending in the CUDA runtime when the call begins is
+ * returned as SGMAS_ERR_CUDA and left pending, with no work queued.  All
+ * calls share the array: calls that overlap on the GPU race, so order them
+ * (same stream or synchronised). */
 #define SGMAS_MORTON_NOALLOC_MAX_VERTS 2097152
 int sgmas_morton_codes_noalloc(const double* d_pos, int n, const double* aabb, uint64_t* d_codes,
                                void* stream);

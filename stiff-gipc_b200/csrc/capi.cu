@@ -401,7 +401,20 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
         report->rr_x0 = rc_cfg.warm ? h.w_rr : 0.0;
         report->bb = rc_cfg.warm ? h.w_bb : h.rr0;
     }
+    if (h.breakdown)
+        return ctx_fail(c, SGMAS_ERR_NUMERIC,
+                        "CG breakdown at iteration %d: p.A p <= 0 with r != 0 (the matrix or the preconditioner "
+                        "is not positive definite)", h.iters);
     if (!(h.rz == h.rz) || !(h.rr == h.rr)) return ctx_fail(c, SGMAS_ERR_NUMERIC, "non-finite residual in PCG");
+    return SGMAS_OK;
+}
+
+int sgmas_set_wait_limit(sgmas_context* c, int spin_limit, int phantom_arrivals) {
+    if (!c) return SGMAS_ERR_ARG;
+    if (spin_limit < 0 || phantom_arrivals < 0)
+        return ctx_fail(c, SGMAS_ERR_ARG, "sgmas_set_wait_limit: spin_limit and phantom_arrivals must be >= 0");
+    c->wait_limit = spin_limit > 0 ? spin_limit : kSpinLimit;
+    c->phantom_arrivals = phantom_arrivals;
     return SGMAS_OK;
 }
 

@@ -7,7 +7,7 @@
 namespace sgmas {
 
 constexpr int kMaxLevels = 6;          // levelnum cap (SG/MASPreconditioner.cu:1735-1736)
-constexpr int kSpinLimit = 1 << 22;    // bound on every device-side wait
+constexpr int kSpinLimit = 1 << 22;    // default bound on every device-side wait (polls)
 
 // device error flags (ctx->d_err[0]); kernels never trap
 enum DeviceError : int {
@@ -47,10 +47,11 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
-// bounded wait on phase `parity`; returns false (and flags) if it gave up
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err) {
+// bounded wait on phase `parity` (at most `limit` polls); returns false (and
+// flags) if it gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err, int limit = kSpinLimit) {
     uint32_t addr = smem_u32(bar);
-    for (int it = 0; it < kSpinLimit; ++it) {
+    for (int it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

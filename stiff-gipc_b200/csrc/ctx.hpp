@@ -17,6 +17,7 @@ struct PcgState {
     // start guess (initial_guess = 1): x0.b, b.b, scale, ||b - alpha A x0||^2
     double w_xb, w_bb, w_alpha, w_rr;
     int warm, w_reject;
+    int breakdown;  // p.Ap <= 0 with r != 0: A (or the preconditioner) is not SPD
 };
 
 // Rows of a solve outside the MAS range (the reference's hybrid scenes:
@@ -121,6 +122,8 @@ struct sgmas_context {
     unsigned* d_coarse_ticket = nullptr;  // last-CTA ticket of the coarse MAS kernel
     unsigned* d_psync = nullptr;          // grid barrier + ticket of the persistent PCG kernel
     bool persistent = true;               // solve with the persistent kernel when the system fits
+    int wait_limit = sgmas::kSpinLimit;   // polls of each device-side wait of the persistent kernel
+    int phantom_arrivals = 0;             // fault injection: arrivals each grid barrier waits for beyond the grid
     int pcg_ctas = 0;                     // CTAs of the persistent kernel (0: one per SM)
     bool last_persistent = false;         // the last solve ran the persistent kernel
     PcgRunCfg last_run = {};

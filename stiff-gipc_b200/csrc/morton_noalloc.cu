@@ -3,10 +3,10 @@
 //
 // sgmas_morton_codes needs a context (whose creation allocates) and a scratch
 // buffer for the bounding-box reduction (allocated on first use).  Some
-// callers cannot do either: code that runs while a CUDA graph is being
-// captured (cudaMalloc is not allowed there), or a host application whose
-// device memory is handed out by its own pool and must not grow behind its
-// back.  For them this file offers sgmas_morton_codes_noalloc: the same codes
+// callers cannot do either: a host application whose device memory is handed
+// out by its own pool or fixed at start-up, which must not grow behind its
+// back, or a simulation loop that has a rule against allocating once it runs.
+// For them this file offers sgmas_morton_codes_noalloc: the same codes
 // (hash_code type -1 of SG/GIPC.cu:142-168, packed as in _calcVertMChash
 // SG/GIPC.cu:412-461), with the reduction scratch in a fixed static device
 // array instead of an allocation.
@@ -17,6 +17,11 @@
 // library holds the 49,216-byte array until the process exits.  All calls
 // share it: two calls whose kernels overlap on the GPU race on it, so calls
 // must be ordered (same stream, or synchronised).
+//
+// The first call on a device looks the array's device address up and loads
+// both kernels; the address is kept per device for the life of the process,
+// which assumes the device's primary context (the runtime's) is never reset
+// (cudaDeviceReset) while the library is loaded.
 #include <mutex>
 
 #include "../../include/sgmas.h"
@@ -121,7 +126,9 @@ __global__ void k_codes(int n, const double* __restrict__ pos, const double* __r
     codes[i] = (mc << 32) | (uint64_t)(uint32_t)i;
 }
 
-// Look the scratch array up on the current device (first call per device).
+// Look the scratch array up on the current device (first call per device)
+// and load both kernels there, so that no later call is the first to touch
+// them (under lazy module loading a kernel loads on its first use).
 int scratch_for_current_device(double** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SGMAS_ERR_CUDA;
@@ -129,6 +136,9 @@ int scratch_for_current_device(double** out) {
     if (!g_scratch_ptr[dev]) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return SGMAS_ERR_CUDA;
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, k_box_tiles) != cudaSuccess) return SGMAS_ERR_CUDA;
+        if (cudaFuncGetAttributes(&fa, k_codes) != cudaSuccess) return SGMAS_ERR_CUDA;
         g_scratch_ptr[dev] = static_cast<double*>(p);
     }
     *out = g_scratch_ptr[dev];
@@ -142,6 +152,9 @@ extern "C" int sgmas_morton_codes_noalloc(const double* d_pos, int n, const doub
     if (n < 0 || (n > 0 && (!d_pos || !d_codes))) return SGMAS_ERR_ARG;
     if (n > SGMAS_MORTON_NOALLOC_MAX_VERTS) return SGMAS_ERR_CAPACITY;
     if (n == 0) return SGMAS_OK;
+    // an error left pending by the caller's own earlier work is theirs: report it
+    // without clearing it, and queue nothing
+    if (cudaPeekAtLastError() != cudaSuccess) return SGMAS_ERR_CUDA;
     double* scratch = nullptr;
     const int rc = scratch_for_current_device(&scratch);
     if (rc != SGMAS_OK) return rc;
@@ -150,6 +163,7 @@ extern "C" int sgmas_morton_codes_noalloc(const double* d_pos, int n, const doub
         // the ticket must start at zero (a failed earlier call may have left it set)
         if (cudaMemsetAsync(scratch + kTicketOff, 0, sizeof(unsigned), s) != cudaSuccess) return SGMAS_ERR_CUDA;
         k_box_tiles<<<(n + kTile - 1) / kTile, kThreads, 0, s>>>(n, d_pos, scratch);
+        if (cudaGetLastError() != cudaSuccess) return SGMAS_ERR_CUDA;
     }
     const double z = 0.0;
     k_codes<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(

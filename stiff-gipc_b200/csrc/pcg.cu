@@ -291,7 +291,17 @@ __global__ void __launch_bounds__(kT) k_bsr_spmv(BsrView A, const double* __rest
     double total;
     if (grid_sum_last<kT>(block_sum<kT>(dot, sh), partials, ticket, sh, &total)) {
         st->pAp = total;
-        st->alpha = st->rz / total;
+        if (!(total > 0.0)) {  // stop: finite p.Ap <= 0 is a CG breakdown (r = 0 exactly is a solution),
+                               // NaN is reported as a non-finite residual
+            const bool finite = total == total && st->rz == st->rz;
+            st->breakdown = finite && st->rz != 0.0;
+            st->converged = finite && st->rz == 0.0;
+            st->iters = st->k;
+            st->done = 1;
+            st->alpha = 0.0;
+        } else {
+            st->alpha = st->rz / total;
+        }
     }
 }
 

@@ -76,6 +76,8 @@ struct PArgs {
     double rel2, abs2;
     double* partials;  // [4][grid]
     unsigned* sync;    // [0] barrier arrivals (monotonic)
+    int spin_limit;    // polls of each grid barrier / mbarrier wait before it gives up
+    int phantom;       // arrivals each grid barrier expects beyond the grid (fault injection; 0 normally)
     PcgState* st;
     int* err;
     // optional phase stamps (clock64 of CTA 0): [0] start, [1] end, [2] loop
@@ -96,20 +98,22 @@ __device__ __forceinline__ void stamp(const PArgs& a, int k, int slot) {
 
 // ---- grid barrier: monotonic arrival counter, release add / acquire poll ---
 // Barrier number `epoch` (1, 2, ...) completes when the counter reaches
-// epoch * gridDim.x.  Bounded spin; a timeout sets the error flag.
+// epoch * (gridDim.x + phantom).  At most `limit` polls; a timeout sets the
+// error flag.  (phantom > 0 makes every barrier wait for arrivals that never
+// come: the host's fault injection for the timeout path.)
 // acc (thread 0 of each CTA, profiling only): += work and wait cycles of this
 // barrier slot; t_rel carries the previous release time.
-__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned& epoch, int* err,
+__device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned& epoch, int* err, int limit, int phantom,
                                              unsigned long long* acc = nullptr, long long* t_rel = nullptr) {
     __shared__ int ok_sh;
     __syncthreads();
     if (threadIdx.x == 0) {
         const long long t_arrive = acc ? clock64() : 0;
         epoch += 1u;
-        const unsigned target = epoch * gridDim.x;
+        const unsigned target = epoch * (gridDim.x + (unsigned)phantom);
         asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
         int ok = 0;
-        for (int it = 0; it < kSpinLimit; ++it) {
+        for (int it = 0; it < limit; ++it) {
             unsigned v;
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
             if ((int)(v - target) >= 0) { ok = 1; break; }
@@ -337,7 +341,7 @@ __device__ __forceinline__ bool levels_c(const PArgs& a, const Anc& anc, S* tile
                     mbar_expect_tx(mbar, bytes);
                     bulk_g2s(tilesC, (const S*)a.inv + (size_t)(anc.lo[l] + c0) * bs * 9, bytes, mbar);
                 }
-                if (!mbar_wait(mbar, mphase, a.err)) return false;
+                if (!mbar_wait(mbar, mphase, a.err, a.spin_limit)) return false;
                 mphase ^= 1u;
                 const int off = (anc.lo[l] + c0 - bbase) * B;
                 smem_banks<B, S, Acc>(tilesC, Rc + 3 * (size_t)off, Zc + 3 * (size_t)off, ncb, xch);
@@ -468,7 +472,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             const int i1 = (o.j0 + hw1) * B + lane;
             if (i1 < a.lvl_count[1]) par1 = a.going_next[a.lvl_begin[1] + i1] - a.lvl_begin[2];
         }
-        ok = mbar_wait(&mbar, mphase, a.err);
+        ok = mbar_wait(&mbar, mphase, a.err, a.spin_limit);
         mphase ^= 1u;
     }
     const bool act0 = (hw / HPW) * HPW < o.nbk0;  // this warp has level-0 work
@@ -588,7 +592,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         xb = block_sum<kPT>(xb, sh);
         bb = block_sum<kPT>(bb, sh);
         if (threadIdx.x == 0) { part_pap[blockIdx.x] = xax; part_rz[blockIdx.x] = xb; part_rr[blockIdx.x] = bb; }
-        ok = ok && grid_barrier(a.sync, epoch, a.err);
+        ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
         if (ok) {
             xax = sum_partials(part_pap, sh);
             sum_partials2(part_rz, part_rr, sh, xb, bb);
@@ -604,7 +608,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             rr = block_sum<kPT>(rr, sh);
             if (threadIdx.x == 0) part_w[blockIdx.x] = rr;
         }
-        ok = ok && grid_barrier(a.sync, epoch, a.err);
+        ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
         if (ok) {
             w_rr = sum_partials(part_w, sh);
             const int w_rej = !(w_rr <= w_bb) || w_alpha == 0.0;
@@ -616,7 +620,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                     a.r[i] = a.b[i];
                     a.x[i] = 0.0;
                 }
-                ok = grid_barrier(a.sync, epoch, a.err);
+                ok = grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
             }
         }
     }
@@ -628,21 +632,21 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         }
         if (ok) apply_b();
         if (a.L > 2) {
-            ok = ok && grid_barrier(a.sync, epoch, a.err);
+            ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
             if (ok) ok = levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch);
         }
         if (ok) collect(0, 0.0, a.p1);
     } else {
-        ok = ok && grid_barrier(a.sync, epoch, a.err);
+        ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
         if (ok) phase_jacobi(a, 0, 0.0, a.p1, part_rz, part_rr, sh);
     }
-    ok = ok && grid_barrier(a.sync, epoch, a.err);
+    ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
     double rz = ok ? sum_partials(part_rz, sh) : 0.0;
     const double rz0 = rz;
     const double rr0_r = ok ? sum_partials(part_rr, sh) : 0.0;
     const double rr0 = a.warm ? w_bb : rr0_r;  // a start guess: convergence relative to ||b||
     double rr_last = rr0_r, beta = 0.0;
-    int k = 1, iters = 1, converged = 0;
+    int k = 1, iters = 1, converged = 0, breakdown = 0;
     bool done = !ok || a.max_iter <= 1;
     double* pold = a.p0;
     double* pnew = a.p1;
@@ -666,7 +670,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         }
         dot = block_sum<kPT>(dot, sh);
         if (threadIdx.x == 0) part_pap[blockIdx.x] = dot;
-        if (!grid_barrier(a.sync, epoch, a.err, SLOT(0))) { ok = false; break; }
+        if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(0))) { ok = false; break; }
         stamp(a, k, 1);
         const bool refresh = k % 10 == 0;  // true residual (pcg_solver.cu:240-244)
         // B: the slot's p and Ap are loaded before the partials are summed
@@ -675,7 +679,16 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             if (own) { p0v = pnew[vo]; p1v = pnew[vo + 1]; p2v = pnew[vo + 2]; }
             if (!refresh) { q0 = a.Ap[vo]; q1 = a.Ap[vo + 1]; q2 = a.Ap[vo + 2]; }
         }
-        const double alpha = rz / sum_partials(part_pap, sh);
+        const double pap = sum_partials(part_pap, sh);
+        if (!(pap > 0.0)) {  // same value in every CTA: all stop here
+            // finite p.Ap <= 0: CG breakdown (r = 0 exactly is a solution); NaN: reported as non-finite
+            const bool finite = pap == pap && rz == rz;
+            breakdown = finite && rz != 0.0;
+            converged = finite && rz == 0.0;
+            iters = k;
+            break;
+        }
+        const double alpha = rz / pap;
         if (refresh) {
             if (mas) {
                 if (own) {
@@ -692,13 +705,13 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                 for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT)
                     a.x[i] = a.x[i] + alpha * pnew[i];
             }
-            if (!grid_barrier(a.sync, epoch, a.err, SLOT(1))) { ok = false; break; }
+            if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(1))) { ok = false; break; }
             const int4* ud = udesc + (threadIdx.x / 32) * a.upw * kRowGroups + (threadIdx.x & 31) / kRowLanes;
             for (int u = gw0, i = 0; u < a.units; u += gridDim.x * warps, ++i) {
                 const int4 d = i < a.upw ? ud[kRowGroups * i] : unit_desc(a.A, u, threadIdx.x & 31);
                 spmv_unit_d<2, true>(a.A, d, threadIdx.x & 31, a.x, nullptr, nullptr, a.r, a.b, 1.0, 0.0, 0.0);
             }
-            if (!grid_barrier(a.sync, epoch, a.err, SLOT(2))) { ok = false; break; }
+            if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(2))) { ok = false; break; }
             if (mas && v >= 0) { r0 = a.r[vo]; r1 = a.r[vo + 1]; r2 = a.r[vo + 2]; }
         } else if (mas && v >= 0) {
             r0 = r0 - alpha * q0; r1 = r1 - alpha * q1; r2 = r2 - alpha * q2;
@@ -708,7 +721,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         if (mas) {
             apply_b();
             if (a.L > 2) {
-                if (!grid_barrier(a.sync, epoch, a.err, SLOT(3))) { ok = false; break; }
+                if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(3))) { ok = false; break; }
                 stamp(a, k, 3);
                 if (!levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch)) ok = false;
             }
@@ -716,7 +729,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         } else {
             phase_jacobi(a, refresh ? 0 : 1, alpha, pnew, part_rz, part_rr, sh);
         }
-        if (!grid_barrier(a.sync, epoch, a.err, SLOT(5)) || !ok) { ok = false; break; }
+        if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(5)) || !ok) { ok = false; break; }
         stamp(a, k, 5);
         double rz_new, rr;
         sum_partials2(part_rz, part_rr, sh, rz_new, rr);
@@ -749,6 +762,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         PcgState s = {};
         s.rz = rz; s.rz0 = rz0; s.rr0 = rr0; s.rr = rr_last; s.k = k; s.iters = iters; s.done = 1;
         s.converged = converged;
+        s.breakdown = breakdown;
         s.max_iter = a.max_iter;
         s.check_every = a.check_every;
         s.warm = a.warm;
@@ -920,6 +934,8 @@ int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRu
         if (ctx_alloc(c, &c->d_psync, 8)) return SGMAS_ERR_CUDA;
     }
     a.sync = c->d_psync;
+    a.spin_limit = c->wait_limit;
+    a.phantom = c->phantom_arrivals;
     int dev_sms = 0;
     SG_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device));
     if (2 * c->partial_cap < 4 * dev_sms) {  // partials of p.Ap, r.z, r.r (+ start guess) per CTA (2 * partial_cap doubles)

@@ -67,7 +67,7 @@ EXPORTS = [
     "sgmas_pcg_solve", "sgmas_pcg_solve_host", "sgmas_spmv", "sgmas_convert", "sgmas_write_upper_blocks",
     "sgmas_morton_codes", "sgmas_morton_partition", "sgmas_pcg_profile", "sgmas_vert_neighbors",
     "sgmas_part_maps", "sgmas_morton_codes_noalloc", "sgmas_set_pcg_mode", "sgmas_pcg_last_vectors",
-    "sgmas_mtx_write", "sgmas_mtx_read", "sgmas_set_pcg_ctas", "sgmas_mlp_set_params", "sgmas_mlp_get_params", "sgmas_mlp_features",
+    "sgmas_mtx_write", "sgmas_mtx_read", "sgmas_set_pcg_ctas", "sgmas_set_wait_limit", "sgmas_mlp_set_params", "sgmas_mlp_get_params", "sgmas_mlp_features",
     "sgmas_mlp_gradient", "sgmas_mlp_train_step", "sgmas_mlp_forward", "sgmas_mlp_warm_start",
     "sgmas_autotune_pcg", "sgmas_assembly_plan", "sgmas_assemble", "sgmas_abd_body_blocks",
     "sgmas_abd_pair_blocks", "sgmas_abd_fem_blocks",
@@ -116,6 +116,7 @@ def lib(build_if_missing: bool = False):
     L.sgmas_morton_codes_noalloc.argtypes = [vp, i, vp, vp, vp]
     L.sgmas_set_pcg_mode.argtypes = [vp, i]
     L.sgmas_set_pcg_ctas.argtypes = [vp, i]
+    L.sgmas_set_wait_limit.argtypes = [vp, i, i]
     L.sgmas_autotune_pcg.argtypes = [vp, C.POINTER(Bcoo), vp, C.POINTER(PcgConfig), i, i, i, i, C.POINTER(TuneReport)]
     L.sgmas_pcg_last_vectors.argtypes = [vp, vp, vp]
     L.sgmas_assembly_plan.argtypes = [vp, vp, vp, i, vp, vp, C.POINTER(i)]
@@ -140,8 +141,9 @@ def lib(build_if_missing: bool = False):
 def morton_codes_noalloc(pos, codes, aabb=None, stream=None, n=None):
     """Morton codes without any device allocation (sgmas_morton_codes_noalloc).
 
-    For callers that may not allocate device memory (e.g. during CUDA graph
-    capture).  Runs on the current device; returns the C status code (0 = ok,
+    For callers that may not allocate device memory (a host whose device
+    memory comes from its own pool, a loop that must not allocate once it
+    runs).  Runs on the current device; returns the C status code (0 = ok,
     SGMAS_ERR_CAPACITY = -4 when n exceeds MORTON_NOALLOC_MAX_VERTS)."""
     box = None if aabb is None else _h(aabb, np.float64)
     count = int(pos.shape[0]) if n is None else n
@@ -274,6 +276,12 @@ class Context:
         """Cap the persistent kernel's CTAs (0 = one per SM): small systems on a
         few SMs leave the rest to concurrent solves on other streams."""
         self._check(self.L.sgmas_set_pcg_ctas(self.h, int(max_ctas)))
+
+    def set_wait_limit(self, spin_limit=0, phantom_arrivals=0):
+        """Polls per device-side wait of the persistent kernel (0 = default);
+        phantom_arrivals > 0 injects a grid barrier that never completes
+        (tests of the timeout path)."""
+        self._check(self.L.sgmas_set_wait_limit(self.h, int(spin_limit), int(phantom_arrivals)))
 
     def autotune(self, vals, rows, cols, n_block_rows, b, objective="throughput", concurrency=1, trial_iters=30,
                  reps=2, **cfg):
@@ -490,10 +498,10 @@ class Context:
         box = None if aabb is None else _h(aabb, np.float64)
         self._check(self.L.sgmas_morton_codes(self.h, _ptr(pos), int(pos.shape[0]), _ptr(box), _ptr(codes)))
 
-    def morton_partition(self, pos):
+    def morton_partition(self, pos, part_map_cap=None):
         n = int(pos.shape[0])
-        cap = (n + self.bank - 1) // self.bank * self.bank
-        pm = np.zeros(cap, np.int32)
+        cap = (n + self.bank - 1) // self.bank * self.bank if part_map_cap is None else int(part_map_cap)
+        pm = np.zeros(max(cap, 1), np.int32)
         rm = np.zeros(n, np.int32)
         size = C.c_int()
         self._check(self.L.sgmas_morton_partition(self.h, _ptr(pos), n, _ptr(pm), cap, C.byref(size), _ptr(rm)))

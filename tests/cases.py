@@ -59,3 +59,20 @@ def build(name, bank=16):
         raise KeyError(name)
     st, nn, nl = O.vert_neighbors(s.tets, s.n_verts)
     return Case(name, s, pm, rm, st, nn, nl)
+
+
+def oracle_iteration_band(s, precond, mas=None, rel_tol=1e-4, n_perturb=6, **kw):
+    """Iteration counts of the oracle port's PCG on b scaled by
+    (1 + k 2^-52), k = 0 .. n_perturb - 1, serial and on every host thread.
+    On ill-conditioned systems CG's count moves with the last bit of any sum;
+    this measured spread (not a guess) is the band a device solve must fall
+    in, widened by one check interval."""
+    its = []
+    nth = O.lib().or_omp_max_threads()
+    for k in range(n_perturb):
+        b = s.b * (1.0 + k * 2.0 ** -52)
+        for nt in ((1, nth) if k < 2 else (nth,)):
+            _, r = O.pcg(s.vals, s.rows, s.cols, s.n_verts, b, precond=precond, rel_tol=rel_tol, mas=mas,
+                         nthreads=nt, **kw)
+            its.append(r["iterations"])
+    return min(its), max(its)

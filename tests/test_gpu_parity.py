@@ -220,7 +220,8 @@ def direct_solve(s):
 # reference's FP32 MAS does not converge (oracle and device alike, see
 # test_fp32_mas_stalls_on_stiff_contact) so the plain FP64 MAS is used.
 SOLVES = [("c1", "jacobi", "fp32"), ("c1", "mas", "fp32"), ("bar", "jacobi", "fp32"), ("bar", "mas", "fp32"),
-          ("c2s", "jacobi", "fp32"), ("c2s", "mas", "fp64"), ("c1", "mas", "bf16"), ("c1", "mas", "fp64")]
+          ("c2s", "jacobi", "fp32"), ("c2s", "mas", "fp64"), ("c2s", "mas", "bf16"), ("c1", "mas", "bf16"),
+          ("c1", "mas", "fp64")]
 
 
 @pytest.mark.parametrize("mode", ["persistent", "graph"])
@@ -245,10 +246,15 @@ def test_pcg_matches_oracle(sgm, name, precond, precision, mode):
     assert res <= 1e-4 * 1.0001, res
     assert rep["iterations"] % 10 == 0
     # CG iteration counts on ill-conditioned systems move with the last bit of
-    # any sum (the oracle alone goes 950 -> 1180 on c2s for a 1e-15 change of
-    # b); well-conditioned cases must agree to one check interval.
-    tol_it = 10 if name != "c2s" else max(10, ro["iterations"] // 2)
-    assert abs(rep["iterations"] - ro["iterations"]) <= tol_it, (rep["iterations"], ro["iterations"])
+    # any sum; on the contact case (cond ~ 2e10) the device's count must lie in
+    # the spread the oracle itself shows when b moves in its last bit
+    # (measured here: about 20-30 iterations), widened by one check interval.
+    # Well-conditioned cases must agree with the oracle to one check interval.
+    if name == "c2s":
+        lo, hi = cases.oracle_iteration_band(s, 2 if precond == "mas" else 1, mas=mas)
+        assert lo - 10 <= rep["iterations"] <= hi + 10, (rep["iterations"], lo, hi)
+    else:
+        assert abs(rep["iterations"] - ro["iterations"]) <= 10, (rep["iterations"], ro["iterations"])
     xs = direct_solve(s)
     err_o = np.linalg.norm(xo - xs) / np.linalg.norm(xs)
     err_g = np.linalg.norm(xg - xs) / np.linalg.norm(xs)
@@ -371,6 +377,41 @@ def test_hybrid_mas_abd_solve(sgm, hybrid, mode, precision):
     assert rj["converged"] == 1 and rep["iterations"] < rj["iterations"]
     assert rj["kernel_launches"] == 1 if mode == "persistent" else rj["kernel_launches"] > 1
     ctx.close()
+
+
+def test_mas_assemble_with_indices(sgm, hybrid):
+    """The indices argument of sgmas_mas_assemble (setPreconditioner_bcoo's
+    `indices`, filled by calculate_subsystem_bcoo_indices,
+    i_preconditioner.cu:32-72, and passed by fem_mas_preconditioner.cu:24-30):
+    with the indices of every block inside the FEM range the assembled
+    subdomain matrices equal those of the range filter (indices = NULL); with
+    a subset they equal the oracle's assembly of the same subset."""
+    s, N, pm, rm, st, nn, nl = hybrid
+    off = s.info["fem_offset"]
+    vals, rows, cols = dev(s.vals), dev(s.rows), dev(s.cols)
+    in_fem = (s.rows >= off) & (s.rows < off + N) & (s.cols >= off) & (s.cols < off + N)
+    sel_all = np.flatnonzero(in_fem).astype(np.uint32)          # what the reference's select produces
+    rng = np.random.default_rng(11)
+    keep = in_fem & ((s.rows == s.cols) | (rng.random(len(s.rows)) < 0.6))
+    sel_sub = np.flatnonzero(keep).astype(np.uint32)
+    mats = {}
+    for name, idx in (("null", None), ("all", sel_all), ("sub", sel_sub)):
+        ctx = sgm.Context(0, bank=16, precision="fp32")
+        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        ctx.mas_init(N, st, nn, nl, pm, rm)
+        ctx.mas_assemble(vals, rows, cols, indices=None if idx is None else dev(idx), offset=off, cp_num=0)
+        torch.cuda.synchronize()
+        mats[name] = ctx.mas_matrices()[0]
+        ctx.close()
+    scale = np.abs(mats["null"]).max()
+    assert np.abs(mats["all"] - mats["null"]).max() <= 1e-12 * scale
+    m = O.MAS(N, st, nn, nl, pm, rm)
+    m.reorder(None)
+    m.assemble(s.vals, s.rows, s.cols, offset=off, indices=sel_sub, precision=0)
+    hess_o = m.matrices()[0]
+    assert np.abs(mats["sub"] - hess_o).max() <= 1e-12 * np.abs(hess_o).max()
+    # the subset really is a different matrix
+    assert np.abs(mats["sub"] - mats["null"]).max() > 1e-6 * scale
 
 
 def test_fp32_mas_stalls_on_stiff_contact(sgm):

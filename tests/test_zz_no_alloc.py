@@ -1,6 +1,6 @@
 """sgmas_morton_codes_noalloc: Morton codes for callers that cannot allocate
-device memory (code running during CUDA graph capture, or hosts that hand out
-device memory from their own pool).  The entry point keeps its reduction
+device memory (hosts that hand out device memory from their own pool or fix
+it at start-up, loops that must not allocate once they run).  The entry point keeps its reduction
 scratch in a fixed static device array, so it must give exactly the codes of
 the allocating entry point sgmas_morton_codes -- on consecutive calls that
 share that array -- and refuse inputs larger than the array can serve.
