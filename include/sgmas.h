@@ -132,8 +132,11 @@ int sgmas_mas_init(sgmas_context* ctx, int vert_num, int collision_node_offset,
 /* the int4 contact pairs the reference keeps as _collisonPairs (device, borrowed) */
 int sgmas_mas_set_contacts(sgmas_context* ctx, const int* d_pairs_int4, int cp_num);
 /* setPreconditioner_bcoo (:2169-2207): hierarchy rebuild + Hessian scatter +
- * dense subdomain inverses.  d_indices selects the FEM blocks (NULL = every
- * block whose row and column lie in [offset, offset + vert_num)). */
+ * dense subdomain inverses.  d_indices selects the FEM blocks: triplet_num
+ * block indices into d_values / d_rows / d_cols, each below the BCOO's block
+ * count (what calculate_subsystem_bcoo_indices, i_preconditioner.cu:32-72,
+ * returns with its count).  NULL = every one of the triplet_num blocks whose
+ * row and column lie in [offset, offset + vert_num). */
 int sgmas_mas_assemble(sgmas_context* ctx, const double* d_values, const int* d_rows,
                        const int* d_cols, const uint32_t* d_indices, int offset,
                        int triplet_num, int cp_num);

@@ -219,7 +219,8 @@ class MAS:
             self._idx = np.ascontiguousarray(indices, np.uint32)
             ip = self._idx.ctypes.data_as(C.c_void_p)
         self._vals = cf64(vals).reshape(-1)
-        rc = lib().or_mas_assemble(self.h, self._vals, c32(rows), c32(cols), ip, offset, len(rows), precision)
+        n = len(rows) if indices is None else len(self._idx)  # with indices: their count (as the reference's triplet_num)
+        rc = lib().or_mas_assemble(self.h, self._vals, c32(rows), c32(cols), ip, offset, n, precision)
         if rc != 0:
             raise ValueError("or_mas_assemble failed")
 

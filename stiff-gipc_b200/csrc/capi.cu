@@ -86,7 +86,8 @@ void free_all(sgmas_context* c) {
                     c->d_state, c->d_hvals, c->d_hb, c->d_hx, c->d_hrows, c->d_hcols, c->d_sort_scratch,
                     c->d_coarse_ticket, c->bsr.row_list, c->bsr.d_nlong, c->bsr.tcols, c->bsr.tsrc,
                     c->d_psync, c->d_stamps, c->d_l1_bank, c->d_own1, c->d_tune_x, c->bsr.udesc, c->d_plan_idx,
-                    c->d_plan_start};
+                    c->d_plan_start, c->d_row_order, c->d_cpre, c->d_udesc_c, c->d_lcols, c->d_halo,
+                    c->d_cinfo, c->d_plan_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

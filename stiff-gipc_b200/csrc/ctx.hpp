@@ -133,6 +133,17 @@ struct sgmas_context {
     int l1_bank_cap = 0;
     int* d_own1 = nullptr;                // first level-1 bank of each CTA of the persistent kernel
     int own1_cap = 0;
+    // SpMV plan of the persistent kernel (per solve): row order, cost prefixes, CTA work units,
+    // halo-local column indices, halo vertex lists, per-CTA info, largest halo / unit count
+    int* d_row_order = nullptr;
+    int* d_cpre = nullptr;
+    int4* d_udesc_c = nullptr;
+    int* d_lcols = nullptr;
+    int* d_halo = nullptr;
+    int4* d_cinfo = nullptr;
+    int* d_plan_stats = nullptr;
+    int row_order_cap = 0, cpre_cap = 0, udesc_c_cap = 0, lcols_cap = 0, halo_cap = 0, cinfo_cap = 0,
+        plan_stats_cap = 0;
     int partial_cap = 0;
     double* d_tune_x = nullptr;           // scratch solution of the autotuner's trial solves
     int spmv_resident = 0;                // resident CTAs of the graph-form SpMV (0: not yet queried)

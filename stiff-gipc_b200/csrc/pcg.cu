@@ -271,7 +271,8 @@ __global__ void k_unit_desc(int nrows, const int* __restrict__ row_ptr, const in
 template <int MODE>
 __global__ void __launch_bounds__(kT) k_bsr_spmv(BsrView A, const double* __restrict__ xin, const double* __restrict__ pold,
                                                  double* pnew, double* y, const double* __restrict__ rhs, double a,
-                                                 double b, PcgState* st, double* partials, unsigned* ticket) {
+                                                 double b, PcgState* st, double* partials, unsigned* ticket,
+                                                 int loop = 0) {
     if (MODE != 0 && st->done) return;
     __shared__ double sh[32];
     const double beta = MODE == 1 ? st->beta : 0.0;
@@ -291,8 +292,10 @@ __global__ void __launch_bounds__(kT) k_bsr_spmv(BsrView A, const double* __rest
     double total;
     if (grid_sum_last<kT>(block_sum<kT>(dot, sh), partials, ticket, sh, &total)) {
         st->pAp = total;
-        if (!(total > 0.0)) {  // stop: finite p.Ap <= 0 is a CG breakdown (r = 0 exactly is a solution),
-                               // NaN is reported as a non-finite residual
+        // in a loop iteration (the start guess's x0.A x0 is judged by k_warm_residual): stop when
+        // p.Ap <= 0 -- a finite value is a CG breakdown (r = 0 exactly is a solution), NaN is
+        // reported as a non-finite residual
+        if (loop && !(total > 0.0)) {
             const bool finite = total == total && st->rz == st->rz;
             st->breakdown = finite && st->rz != 0.0;
             st->converged = finite && st->rz == 0.0;
@@ -693,7 +696,7 @@ static int record_body(sgmas_context* c, cudaStream_t s, const double* b, double
         const bool check = (t == 9);
         const unsigned long long cnd = check ? cond : 0ull;
         k_bsr_spmv<1><<<gs, kT, 0, s>>>(bsr_view(B), c->d_z, pold, pnew, c->d_Ap, nullptr, 1.0, 0.0, c->d_state,
-                                        c->d_partials, c->d_ticket);
+                                        c->d_partials, c->d_ticket, 1);
         *nk += 1;
         if (check) {
             k_update_x<<<(n + kT - 1) / kT, kT, 0, s>>>(n, x, pnew, c->d_state);

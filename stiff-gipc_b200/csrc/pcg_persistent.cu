@@ -51,7 +51,13 @@ struct PArgs {
     BsrView A;
     const double* b;
     double *x, *r, *z, *p0, *p1, *Ap;
-    int nrows, units;  // SpMV warp units
+    int nrows;
+    // SpMV plan (k_spmv_plan): per CTA {units, halo offset, halo size, first unit}
+    const int4* cinfo;
+    const int4* udesc_c;  // work-unit descriptors of every CTA, [first unit + u][lane group]
+    const int* lcols;     // halo-local column index of every stored block
+    const int* halo;      // vertex of each halo index (per CTA from its halo offset)
+    int hcap;             // halo entries staged in shared memory (the largest halo)
     // MAS
     int N, Mm, L, total;
     int lvl_count[kMaxLevels + 2], lvl_begin[kMaxLevels + 2];
@@ -352,6 +358,33 @@ __device__ __forceinline__ bool levels_c(const PArgs& a, const Anc& anc, S* tile
     return true;
 }
 
+// One SpMV over this CTA's row range: stage the halo (MODE 1: p_new = z +
+// beta p_old from src = z and pold; MODE 2: src = x) in shared memory, then
+// the CTA's work units round-robin over its warps (descriptors cached in
+// shared memory, ud_sm, the first a.upw per warp).
+template <int MODE>
+__device__ __forceinline__ double spmv_cta(const PArgs& a, int4 ci, const int4* ud_sm, double* hv,
+                                           const double* src, const double* pold, double beta, double* pnew,
+                                           double* y, const double* rhs) {
+    for (int h = threadIdx.x; h < ci.z; h += kPT) {
+        const int v = a.halo[ci.y + h];
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double s0 = ldv<true>(src + 3 * (size_t)v + d);
+            hv[3 * h + d] = MODE == 1 ? __fma_rn(beta, ldv<true>(pold + 3 * (size_t)v + d), s0) : s0;
+        }
+    }
+    __syncthreads();
+    double dot = 0.0;
+    const int w = threadIdx.x / 32, lane = threadIdx.x & 31;
+    const int4* ud = ud_sm + w * a.upw * kRowGroups + lane / kRowLanes;
+    for (int u = w, i = 0; u < ci.x; u += kPT / 32, ++i) {
+        const int4 d = i < a.upw ? ud[kRowGroups * i] : a.udesc_c[(size_t)(ci.w + u) * kRowGroups + lane / kRowLanes];
+        dot += spmv_unit_h<MODE>(a.A, d, lane, a.lcols, hv, pnew, y, rhs);
+    }
+    return dot;
+}
+
 // TG: some level-0 / level-1 tiles are read from global memory (a.t0g, a.t1g)
 template <int B, typename S, typename Acc, bool TG>
 __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
@@ -377,6 +410,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     // SpMV unit descriptors: [warp][unit of the warp][lane group of 8]
     int4* udesc = reinterpret_cast<int4*>(smem_raw + (((size_t)(reinterpret_cast<unsigned char*>(parc + a.nc) -
                                                                 smem_raw) + 15) & ~(size_t)15));
+    // staged halo of the SpMV: 3 doubles per halo vertex
+    double* hv = reinterpret_cast<double*>(udesc + (size_t)(kPT / 32) * a.upw * kRowGroups);
+    const int4 ci = a.cinfo[blockIdx.x];
     if (a.stamps && blockIdx.x == 0 && threadIdx.x == 0) a.stamps[0] = clock64();
     unsigned epoch = 0u, mphase = 0u;
     double* part_pap = a.partials;
@@ -560,11 +596,10 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     // ---- SpMV unit descriptors of this CTA's warps (fixed for the solve)
     {
         const int w = threadIdx.x / 32, lane32 = threadIdx.x & 31;
-        const int gw = blockIdx.x * (kPT / 32) + w;
         for (int i = 0; i < a.upw; ++i) {
-            const int u = gw + i * (int)gridDim.x * (kPT / 32);
+            const int u = w + i * (kPT / 32);
             int4 d = {-1, 0, 0, 0};
-            if (u < a.units) d = unit_desc(a.A, u, lane32);
+            if (u < ci.x) d = a.udesc_c[(size_t)(ci.w + u) * kRowGroups + lane32 / kRowLanes];
             if (lane32 % kRowLanes == 0) udesc[(w * a.upw + i) * kRowGroups + lane32 / kRowLanes] = d;
         }
     }
@@ -583,14 +618,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         double w_alpha = 0.0, w_rr = 0.0;
         double* part_w = a.partials + 3 * gridDim.x;
         double xax = 0.0, xb = 0.0, bb = 0.0;
-        {
-            const int4* ud = udesc + (threadIdx.x / 32) * a.upw * kRowGroups + (threadIdx.x & 31) / kRowLanes;
-            const int gw = blockIdx.x * (kPT / 32) + threadIdx.x / 32;
-            for (int u = gw, i = 0; u < a.units; u += gridDim.x * (kPT / 32), ++i) {
-                const int4 d = i < a.upw ? ud[kRowGroups * i] : unit_desc(a.A, u, threadIdx.x & 31);
-                xax += spmv_unit_d<1, true>(a.A, d, threadIdx.x & 31, a.x, a.x, a.p1, a.Ap, nullptr, 1.0, 0.0, 0.0);
-            }
-        }
+        __syncthreads();  // the descriptor cache is complete
+        xax = spmv_cta<1>(a, ci, udesc, hv, a.x, a.x, 0.0, a.p1, a.Ap, nullptr);  // p = x0 (beta 0)
         for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT) {
             const double bi = a.b[i];
             xb += a.x[i] * bi;
@@ -661,21 +690,12 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     unsigned long long* acc = a.stamps ? a.stamps + 8 * (size_t)(a.stamp_iters + 2) + 16 * (size_t)blockIdx.x : nullptr;
     long long t_rel = clock64();
 #define SLOT(i) (acc ? acc + 2 * (i) : nullptr), &t_rel
-    // SpMV units round-robin over the grid's warps (a contiguous range per CTA
-    // measured no faster: long contact rows then pile up on a few CTAs)
-    constexpr int warps = kPT / 32;
-    const int gw0 = blockIdx.x * warps + threadIdx.x / 32;
     int passes = 0;
     while (!done) {
         ++passes;
         // A: p_new = z + beta p_old, Ap = A p_new, p.Ap
         stamp(a, k, 0);
-        double dot = 0.0;
-        const int4* ud = udesc + (threadIdx.x / 32) * a.upw * kRowGroups + (threadIdx.x & 31) / kRowLanes;
-        for (int u = gw0, i = 0; u < a.units; u += gridDim.x * warps, ++i) {
-            const int4 d = i < a.upw ? ud[kRowGroups * i] : unit_desc(a.A, u, threadIdx.x & 31);
-            dot += spmv_unit_d<1, true>(a.A, d, threadIdx.x & 31, a.z, pold, pnew, a.Ap, nullptr, 1.0, 0.0, beta);
-        }
+        double dot = spmv_cta<1>(a, ci, udesc, hv, a.z, pold, beta, pnew, a.Ap, nullptr);
         dot = block_sum<kPT>(dot, sh);
         if (threadIdx.x == 0) part_pap[blockIdx.x] = dot;
         if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(0))) { ok = false; break; }
@@ -714,11 +734,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                     a.x[i] = a.x[i] + alpha * pnew[i];
             }
             if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(1))) { ok = false; break; }
-            const int4* ud = udesc + (threadIdx.x / 32) * a.upw * kRowGroups + (threadIdx.x & 31) / kRowLanes;
-            for (int u = gw0, i = 0; u < a.units; u += gridDim.x * warps, ++i) {
-                const int4 d = i < a.upw ? ud[kRowGroups * i] : unit_desc(a.A, u, threadIdx.x & 31);
-                spmv_unit_d<2, true>(a.A, d, threadIdx.x & 31, a.x, nullptr, nullptr, a.r, a.b, 1.0, 0.0, 0.0);
-            }
+            spmv_cta<2>(a, ci, udesc, hv, a.x, nullptr, 0.0, nullptr, a.r, a.b);
             if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(2))) { ok = false; break; }
             if (mas && v >= 0) { r0 = a.r[vo]; r1 = a.r[vo + 1]; r2 = a.r[vo + 2]; }
         } else if (mas && v >= 0) {
@@ -783,6 +799,244 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     }
 }
 
+// ---- SpMV plan of the persistent loop (once per solve) ----------------------
+// CTA c takes a contiguous range of block rows in partition order (the MAS
+// rows in slot order, so a range is a compact piece of the mesh), balanced by
+// stored blocks plus a per-row cost.  Its halo is every column its rows touch;
+// the rows' column indices are rewritten as halo indices (lcols), so the SpMV
+// gathers from shared memory.  Work units inside the range as the graph form
+// makes them: a long row (more than kLongRowP blocks) per warp, else four
+// short rows of 8 lanes each.
+constexpr int kLongRowP = 32;
+constexpr int kRowCost = 4;
+
+// exclusive block-wide scan of one int per thread (1024 threads); returns the
+// prefix, *total receives the sum
+__device__ __forceinline__ int block_scan1024(int v, int* sh, int* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+    #pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int y = sh[lane];
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += t;
+        }
+        sh[32 + lane] = y;
+    }
+    __syncthreads();
+    const int pre = (w ? sh[32 + w - 1] : 0) + x - v;
+    *total = sh[63];
+    __syncthreads();
+    return pre;
+}
+
+// row order + prefix sums of the balance cost and of the stored blocks along
+// it (cpre, epre: nrows + 1 entries); one CTA of 1024 threads
+__global__ void __launch_bounds__(1024) k_row_plan(int nrows, int mas, int fem_off, int N, int Mm,
+                                                   const int* __restrict__ part_map, const int* __restrict__ row_ptr,
+                                                   int* row_order, int* cpre, int* epre) {
+    __shared__ int sh[64];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    // order: rows [0, fem_off) and [fem_off + N, nrows) in place, MAS rows by slot
+    if (!mas) {
+        for (int i = threadIdx.x; i < nrows; i += 1024) row_order[i] = i;
+    } else {
+        for (int i = threadIdx.x; i < fem_off; i += 1024) row_order[i] = i;
+        for (int i = fem_off + N + threadIdx.x; i < nrows; i += 1024) row_order[i] = i;
+        for (int base = 0; base < Mm; base += 1024) {
+            const int s = base + threadIdx.x;
+            const int v = s < Mm ? part_map[s] : -1;
+            int tot;
+            const int pre = block_scan1024(v >= 0, sh, &tot);
+            if (v >= 0) row_order[fem_off + carry + pre] = fem_off + v;
+            __syncthreads();
+            if (threadIdx.x == 0) carry += tot;
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    // prefix sums along the order, a contiguous chunk per thread
+    const int chunk = (nrows + 1023) / 1024;
+    const int b0 = min(nrows, (int)threadIdx.x * chunk), b1 = min(nrows, b0 + chunk);
+    int cs = 0, es = 0;
+    for (int i = b0; i < b1; ++i) {
+        const int r = row_order[i];
+        const int len = row_ptr[r + 1] - row_ptr[r];
+        cs += len + kRowCost;
+        es += max(len, 1);  // room in the halo list for every row (a row is in its own halo)
+    }
+    int ct, et;
+    const int cp = block_scan1024(cs, sh, &ct);
+    const int ep = block_scan1024(es, sh, &et);
+    cs = cp;
+    es = ep;
+    for (int i = b0; i < b1; ++i) {
+        const int r = row_order[i];
+        const int len = row_ptr[r + 1] - row_ptr[r];
+        cpre[i] = cs;
+        epre[i] = es;
+        cs += len + kRowCost;
+        es += max(len, 1);
+    }
+    if (threadIdx.x == 0) { cpre[nrows] = ct; epre[nrows] = et; }
+}
+
+__device__ __forceinline__ int range_begin(const int* cpre, int nrows, int c, int G) {
+    const long long target = ((long long)cpre[nrows] * c + G - 1) / G;  // first i with cpre[i] >= c T / G
+    int lo = 0, hi = nrows;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((long long)cpre[mid] < target) lo = mid + 1;
+        else hi = mid;
+    }
+    return c == 0 ? 0 : lo;
+}
+
+// one CTA (512 threads) per CTA of the persistent launch: its row range, halo
+// (bitmap over all rows in shared memory, nrows bits + a word prefix),
+// lcols, work units.  cinfo[c] = {units, halo offset, halo size, first unit};
+// stats[0] = largest halo, stats[1] = most units of a CTA (atomicMax).
+__global__ void __launch_bounds__(512) k_spmv_plan(int nrows, const int* __restrict__ row_order,
+                                                   const int* __restrict__ cpre, const int* __restrict__ epre,
+                                                   const int* __restrict__ row_ptr, const int* __restrict__ cols,
+                                                   int* lcols, int* halo, int4* cinfo, int4* udesc, int* stats) {
+    extern __shared__ unsigned bm[];  // [nw] bitmap, then [nw] exclusive word prefix (as int)
+    __shared__ int sh[64];
+    __shared__ int rng[2];
+    __shared__ int nlong_sh, carry_l, carry_s;
+    const int G = gridDim.x, c = blockIdx.x;
+    const int nw = (nrows + 31) >> 5;
+    int* wpre = reinterpret_cast<int*>(bm + nw);
+    if (threadIdx.x == 0) {
+        rng[0] = range_begin(cpre, nrows, c, G);
+        rng[1] = c + 1 == G ? nrows : range_begin(cpre, nrows, c + 1, G);
+        carry_l = 0;
+        carry_s = 0;
+    }
+    for (int w = threadIdx.x; w < nw; w += 512) bm[w] = 0u;
+    __syncthreads();
+    const int lo = rng[0], hi = rng[1];
+    const int hoff = epre[lo];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = lo + warp; i < hi; i += 16) {  // mark the range's rows and the columns they touch
+        const int r = row_order[i];
+        if (lane == 0) atomicOr(bm + (r >> 5), 1u << (r & 31));
+        for (int p = row_ptr[r] + lane; p < row_ptr[r + 1]; p += 32) {
+            const int col = cols[p];
+            atomicOr(bm + (col >> 5), 1u << (col & 31));
+        }
+    }
+    __syncthreads();
+    // word prefix of the bit counts: a contiguous chunk of words per thread
+    const int chunk = (nw + 511) / 512;
+    const int w0 = min(nw, (int)threadIdx.x * chunk), w1 = min(nw, w0 + chunk);
+    int cnt = 0;
+    for (int w = w0; w < w1; ++w) cnt += __popc(bm[w]);
+    // block scan of 512 values with the 1024-thread helper's pattern
+    int x = cnt;
+    #pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int y = lane < 16 ? sh[lane] : 0;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += t;
+        }
+        sh[32 + lane] = y;
+    }
+    __syncthreads();
+    int pre = (warp ? sh[32 + warp - 1] : 0) + x - cnt;
+    const int H = sh[32 + 15];
+    for (int w = w0; w < w1; ++w) {
+        wpre[w] = pre;
+        pre += __popc(bm[w]);
+    }
+    __syncthreads();
+    // halo list: vertex of each halo index
+    for (int w = threadIdx.x; w < nw; w += 512) {
+        unsigned m = bm[w];
+        int k = wpre[w];
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1u;
+            halo[hoff + k++] = 32 * w + b;
+        }
+    }
+    auto local = [&](int col) { return wpre[col >> 5] + __popc(bm[col >> 5] & ((1u << (col & 31)) - 1u)); };
+    for (int i = lo + warp; i < hi; i += 16) {  // halo-local column indices
+        const int r = row_order[i];
+        for (int p = row_ptr[r] + lane; p < row_ptr[r + 1]; p += 32) lcols[p] = local(cols[p]);
+    }
+    // work units: the range's long rows first (one unit each), then its short rows, four per unit
+    if (threadIdx.x == 0) nlong_sh = 0;
+    __syncthreads();
+    {
+        int nl = 0;
+        for (int i = lo + (int)threadIdx.x; i < hi; i += 512) {
+            const int r = row_order[i];
+            nl += (row_ptr[r + 1] - row_ptr[r]) > kLongRowP;
+        }
+        if (nl) atomicAdd(&nlong_sh, nl);
+    }
+    __syncthreads();
+    const int nl = nlong_sh;
+    for (int base = lo; base < hi; base += 512) {
+        const int i = base + threadIdx.x;
+        int r = -1, len = 0;
+        if (i < hi) {
+            r = row_order[i];
+            len = row_ptr[r + 1] - row_ptr[r];
+        }
+        const bool isl = i < hi && len > kLongRowP, iss = i < hi && !isl;
+        const unsigned bl = __ballot_sync(0xffffffffu, isl), bs = __ballot_sync(0xffffffffu, iss);
+        if (lane == 0) { sh[warp] = __popc(bl); sh[16 + warp] = __popc(bs); }
+        __syncthreads();
+        int offl = carry_l, offs = carry_s;
+        for (int k = 0; k < warp; ++k) { offl += sh[k]; offs += sh[16 + k]; }
+        const unsigned lt = (1u << lane) - 1u;
+        if (isl) {
+            const int u = offl + __popc(bl & lt);
+            const int4 d = make_int4(r, row_ptr[r], row_ptr[r + 1], 1 | (local(r) << 1));
+            #pragma unroll
+            for (int g = 0; g < kRowGroups; ++g) udesc[(size_t)(lo + u) * kRowGroups + g] = d;
+        } else if (iss) {
+            const int sidx = offs + __popc(bs & lt);
+            const int u = nl + sidx / kRowGroups, g = sidx % kRowGroups;
+            udesc[(size_t)(lo + u) * kRowGroups + g] = make_int4(r, row_ptr[r], row_ptr[r + 1], local(r) << 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < 16; ++k) { carry_l += sh[k]; carry_s += sh[16 + k]; }
+        }
+        __syncthreads();
+    }
+    const int ns = carry_s;
+    const int units = nl + (ns + kRowGroups - 1) / kRowGroups;
+    if (threadIdx.x < kRowGroups && ns % kRowGroups && threadIdx.x >= ns % kRowGroups)  // empty groups of the last unit
+        udesc[(size_t)(lo + units - 1) * kRowGroups + threadIdx.x] = make_int4(-1, 0, 0, 0);
+    if (threadIdx.x == 0) {
+        cinfo[c] = make_int4(units, hoff, H, lo);
+        atomicMax(stats, H);
+        atomicMax(stats + 1, units);
+    }
+}
+
 // level-0 bank of every level-1 node (all slots of a component agree)
 template <int B>
 __global__ void k_l1_bank(int Mm, int l1_begin, const int* __restrict__ part_map, const int* __restrict__ going_next,
@@ -805,6 +1059,47 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
     SG_CUDA(c, cudaFuncGetAttributes(&fa, k_pcg_persistent<B, S, Acc, false>));
     const size_t budget = (size_t)max_smem - fa.sharedSizeBytes - 256;  // minus the kernel's static shared memory
     const int G = c->pcg_ctas > 0 ? std::min(dev_sms, c->pcg_ctas) : dev_sms;  // CTAs of this solve
+    // SpMV plan: row order, CTA row ranges, halos, halo-local columns, work units
+    int max_units = 0;
+    {
+        cudaStream_t s = c->stream;
+        const int nrows = a.nrows;
+        const long long cap = c->bsr.cap;
+        if (ctx_alloc_grow(c, &c->d_row_order, &c->row_order_cap, nrows) ||
+            ctx_alloc_grow(c, &c->d_cpre, &c->cpre_cap, 2 * (nrows + 1)) ||
+            ctx_alloc_grow(c, &c->d_udesc_c, &c->udesc_c_cap, nrows * kRowGroups) ||
+            ctx_alloc_grow(c, &c->d_lcols, &c->lcols_cap, (int)cap) ||
+            ctx_alloc_grow(c, &c->d_halo, &c->halo_cap, (int)cap + nrows) ||
+            ctx_alloc_grow(c, &c->d_cinfo, &c->cinfo_cap, G) ||
+            ctx_alloc_grow(c, &c->d_plan_stats, &c->plan_stats_cap, 2))
+            return SGMAS_ERR_CUDA;
+        int* cpre = c->d_cpre;
+        int* epre = c->d_cpre + nrows + 1;
+        k_row_plan<<<1, 1024, 0, s>>>(nrows, a.precond == 1, a.precond == 1 ? a.ex.fem_off : 0, a.N, a.Mm,
+                                      a.part_map, a.A.row_ptr, c->d_row_order, cpre, epre);
+        SG_CUDA(c, cudaMemsetAsync(c->d_plan_stats, 0, 2 * sizeof(int), s));
+        const size_t plan_smem = 2 * (size_t)((nrows + 31) / 32) * sizeof(unsigned);
+        if (plan_smem + 1024 > (size_t)max_smem) return 1;  // (the kernel's static shared memory is < 1 KB)
+        if (plan_smem > 48 * 1024)
+            SG_CUDA(c, cudaFuncSetAttribute(k_spmv_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan_smem));
+        k_spmv_plan<<<G, 512, plan_smem, s>>>(nrows, c->d_row_order, cpre, epre, a.A.row_ptr, a.A.cols, c->d_lcols,
+                                              c->d_halo, c->d_cinfo, c->d_udesc_c, c->d_plan_stats);
+        c->build_launches += 2;
+        SG_CUDA(c, cudaGetLastError());
+        int st[2] = {0, 0};  // largest halo, most units of a CTA
+        SG_CUDA(c, cudaMemcpyAsync(st, c->d_plan_stats, sizeof(st), cudaMemcpyDeviceToHost, s));
+        SG_CUDA(c, cudaStreamSynchronize(s));
+        a.hcap = st[0];
+        max_units = st[1];
+        a.cinfo = c->d_cinfo;
+        a.udesc_c = c->d_udesc_c;
+        a.lcols = c->d_lcols;
+        a.halo = c->d_halo;
+    }
+    // the staged halo comes first; the subdomain tiles share what is left
+    const size_t hbytes = (3 * sizeof(double) * (size_t)a.hcap + 15) & ~(size_t)15;
+    if (hbytes + 256 > budget) return 1;
+    const size_t tbudget = budget - hbytes;
     size_t smem = 0;
     if (a.precond == 1) {
         a.nb0 = a.Mm / B;
@@ -871,28 +1166,30 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
                              (size_t)a.nc * sizeof(int);
         // level-0 tiles stay in shared memory if anything does; level-1 tiles next
         a.t0g = a.t1g = 0;
-        if (small + (size_t)(a.k0 + a.k1) * tb + (a.L > 2 ? tb : 0) > budget) a.t1g = 1;
-        if (small + (size_t)a.k0 * tb + (a.L > 2 ? tb : 0) > budget) a.t0g = 1;
+        if (small + (size_t)(a.k0 + a.k1) * tb + (a.L > 2 ? tb : 0) > tbudget) a.t1g = 1;
+        if (small + (size_t)a.k0 * tb + (a.L > 2 ? tb : 0) > tbudget) a.t0g = 1;
         const size_t fixed = small + (size_t)((a.t0g ? 0 : a.k0) + (a.t1g ? 0 : a.k1)) * tb;
         if (a.L > 2) {
-            if (fixed + tb > budget) return 1;
-            a.capc = (int)std::min<size_t>({(size_t)(a.nc / B), (size_t)(kPT / B), (budget - fixed) / tb});
+            if (fixed + tb > tbudget) return 1;
+            a.capc = (int)std::min<size_t>({(size_t)(a.nc / B), (size_t)(kPT / B), (tbudget - fixed) / tb});
         } else {
-            if (fixed > budget) return 1;
+            if (fixed > tbudget) return 1;
             a.capc = 0;
         }
         smem = fixed + (size_t)a.capc * tb;
     } else {
         a.k0 = a.k1 = a.nb0 = a.nb1 = a.nc = a.capc = a.t0g = a.t1g = 0;
     }
-    // SpMV unit descriptors (16 B per warp, unit and lane group), as many as fit, at most 16 units per warp
+    // the staged halo (3 doubles per vertex), then as many cached unit descriptors (16 B per warp,
+    // unit and lane group) as fit, at most 16 units per warp
     {
-        const int per_warp = (a.units + G * (kPT / 32) - 1) / (G * (kPT / 32));
         smem = (smem + 15) & ~(size_t)15;
+        if (smem + hbytes > budget) return 1;
+        const int per_warp = (max_units + kPT / 32 - 1) / (kPT / 32);
         const size_t per_unit = (size_t)(kPT / 32) * kRowGroups * sizeof(int4);
-        const size_t room = budget > smem ? (budget - smem) / per_unit : 0;
+        const size_t room = (budget - smem - hbytes) / per_unit;
         a.upw = (int)std::min<size_t>({(size_t)per_warp, (size_t)16, room});
-        smem += (size_t)a.upw * per_unit;
+        smem += (size_t)a.upw * per_unit + hbytes;
     }
     auto kern = (a.t0g || a.t1g) ? k_pcg_persistent<B, S, Acc, true> : k_pcg_persistent<B, S, Acc, false>;
     // the attribute is per function, shared by every context and host thread: always the full
@@ -923,7 +1220,6 @@ int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRu
     a.A = BsrView{M.row_ptr, M.cols, M.vals, M.cap, M.row_list, M.nrows, M.n_long, nullptr};
     a.b = b; a.x = x; a.r = c->d_r; a.z = c->d_z; a.p0 = c->d_p0; a.p1 = c->d_p1; a.Ap = c->d_Ap;
     a.nrows = M.nrows;
-    a.units = spmv_units(M.n_long, M.nrows);
     a.precond = cfg.precond;
     a.dinv = c->d_diag_inv;
     a.abd_rows = cfg.precond == 0 ? 4 * cfg.abd_bodies : 0;

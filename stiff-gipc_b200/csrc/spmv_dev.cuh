@@ -135,4 +135,67 @@ __device__ __forceinline__ double spmv_unit_d(const BsrView& A, int4 desc, int l
     return dot;
 }
 
+// ---- SpMV over a CTA's halo (the persistent loop) --------------------------
+// A CTA owns a contiguous range of block rows (in partition order, balanced
+// by stored blocks).  Once per SpMV it stages the vector entries of every
+// column its rows touch (its halo, 3 doubles per vertex) in shared memory;
+// the rows' column indices are stored local to that halo (lcols), so the
+// gathers read shared memory.  desc.w = 1 for a whole-warp (long) row, plus
+// twice the row's own halo index.
+//   MODE 1: hv holds p_new = z + beta p_old; y = A p_new, pnew[row] = p_new;
+//           returns p_new.Ap of the rows this lane wrote
+//   MODE 2: hv holds x; y = rhs - A x
+template <int MODE>
+__device__ __forceinline__ double spmv_unit_h(const BsrView& A, int4 desc, int lane, const int* __restrict__ lcols,
+                                              const double* hv, double* pnew, double* y,
+                                              const double* __restrict__ rhs) {
+    const double* __restrict__ bvals = A.vals;
+    const long long cap = A.cap;
+    const bool longw = (desc.w & 1) != 0;
+    const int row = desc.x, l = longw ? lane : (lane % kRowLanes), G = longw ? 32 : kRowLanes;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    double dot = 0.0;
+    for (int p = desc.y + 2 * l; p < desc.z; p += 2 * G) {
+        const int2 cc = __ldg(reinterpret_cast<const int2*>(lcols + p));
+        double2 v[9];
+        #pragma unroll
+        for (int q = 0; q < 9; ++q) v[q] = __ldg(reinterpret_cast<const double2*>(bvals + q * cap + p));
+        const double* h0 = hv + 3 * cc.x;
+        const double* h1 = hv + 3 * cc.y;
+        const double x00 = h0[0], x01 = h0[1], x02 = h0[2], x10 = h1[0], x11 = h1[1], x12 = h1[2];
+        a0 += v[0].x * x00 + v[1].x * x01 + v[2].x * x02 + v[0].y * x10 + v[1].y * x11 + v[2].y * x12;
+        a1 += v[3].x * x00 + v[4].x * x01 + v[5].x * x02 + v[3].y * x10 + v[4].y * x11 + v[5].y * x12;
+        a2 += v[6].x * x00 + v[7].x * x01 + v[8].x * x02 + v[6].y * x10 + v[7].y * x11 + v[8].y * x12;
+    }
+    if (longw) {  // warp-uniform branch
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+    } else {
+        #pragma unroll
+        for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o, kRowLanes);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o, kRowLanes);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o, kRowLanes);
+        }
+    }
+    if (l == 0 && row >= 0) {
+        double* yr = y + 3 * (size_t)row;
+        if (MODE == 1) {
+            const double* hr = hv + 3 * (desc.w >> 1);
+            const double p0 = hr[0], p1 = hr[1], p2 = hr[2];
+            pnew[3 * (size_t)row] = p0; pnew[3 * (size_t)row + 1] = p1; pnew[3 * (size_t)row + 2] = p2;
+            yr[0] = a0; yr[1] = a1; yr[2] = a2;
+            dot = p0 * a0 + p1 * a1 + p2 * a2;
+        } else {
+            const double* br = rhs + 3 * (size_t)row;
+            yr[0] = br[0] - a0; yr[1] = br[1] - a1; yr[2] = br[2] - a2;
+        }
+    }
+    return dot;
+}
+
 }  // namespace sgmas

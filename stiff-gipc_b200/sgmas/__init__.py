@@ -321,10 +321,14 @@ class Context:
         self.cp_num = n
 
     def mas_assemble(self, vals, rows, cols, indices=None, offset=0, cp_num=None):
+        """setPreconditioner_bcoo: with indices (device uint32), the triplet
+        count is the number of indices, as calculate_subsystem_bcoo_indices
+        returns it; without, every block of the BCOO."""
         if cp_num is None:
             cp_num = getattr(self, "cp_num", 0)
+        n = int(rows.shape[0]) if indices is None else int(indices.shape[0])
         self._check(self.L.sgmas_mas_assemble(self.h, _ptr(vals), _ptr(rows), _ptr(cols), _ptr(indices), offset,
-                                              int(rows.shape[0]), cp_num))
+                                              n, cp_num))
 
     def mas_apply(self, r, z):
         self._check(self.L.sgmas_mas_apply(self.h, _ptr(r), _ptr(z)))

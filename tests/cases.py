@@ -61,12 +61,12 @@ def build(name, bank=16):
     return Case(name, s, pm, rm, st, nn, nl)
 
 
-def oracle_iteration_band(s, precond, mas=None, rel_tol=1e-4, n_perturb=6, **kw):
-    """Iteration counts of the oracle port's PCG on b scaled by
+def oracle_iteration_band(s, precond, mas=None, rel_tol=1e-4, n_perturb=10, **kw):
+    """(min, max) iteration counts of the oracle port's PCG on b scaled by
     (1 + k 2^-52), k = 0 .. n_perturb - 1, serial and on every host thread.
     On ill-conditioned systems CG's count moves with the last bit of any sum;
     this measured spread (not a guess) is the band a device solve must fall
-    in, widened by one check interval."""
+    in (see band_ok)."""
     its = []
     nth = O.lib().or_omp_max_threads()
     for k in range(n_perturb):
@@ -76,3 +76,12 @@ def oracle_iteration_band(s, precond, mas=None, rel_tol=1e-4, n_perturb=6, **kw)
                          nthreads=nt, **kw)
             its.append(r["iterations"])
     return min(its), max(its)
+
+
+def band_ok(iterations, band):
+    """The device's count lies in the oracle's measured band, widened on both
+    sides by that band's own width (a handful of samples under-reads the
+    spread) and by at least one check interval."""
+    lo, hi = band
+    w = max(10, hi - lo)
+    return lo - w <= iterations <= hi + w

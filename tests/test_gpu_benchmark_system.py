@@ -7,7 +7,8 @@ Three checks per precision:
   * the reference's stopping rule at 1e-4: the true relative residual
     ||b - A x|| / ||b|| (computed here from the scipy matrix) is <= 1e-4;
   * the iteration count lies in the band the oracle port itself spans when b
-    moves in its last bit (see below), widened by one check interval;
+    moves in its last bit (see below), widened by that band's width (at least
+    one check interval);
   * at 1e-10, the solution is within 1e-6 relative of an FP64 direct solve
     (banded Cholesky in reverse Cuthill-McKee order, sgmas.synth.direct_solve),
     and at 1e-4 within 1e-5.
@@ -16,7 +17,8 @@ Why a band and not one fixed count: on this system CG's iteration count moves
 with the last bit of any sum.  The oracle port (the same algorithm, serial or
 OpenMP sums) run on b scaled by (1 + k * 2^-52), k = 0..3, spans a range of
 counts by itself (measured in the test, printed on failure); the device's
-count must fall inside that range, widened by one check interval (10).
+count must fall inside that range, widened on each side by its own width
+(at least one check interval, 10): a few samples under-read the spread.
 """
 from __future__ import annotations
 
@@ -104,8 +106,7 @@ def test_benchmark_solve_matches_oracle(precision):
     assert res <= 1e-4 * 1.0001, res
     assert rep["iterations"] % 10 == 0
     band = oracle_band(precision)
-    lo, hi = min(band) - 10, max(band) + 10
-    assert lo <= rep["iterations"] <= hi, (rep["iterations"], band)
+    assert cases.band_ok(rep["iterations"], band), (rep["iterations"], band)
     # solution error at the benchmark tolerance (the oracle's is ~1e-6 here)
     assert rel_err(xg, direct()) <= 1e-5, rel_err(xg, direct())
 
