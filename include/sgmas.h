@@ -63,6 +63,15 @@ typedef struct {
                                     scales it by alpha = x0.b / x0.A x0 (0 unless positive), rejects it
                                     (x0 = 0) when ||b - alpha A x0|| > ||b||, and tests convergence
                                     against ||b|| instead of ||r0|| */
+    int body_patches;            /* 0: the reference's composition (12x12 block-Jacobi on the bodies, MAS on the
+                                    FEM range).  1 (needs preconditioner 1 and abd_bodies > 0, persistent form):
+                                    each body's block is widened to a patch -- the body's 4 block rows plus the
+                                    FEM vertices coupled to it (each FEM vertex in the patch of the lowest-numbered
+                                    body it touches, at most 64) -- factored densely in FP64 and stored as
+                                    W = L^-1 in the MAS storage precision; z = MAS(r) + sum of the patches'
+                                    W^T W r.  For bodies resting on FEM surfaces with stiff barrier contact,
+                                    where the body-FEM couplings dominate.  The library's own; no reference
+                                    counterpart */
 } sgmas_pcg_config;
 
 typedef struct {

@@ -87,7 +87,8 @@ void free_all(sgmas_context* c) {
                     c->d_coarse_ticket, c->bsr.row_list, c->bsr.d_nlong, c->bsr.tcols, c->bsr.tsrc,
                     c->d_psync, c->d_stamps, c->d_l1_bank, c->d_own1, c->d_tune_x, c->bsr.udesc, c->d_plan_idx,
                     c->d_plan_start, c->d_row_order, c->d_cpre, c->d_udesc_c, c->d_lcols, c->d_halo,
-                    c->d_cinfo, c->d_plan_stats};
+                    c->d_cinfo, c->d_plan_stats, c->d_patch_owner, c->d_patch_ent, c->d_patch_list, c->d_patch_info,
+                    c->d_patch_w64, c->d_patch_wcol, c->d_patch_wrow, c->d_patch_zs};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -360,6 +361,11 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
     if (cfg->initial_guess != 0 && cfg->initial_guess != 1)
         return ctx_fail(c, SGMAS_ERR_ARG, "initial_guess must be 0 (x0 = 0) or 1 (x holds the start guess)");
     rc_cfg.warm = cfg->initial_guess;
+    if (cfg->body_patches != 0 && cfg->body_patches != 1)
+        return ctx_fail(c, SGMAS_ERR_ARG, "body_patches must be 0 or 1");
+    if (cfg->body_patches && (cfg->preconditioner != 1 || cfg->abd_bodies < 1))
+        return ctx_fail(c, SGMAS_ERR_ARG, "body_patches needs the MAS preconditioner and abd_bodies > 0");
+    rc_cfg.patches = cfg->body_patches;
     if (!c->ev0) {
         SG_CUDA(c, cudaEventCreate(&c->ev0));
         SG_CUDA(c, cudaEventCreate(&c->ev1));
@@ -379,6 +385,9 @@ int sgmas_pcg_solve(sgmas_context* c, const sgmas_bcoo* A, const double* d_b, do
     SG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     float prep_ms = 0.f;
     rc = c->persistent ? pcg_run_persistent(c, d_b, d_x, rc_cfg, &solve_ms, &launches) : 1;
+    if (rc == 1 && rc_cfg.patches)
+        return ctx_fail(c, SGMAS_ERR_STATE, "body patches run in the persistent form only, which %s",
+                        c->persistent ? "does not fit this system" : "is switched off (sgmas_set_pcg_mode)");
     if (rc == 1) rc = pcg_run(c, d_b, d_x, rc_cfg, &solve_ms, &launches);  // graph path
     if (rc) return rc;
     cudaEventElapsedTime(&prep_ms, c->ev2, c->ev0);

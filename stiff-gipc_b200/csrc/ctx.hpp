@@ -27,6 +27,7 @@ struct PcgState {
 struct ExtraRows {
     int fem_off, abd_bodies, nrows, n_units;
     const double* abd_inv;  // 144 per body, row-major inverse
+    int patch;              // 1: the bodies are preconditioned by their patches (patch.cu), not here
 };
 
 struct PcgRunCfgLite {
@@ -42,6 +43,7 @@ struct PcgRunCfg {
     int fem_offset;
     int check_every;
     int warm;          // 1: x holds a start guess (scaled, rejected when it raises ||r0||)
+    int patches;       // 1: body patches (patch.cu) on the body rows and the FEM vertices they touch
 };
 
 struct BsrMatrix {
@@ -133,6 +135,19 @@ struct sgmas_context {
     int l1_bank_cap = 0;
     int* d_own1 = nullptr;                // first level-1 bank of each CTA of the persistent kernel
     int own1_cap = 0;
+    // body patches (patch.cu): owner body of each FEM vertex, patch lists, {k, truncated}, FP64 scratch,
+    // W packed by columns and by rows (storage precision), the patches' part of z
+    int* d_patch_owner = nullptr;          // per-row entry counts and offsets of the patch lists
+    int* d_patch_ent = nullptr;            // patch entries (b kPatchMax + i) covering each row, body order
+    int* d_patch_list = nullptr;
+    int2* d_patch_info = nullptr;
+    double* d_patch_w64 = nullptr;
+    void* d_patch_wcol = nullptr;
+    void* d_patch_wrow = nullptr;
+    double* d_patch_zs = nullptr;          // [bodies][3 kPatchMax] each patch's part of z on its FEM rows
+    int patch_owner_cap = 0, patch_ent_cap = 0, patch_list_cap = 0, patch_info_cap = 0, patch_w64_cap = 0, patch_zs_cap = 0;
+    size_t patch_w_bytes = 0;
+    int patch_bodies = 0;
     // SpMV plan of the persistent kernel (per solve): row order, cost prefixes, CTA work units,
     // halo-local column indices, halo vertex lists, per-CTA info, largest halo / unit count
     int* d_row_order = nullptr;
@@ -239,6 +254,7 @@ int morton_codes(sgmas_context* c, const double* pos, int n, const double* aabb,
 int sort_u64_pairs(sgmas_context* c, uint64_t* keys, uint32_t* vals, int n, int key_bits);
 int mas_invert_blocks_dev(sgmas_context* c, const double* hess, int nblk, double* out64);
 int pcg_profile(sgmas_context* c, int reps, float* ms, int n_ms);
+int patch_build(sgmas_context* c, int nbodies, int fem_off);  // body patches of the current block CSR
 int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRunCfg& cfg, float* solve_ms,
                        int* launches, unsigned long long* stamps = nullptr, int stamp_iters = 0);
 

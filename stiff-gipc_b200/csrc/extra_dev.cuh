@@ -18,7 +18,7 @@ __device__ __forceinline__ void extra_rows_work(const ExtraRows& ex, int N, int 
                                                 double* r, const double* p, const double* Ap, double* z, int wid,
                                                 int nw, int lane, double& rz, double& rr) {
     const int nb = ex.abd_bodies;
-    for (int g0 = 2 * wid; g0 < nb; g0 += 2 * nw) {  // warp-uniform trip count
+    for (int g0 = 2 * wid; g0 < (ex.patch ? 0 : nb); g0 += 2 * nw) {  // warp-uniform trip count
         const int g = g0 + lane / 16, k = lane % 16;
         const bool valid = g < nb && k < 12;
         const size_t o = 12 * (size_t)g + k;

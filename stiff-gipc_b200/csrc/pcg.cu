@@ -960,13 +960,16 @@ int pcg_prepare(sgmas_context* c, const sgmas_bcoo* A, const PcgRunCfg& cfg) {
     int rc = bsr_reuse(c, A) ? 0 : bsr_build(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows);
     if (rc) return rc;
     if (cfg.precond == 0) return jacobi_setup(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows, cfg.abd_bodies);
-    if (cfg.abd_bodies > 0)  // MAS on the FEM range + 12x12 block-Jacobi on the bodies
-        return jacobi_setup(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows, cfg.abd_bodies, false);
+    if (cfg.abd_bodies > 0) {  // MAS on the FEM range + 12x12 block-Jacobi on the bodies (or body patches)
+        rc = jacobi_setup(c, A->d_values, A->d_rows, A->d_cols, A->n_blocks, nrows, cfg.abd_bodies, false);
+        if (rc == 0 && cfg.patches) rc = patch_build(c, cfg.abd_bodies, cfg.fem_offset);
+        return rc;
+    }
     return 0;
 }
 
 ExtraRows extra_rows_of(const sgmas_context* c, const PcgRunCfg& cfg) {
-    ExtraRows ex;
+    ExtraRows ex = {};
     ex.fem_off = cfg.precond == 1 ? cfg.fem_offset : 0;
     ex.abd_bodies = cfg.precond == 1 ? cfg.abd_bodies : 0;
     ex.nrows = c->bsr.nrows;

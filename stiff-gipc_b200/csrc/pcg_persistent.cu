@@ -40,6 +40,7 @@
 #include "mas_dev.cuh"
 #include "spmv_dev.cuh"
 #include "extra_dev.cuh"
+#include "patch_dev.cuh"
 
 using namespace sgmas;
 
@@ -73,6 +74,7 @@ struct PArgs {
     int t0g, t1g;          // level-0 / level-1 tiles read from global memory (they did not fit)
     int upw;               // SpMV unit descriptors cached per warp in shared memory
     ExtraRows ex;          // rows outside the MAS range (bodies, other rows); MAS vertex v is row ex.fem_off + v
+    PatchView pv;          // body patches (pv.bodies = 0: none)
     // block-Jacobi
     const double* dinv;
     int abd_rows, precond;
@@ -370,7 +372,8 @@ __device__ __forceinline__ double spmv_cta(const PArgs& a, int4 ci, const int4* 
         const int v = a.halo[ci.y + h];
         #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            const double s0 = ldv<true>(src + 3 * (size_t)v + d);
+            double s0 = ldv<true>(src + 3 * (size_t)v + d);
+            if (MODE == 1 && a.pv.bodies) s0 += patch_z(a.pv, v, d);  // z = MAS part + the patches' parts
             hv[3 * h + d] = MODE == 1 ? __fma_rn(beta, ldv<true>(pold + 3 * (size_t)v + d), s0) : s0;
         }
     }
@@ -384,6 +387,11 @@ __device__ __forceinline__ double spmv_cta(const PArgs& a, int4 ci, const int4* 
     }
     return dot;
 }
+
+// storage of the body patches for each MAS storage: factored in every
+// precision (the explicit FP32 MAS pairs with FP32-factored patches)
+template <typename S> struct PatchS { using T = S; };
+template <> struct PatchS<float> { using T = Fact<float>; };
 
 // TG: some level-0 / level-1 tiles are read from global memory (a.t0g, a.t1g)
 template <int B, typename S, typename Acc, bool TG>
@@ -412,6 +420,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                                                                 smem_raw) + 15) & ~(size_t)15));
     // staged halo of the SpMV: 3 doubles per halo vertex
     double* hv = reinterpret_cast<double*>(udesc + (size_t)(kPT / 32) * a.upw * kRowGroups);
+    // body-patch scratch: the patch's r and y (12 + 3 kPatchMax each)
+    Acc* prl = reinterpret_cast<Acc*>(hv + 3 * (size_t)a.hcap);
+    Acc* pyl = prl + 12 + 3 * kPatchMax;
     const int4 ci = a.cinfo[blockIdx.x];
     if (a.stamps && blockIdx.x == 0 && threadIdx.x == 0) a.stamps[0] = clock64();
     unsigned epoch = 0u, mphase = 0u;
@@ -588,6 +599,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             rz += r0 * z0 + r1 * z1 + r2 * z2;
             rr += r0 * r0 + r1 * r1 + r2 * r2;
         }
+        // body patches (r complete in global memory: stored in phase B, a grid barrier since)
+        for (int pb = blockIdx.x; pb < a.pv.bodies; pb += gridDim.x)
+            patch_apply_cta<typename PatchS<S>::T, Acc>(a.pv, pb, a.ex.fem_off, a.r, a.z, prl, pyl, rz, rr);
         rz = block_sum<kPT>(rz, sh);
         rr = block_sum<kPT>(rr, sh);
         if (threadIdx.x == 0) { part_rz[blockIdx.x] = rz; part_rr[blockIdx.x] = rr; }
@@ -668,9 +682,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             if (a.warm && own) { x0 = a.x[vo]; x1 = a.x[vo + 1]; x2 = a.x[vo + 2]; }
         }
         if (ok) apply_b();
-        if (a.L > 2) {
+        if (a.L > 2 || a.pv.bodies) {  // (the patches read r of other CTAs' rows)
             ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
-            if (ok) ok = levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch);
+            if (ok && a.L > 2) ok = levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch);
         }
         if (ok) collect(0, 0.0, a.p1);
     } else {
@@ -737,17 +751,25 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             spmv_cta<2>(a, ci, udesc, hv, a.x, nullptr, 0.0, nullptr, a.r, a.b);
             if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(2))) { ok = false; break; }
             if (mas && v >= 0) { r0 = a.r[vo]; r1 = a.r[vo + 1]; r2 = a.r[vo + 2]; }
-        } else if (mas && v >= 0) {
-            r0 = r0 - alpha * q0; r1 = r1 - alpha * q1; r2 = r2 - alpha * q2;
-            if (own) { x0 += alpha * p0v; x1 += alpha * p1v; x2 += alpha * p2v; }
+        } else {
+            if (mas && v >= 0) {
+                r0 = r0 - alpha * q0; r1 = r1 - alpha * q1; r2 = r2 - alpha * q2;
+                if (own) { x0 += alpha * p0v; x1 += alpha * p1v; x2 += alpha * p2v; }
+                if (own && a.pv.bodies) { a.r[vo] = r0; a.r[vo + 1] = r1; a.r[vo + 2] = r2; }
+            }
+            // body rows with patches: updated here, before the patches read them in phase C
+            for (int i = blockIdx.x * kPT + threadIdx.x; i < 12 * a.pv.bodies; i += gridDim.x * kPT) {
+                a.x[i] = a.x[i] + alpha * pnew[i];
+                a.r[i] = a.r[i] - alpha * a.Ap[i];
+            }
         }
         stamp(a, k, 2);
         if (mas) {
             apply_b();
-            if (a.L > 2) {
+            if (a.L > 2 || a.pv.bodies) {
                 if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(3))) { ok = false; break; }
                 stamp(a, k, 3);
-                if (!levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch)) ok = false;
+                if (a.L > 2 && !levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch)) ok = false;
             }
             collect(refresh ? 0 : 1, alpha, pnew);
         } else {
@@ -781,6 +803,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     if (mas && own) {
         a.x[vo] = x0; a.x[vo + 1] = x1; a.x[vo + 2] = x2;
         a.r[vo] = r0; a.r[vo + 1] = r1; a.r[vo + 2] = r2;
+        if (a.pv.bodies)  // the last z with its patch part (the loop ended after a grid barrier)
+            for (int d = 0; d < 3; ++d) a.z[vo + d] += patch_z(a.pv, vo / 3, d);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         PcgState s = {};
@@ -1098,8 +1122,9 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
     }
     // the staged halo comes first; the subdomain tiles share what is left
     const size_t hbytes = (3 * sizeof(double) * (size_t)a.hcap + 15) & ~(size_t)15;
-    if (hbytes + 256 > budget) return 1;
-    const size_t tbudget = budget - hbytes;
+    const size_t pbytes = a.pv.bodies ? 2 * (12 + 3 * kPatchMax) * sizeof(Acc) : 0;  // body-patch scratch
+    if (hbytes + pbytes + 256 > budget) return 1;
+    const size_t tbudget = budget - hbytes - pbytes;
     size_t smem = 0;
     if (a.precond == 1) {
         a.nb0 = a.Mm / B;
@@ -1187,9 +1212,10 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
         if (smem + hbytes > budget) return 1;
         const int per_warp = (max_units + kPT / 32 - 1) / (kPT / 32);
         const size_t per_unit = (size_t)(kPT / 32) * kRowGroups * sizeof(int4);
-        const size_t room = (budget - smem - hbytes) / per_unit;
+        if (smem + hbytes + pbytes > budget) return 1;
+        const size_t room = (budget - smem - hbytes - pbytes) / per_unit;
         a.upw = (int)std::min<size_t>({(size_t)per_warp, (size_t)16, room});
-        smem += (size_t)a.upw * per_unit + hbytes;
+        smem += (size_t)a.upw * per_unit + hbytes + pbytes;
     }
     auto kern = (a.t0g || a.t1g) ? k_pcg_persistent<B, S, Acc, true> : k_pcg_persistent<B, S, Acc, false>;
     // the attribute is per function, shared by every context and host thread: always the full
@@ -1257,6 +1283,14 @@ int pcg_run_persistent(sgmas_context* c, const double* b, double* x, const PcgRu
         a.coarse_table = c->d_coarse_table; a.fine_mask = c->d_fine_mask;
         a.inv = c->d_inv; a.R = c->d_R;
         a.ex = extra_rows_of(c, cfg);
+        if (cfg.patches) {
+            if (c->patch_bodies != cfg.abd_bodies || !c->d_patch_info) return SGMAS_ERR_STATE;
+            if (ctx_alloc_grow(c, &c->d_patch_zs, &c->patch_zs_cap, 3 * kPatchMax * cfg.abd_bodies))
+                return SGMAS_ERR_CUDA;
+            a.pv = PatchView{cfg.abd_bodies, c->d_patch_list, c->d_patch_info, c->d_patch_wcol, c->d_patch_wrow,
+                             c->d_patch_zs, c->d_patch_owner + M.nrows, c->d_patch_ent};
+            a.ex.patch = 1;
+        }
     }
     int rc;
     switch ((c->bank == 16 ? 0 : 4) + c->precision) {

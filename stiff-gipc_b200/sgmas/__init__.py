@@ -36,7 +36,7 @@ class PcgConfig(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("rel_tol", C.c_double), ("abs_tol", C.c_double),
                 ("use_preconditioned_norm", C.c_int), ("preconditioner", C.c_int),
                 ("abd_bodies", C.c_int), ("fem_offset", C.c_int), ("check_every", C.c_int),
-                ("initial_guess", C.c_int)]
+                ("initial_guess", C.c_int), ("body_patches", C.c_int)]
 
 
 class PcgReport(C.Structure):
@@ -223,13 +223,14 @@ def _h(a, dtype):
 
 
 def pcg_config(max_iter=0, rel_tol=1e-4, abs_tol=0.0, use_preconditioned_norm=False, preconditioner="mas",
-               abd_bodies=0, fem_offset=0, check_every=10, initial_guess=False):
+               abd_bodies=0, fem_offset=0, check_every=10, initial_guess=False, body_patches=False):
     """initial_guess=True: x holds a start guess x0 on entry (scaled by
     x0.b / x0.A x0, rejected when it raises the residual; convergence is then
-    tested against ||b||)."""
+    tested against ||b||).  body_patches=True: each affine body's block is
+    widened to the body plus the FEM vertices it touches (sgmas.h)."""
     pc = {"jacobi": 0, "mas": 1, 0: 0, 1: 1}[preconditioner]
     return PcgConfig(max_iter, rel_tol, abs_tol, int(use_preconditioned_norm), pc, abd_bodies, fem_offset,
-                     check_every, int(bool(initial_guess)))
+                     check_every, int(bool(initial_guess)), int(bool(body_patches)))
 
 
 class Context:

@@ -8,8 +8,8 @@ import sys
 PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))   # stiff-gipc_b200/
 REPO_ROOT = os.path.dirname(PKG_ROOT)
 LIB_PATH = os.path.join(PKG_ROOT, "libsgmas.so")
-SOURCES = ["capi.cu", "mas.cu", "pcg.cu", "pcg_persistent.cu", "convert.cu", "morton_noalloc.cu", "mtx.cu", "mlp.cu", "tune.cu", "abd.cu"]
-HEADERS = ["common.cuh", "ctx.hpp", "pcg_state.cuh", "mas_dev.cuh", "spmv_dev.cuh", "extra_dev.cuh"]
+SOURCES = ["capi.cu", "mas.cu", "pcg.cu", "pcg_persistent.cu", "convert.cu", "morton_noalloc.cu", "mtx.cu", "mlp.cu", "tune.cu", "abd.cu", "patch.cu"]
+HEADERS = ["common.cuh", "ctx.hpp", "pcg_state.cuh", "mas_dev.cuh", "spmv_dev.cuh", "extra_dev.cuh", "patch_dev.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 OBJ_DIR = os.path.join(PKG_ROOT, "_build")
