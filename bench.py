@@ -455,8 +455,12 @@ def run_sgmas(args):
 
 def other_configs(args, dev, stream):
     """The other single-system configs, measured briefly beside the headline:
-    config 1 (small tet grid: latency-bound) and config 3 (affine bodies on a
-    cloth sheet, MAS on the cloth + 12x12 ABD block-Jacobi on the bodies)."""
+    config 1 (small tet grid: latency-bound) and config 3 (200 affine bodies
+    on a 200 x 200 cloth sheet, 80,000 body-cloth barrier pairs drawn as in
+    the contact benchmark: kappa 1e5, d ~ U(0, dhat)).  Config 3 variants:
+    the reference's composition (MAS on the cloth + 12x12 block-Jacobi on the
+    bodies; bf16 / fp32 / fp64), block-Jacobi (3x3 + 12x12), and MAS + body
+    patches (bf16 / fp64 '+patches'), each capped at MAX_ITER iterations."""
     import torch
     import sgmas
     from sgmas import synth
@@ -476,15 +480,17 @@ def other_configs(args, dev, stream):
             nbs = sgmas.vert_neighbors(s.tets, s.n_verts)
         vals, rows, cols, b, pos = tdev(s.vals), tdev(s.rows), tdev(s.cols), tdev(s.b), tdev(s.pos)
         res = {"n_block_rows": int(s.n_verts), "n_blocks": int(len(s.rows)), "abd_bodies": nb}
-        for v in ("bf16", "fp32", "fp64", "jacobi"):
-            prec = "fp32" if v == "jacobi" else v
+        vs = ("bf16", "fp32", "fp64", "jacobi") + (("bf16+patches", "fp64+patches") if kind == "c3" else ())
+        for v in vs:
+            base = v.split("+")[0]
+            prec = "fp32" if base == "jacobi" else base
             ctx = sgmas.Context(dev.index or 0, bank=16, precision=prec)
             ctx.set_stream(stream.cuda_stream)
             pm, rm = ctx.morton_partition(pos)
             ctx.mas_init(N, *nbs, pm, rm)
             x = torch.zeros_like(b)
-            kw = dict(rel_tol=REL_TOL, max_iter=MAX_ITER, preconditioner="jacobi" if v == "jacobi" else "mas",
-                      abd_bodies=nb, fem_offset=off if v != "jacobi" else 0)
+            kw = dict(rel_tol=REL_TOL, max_iter=MAX_ITER, preconditioner="jacobi" if base == "jacobi" else "mas",
+                      abd_bodies=nb, fem_offset=off if base != "jacobi" else 0, body_patches=v.endswith("+patches"))
             try:
                 times = []
                 for i in range(warm + steps):
@@ -496,8 +502,11 @@ def other_configs(args, dev, stream):
                     e1.synchronize()
                     if i >= warm:
                         times.append(e0.elapsed_time(e1))
+                y = torch.zeros_like(b)
+                ctx.spmv(1.0, vals, rows, cols, s.n_verts, x, 0.0, y)
                 res[v] = {"ms": round(statistics.mean(times), 4), "iterations": rep["iterations"],
-                          "converged": bool(rep["converged"]), "loop_launches": rep["kernel_launches"]}
+                          "converged": bool(rep["converged"]), "loop_launches": rep["kernel_launches"],
+                          "rel_residual": float(torch.linalg.norm(b - y) / torch.linalg.norm(b))}
             except sgmas.SgmasError as e:
                 res[v] = {"error": str(e)}
             ctx.close()

@@ -66,12 +66,11 @@ typedef struct {
     int body_patches;            /* 0: the reference's composition (12x12 block-Jacobi on the bodies, MAS on the
                                     FEM range).  1 (needs preconditioner 1 and abd_bodies > 0, persistent form):
                                     each body's block is widened to a patch -- the body's 4 block rows plus the
-                                    FEM vertices coupled to it (each FEM vertex in the patch of the lowest-numbered
-                                    body it touches, at most 64) -- factored densely in FP64 and stored as
-                                    W = L^-1 in the MAS storage precision; z = MAS(r) + sum of the patches'
-                                    W^T W r.  For bodies resting on FEM surfaces with stiff barrier contact,
-                                    where the body-FEM couplings dominate.  The library's own; no reference
-                                    counterpart */
+                                    FEM vertices coupled to it (at most 64, the lowest ids; neighbouring patches
+                                    overlap) -- factored densely in FP64 and stored as W = L^-1 in FP32 (FP64
+                                    with the FP64 MAS); z = MAS(r) + sum of the patches' W^T W r.  For bodies
+                                    resting on FEM surfaces with stiff barrier contact, where the body-FEM
+                                    couplings dominate.  The library's own; no reference counterpart */
 } sgmas_pcg_config;
 
 typedef struct {

@@ -11,8 +11,8 @@ are this library's addition; the reference has none.
 A patch is body b's 12 unknowns plus the FEM vertices coupled to it (at
 most 64, the lowest ids; neighbouring patches overlap); its dense block is
 factored in FP64 (Cholesky, a non-positive pivot replaced by 1), W = L^-1 is
-rounded to the storage precision, and the apply adds W^T W r on the patch's
-unknowns.
+rounded to FP32 (FP64 beside the FP64 MAS), and the apply adds W^T W r on
+the patch's unknowns.
 """
 from __future__ import annotations
 
@@ -30,12 +30,9 @@ def patch_lists(rows, cols, n_bodies, fem_off, N):
 
 
 def _round(W, precision):
-    from oracle.oracle import bf16_round
     if precision == "fp64":
         return W
-    if precision == "bf16":
-        return bf16_round(W).astype(np.float64).reshape(W.shape)
-    return W.astype(np.float32).astype(np.float64)
+    return W.astype(np.float32).astype(np.float64)  # FP32 beside the BF16 / FP32 MAS
 
 
 class Patches:

@@ -12,15 +12,15 @@
 // coupled to it (at most kPatchMax, the lowest ids; patches of neighbouring
 // bodies overlap): its dense (12 + 3k) square block of A, factored in FP64
 // (Cholesky, non-positive pivots replaced by 1 as the MAS's factored inverse
-// does), stored as W = L^-1 in the MAS storage precision.  The apply adds
+// does), stored as W = L^-1 in FP32 (FP64 beside the FP64 MAS).  The apply adds
 // z += R^T W^T W R r per patch (R = restriction to the patch); the MAS still
 // covers every FEM vertex.  An FEM vertex's patch parts are summed in body
 // order through a per-row list of (body, local vertex) entries.  The
 // library's own addition: the reference has no such block.
 //
-// W is stored twice, packed: column-major (column j holds W[j..n-1][j]) for
-// y = W r with a thread per row, row-major (row i holds W[i][0..i]) for
-// z = W^T y with a thread per column, so both passes read W coalesced.
+// W is stored twice, packed: row-major (row i holds W[i][0..i]) for y = W r
+// with a warp per row, column-major (column j holds W[j..n-1][j]) for
+// z = W^T y with a warp per column, so both passes read W coalesced.
 #include <algorithm>
 
 #include "../../include/sgmas.h"
@@ -274,9 +274,6 @@ int build_t(sgmas_context* c, int nbodies, int fem_off) {
 // rows 0 .. 4 nbodies - 1, the MAS's FEM vertices from fem_off) on the block
 // CSR of the current solve, in the context's MAS storage precision.
 int patch_build(sgmas_context* c, int nbodies, int fem_off) {
-    switch (c->precision) {
-        case SGMAS_MAS_BF16: return build_t<Fact<__nv_bfloat16>>(c, nbodies, fem_off);
-        case SGMAS_MAS_FP64: return build_t<double>(c, nbodies, fem_off);
-        default: return build_t<Fact<float>>(c, nbodies, fem_off);
-    }
+    if (c->precision == SGMAS_MAS_FP64) return build_t<double>(c, nbodies, fem_off);
+    return build_t<Fact<float>>(c, nbodies, fem_off);  // FP32 W beside the BF16 / FP32 MAS
 }

@@ -40,37 +40,49 @@ __device__ __forceinline__ size_t patch_dof(const PatchView& P, int b, int fem_o
 
 // z_patch = W^T (W r_patch) for body b, by the whole CTA (rl, yl: shared
 // scratch of 12 + 3 kPatchMax entries each).  y_i = sum_{j <= i} W_ij r_j
-// (j ascending, one thread per row), z_j = sum_{i >= j} W_ij y_i (i
-// ascending, one thread per column), each an fma chain in Acc.  The body's
-// rows get z in z_body (no other patch covers them), its FEM vertices' part
-// goes to the patch's slice of P.zs (summed per row by patch_z); adds this
-// thread's part of r.z over the patch and of r.r over the body rows.
+// with a warp per row (row i of the row-major copy, contiguous), z_j =
+// sum_{i >= j} W_ij y_i with a warp per column (column j of the
+// column-major copy, contiguous): lane l sums the terms l, l + 32, ... as an
+// fma chain in Acc, then an xor-shuffle tree (every lane gets the same
+// bits).  The body's rows get z in z_body (no other patch covers them), its
+// FEM vertices' part goes to the patch's slice of P.zs (summed per row by
+// patch_z); adds this thread's part of r.z over the patch and of r.r over
+// the body rows.
 template <typename S, typename Acc>
 __device__ __forceinline__ void patch_apply_cta(const PatchView& P, int b, int fem_off, const double* r, double* z_body,
                                                 Acc* rl, Acc* yl, double& rz, double& rr) {
     const int k = P.info[b].x, n = 12 + 3 * k;
     const S* wc = (const S*)P.wcol + (size_t)b * patch_packed(kPatchMax);
     const S* wr = (const S*)P.wrow + (size_t)b * patch_packed(kPatchMax);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int i = threadIdx.x; i < n; i += blockDim.x) rl[i] = (Acc)r[patch_dof(P, b, fem_off, i)];
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int i = warp; i < n; i += nw) {
+        const S* row = wr + packed_lower(i, 0);
         Acc s = 0;
-        for (int j = 0; j <= i; ++j) s = fma_acc(Store<S>::to_acc(wc[packed_col(n, i, j)]), rl[j], s);
-        yl[i] = s;
+        for (int j = lane; j <= i; j += 32) s = fma_acc(Store<S>::to_acc(row[j]), rl[j], s);
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) yl[i] = s;
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    for (int j = warp; j < n; j += nw) {
+        const S* col = wc + packed_col(n, j, j);  // W[j..n-1][j]
         Acc s = 0;
-        for (int i = j; i < n; ++i) s = fma_acc(Store<S>::to_acc(wr[packed_lower(i, j)]), yl[i], s);
-        const size_t d = patch_dof(P, b, fem_off, j);
-        const double zv = (double)s, rv = r[d];
-        if (j < 12) {
-            z_body[d] = zv;
-            rr += rv * rv;
-        } else {
-            P.zs[3 * kPatchMax * (size_t)b + (j - 12)] = zv;
+        for (int i = j + lane; i < n; i += 32) s = fma_acc(Store<S>::to_acc(col[i - j]), yl[i], s);
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            const size_t d = patch_dof(P, b, fem_off, j);
+            const double zv = (double)s, rv = r[d];
+            if (j < 12) {
+                z_body[d] = zv;
+                rr += rv * rv;
+            } else {
+                P.zs[3 * kPatchMax * (size_t)b + (j - 12)] = zv;
+            }
+            rz += rv * zv;
         }
-        rz += rv * zv;
     }
     __syncthreads();  // rl / yl are free again
 }

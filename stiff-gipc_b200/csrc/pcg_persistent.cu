@@ -388,10 +388,11 @@ __device__ __forceinline__ double spmv_cta(const PArgs& a, int4 ci, const int4* 
     return dot;
 }
 
-// storage of the body patches for each MAS storage: factored in every
-// precision (the explicit FP32 MAS pairs with FP32-factored patches)
-template <typename S> struct PatchS { using T = S; };
-template <> struct PatchS<float> { using T = Fact<float>; };
+// storage of the body patches for each MAS storage: factored W in FP32, or
+// in FP64 with the FP64 MAS (BF16 rounding of W loses the stiff contact
+// directions the patches exist for: measured, it did not converge)
+template <typename S> struct PatchS { using T = Fact<float>; };
+template <> struct PatchS<double> { using T = double; };
 
 // TG: some level-0 / level-1 tiles are read from global memory (a.t0g, a.t1g)
 template <int B, typename S, typename Acc, bool TG>
