@@ -141,6 +141,34 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return r;
 }
 
+// exclusive block-wide scan of one int per thread (1024 threads); returns the
+// prefix, *total receives the sum
+__device__ __forceinline__ int block_scan1024(int v, int* sh, int* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+    #pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int y = sh[lane];
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += t;
+        }
+        sh[32 + lane] = y;
+    }
+    __syncthreads();
+    const int pre = (w ? sh[32 + w - 1] : 0) + x - v;
+    *total = sh[63];
+    __syncthreads();
+    return pre;
+}
+
 // Last-CTA-done grid reduction (no waiting): every CTA writes its partial,
 // the CTA that takes the last ticket sums all partials in blockIdx order.
 // Returns true in thread 0 of the last CTA, with *out = total.

@@ -45,26 +45,21 @@ __global__ void k_bsr_count(int nb, int nrows, const int* __restrict__ rows, con
     if (k == 0 || rows[k - 1] != i) first[i] = k;
 }
 
-// exclusive scan of even-rounded row counts (one CTA)
-__global__ void k_row_scan(int n, const int* __restrict__ cnt, int* row_ptr) {
-    __shared__ int sh[1024];
+// exclusive scan of even-rounded row counts (one CTA of 1024 threads: a
+// warp-shuffle scan per chunk of 1024 rows, two CTA barriers per chunk)
+__global__ void __launch_bounds__(1024) k_row_scan(int n, const int* __restrict__ cnt, int* row_ptr) {
+    __shared__ int sh[64];
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (int base = 0; base < n; base += 1024) {
         const int i = base + threadIdx.x;
         const int v = i < n ? ((cnt[i] + 1) & ~1) : 0;
-        sh[threadIdx.x] = v;
+        int tot;
+        const int pre = block_scan1024(v, sh, &tot);
+        if (i < n) row_ptr[i] = carry + pre;
         __syncthreads();
-        for (int o = 1; o < 1024; o <<= 1) {
-            const int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
-            __syncthreads();
-            sh[threadIdx.x] += t;
-            __syncthreads();
-        }
-        if (i < n) row_ptr[i] = carry + sh[threadIdx.x] - v;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry += sh[1023];
+        if (threadIdx.x == 0) carry += tot;
         __syncthreads();
     }
     if (threadIdx.x == 0) row_ptr[n] = carry;
@@ -116,34 +111,29 @@ __global__ void k_bsr_sort_lower(int nrows, const int* __restrict__ row_ptr, con
 // Split rows into long (more than kLongRow entries: one warp each) and short
 // (8 lanes each), both lists in row order; one CTA.
 constexpr int kLongRow = 32;
-__global__ void k_row_split(int n, const int* __restrict__ row_ptr, int* row_list, int* n_long) {
-    __shared__ int sh[1024];
+__global__ void __launch_bounds__(1024) k_row_split(int n, const int* __restrict__ row_ptr, int* row_list,
+                                                    int* n_long) {
+    __shared__ int sh[64];
     __shared__ int carry, total_long;
     if (threadIdx.x == 0) { carry = 0; total_long = 0; }
     __syncthreads();
     // pass 1: count long rows
     int cnt = 0;
     for (int i = threadIdx.x; i < n; i += 1024) cnt += (row_ptr[i + 1] - row_ptr[i]) > kLongRow;
-    atomicAdd(&total_long, cnt);
+    if (cnt) atomicAdd(&total_long, cnt);
     __syncthreads();
     const int nl = total_long;
     for (int base = 0; base < n; base += 1024) {
         const int i = base + threadIdx.x;
         const int v = i < n ? ((row_ptr[i + 1] - row_ptr[i]) > kLongRow) : 0;
-        sh[threadIdx.x] = v;
-        __syncthreads();
-        for (int o = 1; o < 1024; o <<= 1) {
-            const int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
-            __syncthreads();
-            sh[threadIdx.x] += t;
-            __syncthreads();
-        }
+        int tot;
+        const int pre = block_scan1024(v, sh, &tot);
         if (i < n) {
-            const int before = carry + sh[threadIdx.x] - v;  // long rows before i
+            const int before = carry + pre;  // long rows before i
             row_list[v ? before : nl + (i - before)] = i;
         }
         __syncthreads();
-        if (threadIdx.x == 1023) carry += sh[1023];
+        if (threadIdx.x == 0) carry += tot;
         __syncthreads();
     }
     if (threadIdx.x == 0) *n_long = nl;

@@ -835,70 +835,54 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
 constexpr int kLongRowP = 32;
 constexpr int kRowCost = 4;
 
-// exclusive block-wide scan of one int per thread (1024 threads); returns the
-// prefix, *total receives the sum
-__device__ __forceinline__ int block_scan1024(int v, int* sh, int* total) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int x = v;
-    #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += t;
-    }
-    if (lane == 31) sh[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        int y = sh[lane];
-        #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, y, o);
-            if (lane >= o) y += t;
-        }
-        sh[32 + lane] = y;
-    }
-    __syncthreads();
-    const int pre = (w ? sh[32 + w - 1] : 0) + x - v;
-    *total = sh[63];
-    __syncthreads();
-    return pre;
-}
-
-// row order + prefix sums of the balance cost and of the stored blocks along
-// it (cpre, epre: nrows + 1 entries); one CTA of 1024 threads
-__global__ void __launch_bounds__(1024) k_row_plan(int nrows, int mas, int fem_off, int N, int Mm,
-                                                   const int* __restrict__ part_map, const int* __restrict__ row_ptr,
-                                                   int* row_order, int* cpre, int* epre) {
+// row order (one CTA of 1024 threads): rows [0, fem_off) and [fem_off + N,
+// nrows) in place, the MAS rows by slot
+__global__ void __launch_bounds__(1024) k_row_order(int nrows, int mas, int fem_off, int N, int Mm,
+                                                    const int* __restrict__ part_map, int* row_order) {
     __shared__ int sh[64];
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    // order: rows [0, fem_off) and [fem_off + N, nrows) in place, MAS rows by slot
     if (!mas) {
         for (int i = threadIdx.x; i < nrows; i += 1024) row_order[i] = i;
-    } else {
-        for (int i = threadIdx.x; i < fem_off; i += 1024) row_order[i] = i;
-        for (int i = fem_off + N + threadIdx.x; i < nrows; i += 1024) row_order[i] = i;
-        for (int base = 0; base < Mm; base += 1024) {
-            const int s = base + threadIdx.x;
-            const int v = s < Mm ? part_map[s] : -1;
-            int tot;
-            const int pre = block_scan1024(v >= 0, sh, &tot);
-            if (v >= 0) row_order[fem_off + carry + pre] = fem_off + v;
-            __syncthreads();
-            if (threadIdx.x == 0) carry += tot;
-            __syncthreads();
-        }
+        return;
     }
-    __syncthreads();
-    // prefix sums along the order, a contiguous chunk per thread
+    for (int i = threadIdx.x; i < fem_off; i += 1024) row_order[i] = i;
+    for (int i = fem_off + N + threadIdx.x; i < nrows; i += 1024) row_order[i] = i;
+    for (int base = 0; base < Mm; base += 1024) {
+        const int s = base + threadIdx.x;
+        const int v = s < Mm ? part_map[s] : -1;
+        int tot;
+        const int pre = block_scan1024(v >= 0, sh, &tot);
+        if (v >= 0) row_order[fem_off + carry + pre] = fem_off + v;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += tot;
+        __syncthreads();
+    }
+}
+
+// stored blocks of the row at each position of the order (into cpre, scratch)
+__global__ void k_order_len(int nrows, const int* __restrict__ row_order, const int* __restrict__ row_ptr,
+                            int* len_at) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrows) return;
+    const int r = row_order[i];
+    len_at[i] = row_ptr[r + 1] - row_ptr[r];
+}
+
+// prefix sums along the order (one CTA of 1024 threads, a contiguous chunk
+// per thread): cpre of the balance cost (blocks + kRowCost per row), epre of
+// max(blocks, 1) (room in the halo lists: a row is in its own halo); cpre
+// holds the row lengths on entry, each thread reads its chunk before writing it
+__global__ void __launch_bounds__(1024) k_order_prefix(int nrows, int* cpre, int* epre) {
+    __shared__ int sh[64];
     const int chunk = (nrows + 1023) / 1024;
     const int b0 = min(nrows, (int)threadIdx.x * chunk), b1 = min(nrows, b0 + chunk);
     int cs = 0, es = 0;
     for (int i = b0; i < b1; ++i) {
-        const int r = row_order[i];
-        const int len = row_ptr[r + 1] - row_ptr[r];
+        const int len = cpre[i];
         cs += len + kRowCost;
-        es += max(len, 1);  // room in the halo list for every row (a row is in its own halo)
+        es += max(len, 1);
     }
     int ct, et;
     const int cp = block_scan1024(cs, sh, &ct);
@@ -906,8 +890,7 @@ __global__ void __launch_bounds__(1024) k_row_plan(int nrows, int mas, int fem_o
     cs = cp;
     es = ep;
     for (int i = b0; i < b1; ++i) {
-        const int r = row_order[i];
-        const int len = row_ptr[r + 1] - row_ptr[r];
+        const int len = cpre[i];
         cpre[i] = cs;
         epre[i] = es;
         cs += len + kRowCost;
@@ -1100,8 +1083,10 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
             return SGMAS_ERR_CUDA;
         int* cpre = c->d_cpre;
         int* epre = c->d_cpre + nrows + 1;
-        k_row_plan<<<1, 1024, 0, s>>>(nrows, a.precond == 1, a.precond == 1 ? a.ex.fem_off : 0, a.N, a.Mm,
-                                      a.part_map, a.A.row_ptr, c->d_row_order, cpre, epre);
+        k_row_order<<<1, 1024, 0, s>>>(nrows, a.precond == 1, a.precond == 1 ? a.ex.fem_off : 0, a.N, a.Mm,
+                                       a.part_map, c->d_row_order);
+        k_order_len<<<(nrows + 255) / 256, 256, 0, s>>>(nrows, c->d_row_order, a.A.row_ptr, cpre);
+        k_order_prefix<<<1, 1024, 0, s>>>(nrows, cpre, epre);
         SG_CUDA(c, cudaMemsetAsync(c->d_plan_stats, 0, 2 * sizeof(int), s));
         const size_t plan_smem = 2 * (size_t)((nrows + 31) / 32) * sizeof(unsigned);
         if (plan_smem + 1024 > (size_t)max_smem) return 1;  // (the kernel's static shared memory is < 1 KB)
@@ -1109,7 +1094,7 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
             SG_CUDA(c, cudaFuncSetAttribute(k_spmv_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan_smem));
         k_spmv_plan<<<G, 512, plan_smem, s>>>(nrows, c->d_row_order, cpre, epre, a.A.row_ptr, a.A.cols, c->d_lcols,
                                               c->d_halo, c->d_cinfo, c->d_udesc_c, c->d_plan_stats);
-        c->build_launches += 2;
+        c->build_launches += 4;
         SG_CUDA(c, cudaGetLastError());
         int st[2] = {0, 0};  // largest halo, most units of a CTA
         SG_CUDA(c, cudaMemcpyAsync(st, c->d_plan_stats, sizeof(st), cudaMemcpyDeviceToHost, s));
