@@ -517,7 +517,8 @@ def other_configs(args, dev, stream):
     return out
 
 
-def learned_c4(dev, stream, scale, n_train, n_eval, epochs, steps_per_seq=20, batch_banks=256, keep=1.0):
+def learned_c4(dev, stream, scale, n_train, n_eval, epochs, steps_per_seq=20, batch_banks=256, keep=1.0,
+               anorm_epochs=2, anorm_every=2):
     """Config 4, the learned start guess, on drop sequences (sgmas.sequence:
     the contact scene's two tet blocks, the top one released from U(0.01,
     0.1) m, one linearly implicit Euler step per system).  Training data are
@@ -529,8 +530,11 @@ def learned_c4(dev, stream, scale, n_train, n_eval, epochs, steps_per_seq=20, ba
     MAS-PCG from x0 = 0, BF16 with the learned start (sgmas_mlp_warm_start:
     Galerkin combination of previous step, lumped step, network step and
     coarse term), and the same start with a zero network (previous step +
-    lumped step only: what the network adds).  The trajectory follows the
-    FP64 solution.  Each context solves the first system once untimed."""
+    lumped step only: what the network adds).  A fifth arm starts from the
+    same network fine-tuned for anorm_epochs passes on the energy norm of
+    its start error (learned.train_anorm) over every anorm_every-th training
+    system.  The trajectory follows the FP64 solution.  Each context solves
+    the first system once untimed."""
     import torch
     import sgmas
     from sgmas import learned
@@ -563,7 +567,8 @@ def learned_c4(dev, stream, scale, n_train, n_eval, epochs, steps_per_seq=20, ba
             vals, rows, cols, b = sc.system()
             x = torch.zeros_like(b)
             ctx.pcg_solve(vals, rows, cols, sc.n, b, x, rel_tol=1e-6, max_iter=MAX_ITER)
-            ts.add(ctx, vals, rows, cols, sc.n, b, x, prev=sc.prev, part_map=pm)
+            keep_sys = anorm_epochs > 0 and n_solves % anorm_every == 0
+            ts.add(ctx, vals, rows, cols, sc.n, b, x, prev=sc.prev, part_map=pm, keep_system=keep_sys)
             sc.advance(x)
             n_solves += 1
         ctx.close()
@@ -578,8 +583,15 @@ def learned_c4(dev, stream, scale, n_train, n_eval, epochs, steps_per_seq=20, ba
     torch.cuda.synchronize()
     train_s = time.time() - t0
     P = trainer.mlp_get_params()
+    t0 = time.time()
+    ahist = learned.train_anorm(trainer, ts, epochs=anorm_epochs, lr=2e-4, seed=0) if anorm_epochs > 0 else []
+    torch.cuda.synchronize()
+    anorm_s = time.time() - t0
+    PA = trainer.mlp_get_params()
     trainer.close()
-    arms = ("plain_fp64", "plain_bf16", "learned_bf16", "zero_net_bf16")
+    n_sys = len(ts.systems)
+    ts.systems.clear()
+    arms = ("plain_fp64", "plain_bf16", "learned_bf16", "zero_net_bf16") + (("anorm_bf16",) if ahist else ())
     rec = {a: {"ms": [], "it": []} for a in arms}
     rejected = 0
     coefs = []
@@ -589,9 +601,13 @@ def learned_c4(dev, stream, scale, n_train, n_eval, epochs, steps_per_seq=20, ba
         c16, _ = scene_ctx(sc, "bf16")
         cl, _ = scene_ctx(sc, "bf16")
         cz, _ = scene_ctx(sc, "bf16")
+        ca = scene_ctx(sc, "bf16")[0] if ahist else None
         sc.ctx = c64
         cl.mlp_set_params(P)
         cz.mlp_set_params(np.zeros(len(P), np.float32))
+        if ca is not None:
+            ca.mlp_set_params(PA)
+        warm = [("learned_bf16", cl), ("zero_net_bf16", cz)] + ([("anorm_bf16", ca)] if ca is not None else [])
         for k in range(steps_per_seq):
             vals, rows, cols, b = sc.system()
             args_ = (vals, rows, cols, sc.n, b)
@@ -603,7 +619,7 @@ def learned_c4(dev, stream, scale, n_train, n_eval, epochs, steps_per_seq=20, ba
                 x16 = torch.zeros_like(b)
                 r16, ms16 = timed(lambda: c16.pcg_solve(*args_, x16, **kw))
                 res = {}
-                for name, cc in (("learned_bf16", cl), ("zero_net_bf16", cz)):
+                for name, cc in warm:
                     x0 = torch.zeros_like(b)
 
                     def go(cc=cc, x0=x0):
@@ -618,7 +634,7 @@ def learned_c4(dev, stream, scale, n_train, n_eval, epochs, steps_per_seq=20, ba
                     rejected += r["x0_rejected"]
             coefs.append(cl.mlp_warm_start(*args_, torch.zeros_like(b), prev=sc.prev, coef=True).tolist())
             sc.advance(x64)
-        for cc in (c64, c16, cl, cz):
+        for _, cc in [("plain_fp64", c64), ("plain_bf16", c16)] + warm:
             cc.close()
     mean = lambda v: round(float(np.mean(v)), 3)
     summ = {a: {"ms": mean(rec[a]["ms"]), "iterations": mean(rec[a]["it"])} for a in arms}
@@ -629,6 +645,12 @@ def learned_c4(dev, stream, scale, n_train, n_eval, epochs, steps_per_seq=20, ba
             "speedup_learned_bf16_vs_plain_fp64": round(summ["plain_fp64"]["ms"] / summ["learned_bf16"]["ms"], 3),
             "speedup_plain_bf16_vs_plain_fp64": round(summ["plain_fp64"]["ms"] / summ["plain_bf16"]["ms"], 3),
             "network_gain_vs_zero_net": round(summ["zero_net_bf16"]["ms"] / summ["learned_bf16"]["ms"], 3),
+            "anorm_gain_vs_zero_net": (round(summ["zero_net_bf16"]["ms"] / summ["anorm_bf16"]["ms"], 3)
+                                       if ahist else None),
+            "anorm_training": ({"systems": n_sys, "epochs": anorm_epochs, "s": round(anorm_s, 1),
+                                "energy_loss_first_epoch": round(float(np.mean([h[1] for h in ahist[:n_sys]])), 5),
+                                "energy_loss_last_epoch": round(float(np.mean([h[1] for h in ahist[-n_sys:]])), 5)}
+                               if ahist else None),
             "learned_rejected": rejected, "mean_coef_prev_lumped_step_coarse": np.round(np.mean(coefs, 0), 4).tolist(),
             "training": {"solves": n_solves, "rows": int(ts.X.shape[0]), "epochs": epochs, "data_s": round(data_s, 1),
                          "train_s": round(train_s, 1), "loss_first": round(hist[0][1], 5) if hist else None,

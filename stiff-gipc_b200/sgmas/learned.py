@@ -7,6 +7,12 @@
   subdomain mean.
 * train: minibatch Adam on the GPU (sgmas_mlp_train_step), batches of whole
   subdomains drawn by a seeded permutation each epoch.
+* train_anorm: fine-tuning on the energy norm of the start error instead
+  of its per-vertex squares: for a stored system, L = (x0 - dx)^T A
+  (x0 - dx) / (dx^T b) with x0 = u + s y (lumped step plus the network's
+  prediction); its gradient needs A (x0 - dx), one SpMV of the library per
+  step (sgmas_spmv), and enters the FP32 training kernels through a
+  pseudo-target T' = y - (n / 2) dL/dy.
 * warm_start: the start guess of a new system (sgmas_mlp_warm_start): the
   A-norm-best combination of the previous step, the lumped step and the
   network's step and coarse term, to be passed to sgmas_pcg_solve with
@@ -48,16 +54,24 @@ class TrainingSet:
         self._X, self._T, self._M, self._cnt = [], [], [], []
         self.X = self.T = self.M = None
         self.counts = None
+        self.systems = []
 
-    def add(self, ctx, vals, rows, cols, n_block_rows, b, dx, prev=None, part_map=None, fem_offset=0):
+    def add(self, ctx, vals, rows, cols, n_block_rows, b, dx, prev=None, part_map=None, fem_offset=0,
+            keep_system=False):
         """Features and targets (dx / s_y) of one solved system, a `keep`
-        fraction of its subdomains (seeded), appended."""
+        fraction of its subdomains (seeded), appended.  keep_system: also
+        keep the whole system (matrix, b, dx, all slots) for train_anorm."""
         torch = self.torch
         Mm = ctx.part_map_size
         X = torch.empty(Mm * N_IN, dtype=torch.float32, device=self.dev)
         M = torch.empty(Mm, dtype=torch.float32, device=self.dev)
         T = torch.empty(Mm * 3, dtype=torch.float32, device=self.dev)
-        ctx.mlp_features(vals, rows, cols, n_block_rows, b, X, M, prev=prev, dx=dx, T=T, fem_offset=fem_offset)
+        sc = ctx.mlp_features(vals, rows, cols, n_block_rows, b, X, M, prev=prev, dx=dx, T=T, fem_offset=fem_offset)
+        if keep_system:
+            pm = torch.as_tensor(np.asarray(part_map, np.int64), device=self.dev)
+            self.systems.append(dict(vals=vals.clone(), rows=rows.clone(), cols=cols.clone(), n=n_block_rows,
+                                     b=b.clone(), dx=dx.clone(), X=X.clone(), M=M.clone(), T=T.clone(), s=sc[0],
+                                     part_map=pm, fem_offset=fem_offset))
         nb = Mm // BANK
         banks = np.arange(nb)
         if self.keep < 1.0:
@@ -110,6 +124,55 @@ def train(ctx, ts, epochs=4, batch_banks=512, lr=1e-3, seed=0, lr_final=1e-4, lo
                                       int(rows.numel()), 1.0 / n_valid, float(lr * decay ** step), want_loss=want)
             if want:
                 hist.append((step, loss))
+            step += 1
+    return hist
+
+
+def anorm_loss_grad(ctx, sysd):
+    """(L, y, dL/dy) of one stored system for the current parameters:
+    y [Mm, 3] the combined prediction (step + subdomain mean of the coarse
+    term, as the training kernel forms it), L = e^T A e / (dx^T b) with
+    e = s (y - T) on the MAS rows, dL/dy = 2 s (A e) / (dx^T b) per slot."""
+    import torch
+    X, M, T, s = sysd["X"], sysd["M"], sysd["T"], sysd["s"]
+    Mm = M.numel()
+    Y = torch.empty(Mm * N_OUT, dtype=torch.float32, device=X.device)
+    ctx.mlp_forward(X, Mm, Y, bf16=False)
+    Y = Y.view(Mm, N_OUT)
+    Mb = M.view(-1, BANK)
+    cnt = Mb.sum(1).clamp(min=1.0)
+    cm = (Y[:, 3:6].view(-1, BANK, 3) * Mb[..., None]).sum(1) / cnt[:, None]
+    y = Y[:, 0:3] + cm.repeat_interleave(BANK, 0)
+    valid = sysd["part_map"] >= 0
+    rows_of = sysd["fem_offset"] + sysd["part_map"][valid]
+    n = sysd["n"]
+    e = torch.zeros(n, 3, dtype=torch.float64, device=X.device)
+    e[rows_of] = s * (y[valid].double() - T.view(Mm, 3)[valid].double())
+    g = torch.zeros_like(e)
+    ctx.spmv(1.0, sysd["vals"], sysd["rows"], sysd["cols"], n, e.view(-1), 0.0, g.view(-1))
+    lam = 1.0 / float(torch.dot(sysd["dx"], sysd["b"]))
+    L = lam * float(torch.dot(e.view(-1), g.view(-1)))
+    dLdy = torch.zeros(Mm, 3, dtype=torch.float64, device=X.device)
+    dLdy[valid] = 2.0 * lam * s * g[rows_of]
+    return L, y, dLdy
+
+
+def train_anorm(ctx, ts, epochs=2, lr=2e-4, seed=0):
+    """Fine-tune on the energy norm of the start error over the stored
+    systems (ts.systems), one system per Adam step, seeded order.  Returns
+    [(step, L)]."""
+    rng = np.random.default_rng(seed)
+    hist = []
+    step = 0
+    for _ in range(epochs):
+        for q in rng.permutation(len(ts.systems)):
+            sysd = ts.systems[q]
+            L, y, dLdy = anorm_loss_grad(ctx, sysd)
+            n_valid = float(sysd["M"].sum())
+            Tp = (y.double() - dLdy * (n_valid / 2.0)).float().contiguous()
+            ctx.mlp_train_step(sysd["X"], Tp.view(-1), sysd["M"], int(sysd["M"].numel()), 1.0 / n_valid, float(lr),
+                               want_loss=False)
+            hist.append((step, L))
             step += 1
     return hist
 

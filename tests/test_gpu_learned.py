@@ -278,3 +278,50 @@ def test_learned_start_saves_iterations_on_held_out_steps(sgm):
     print(f"mean iterations: plain {np.mean(it_plain):.1f}, learned {np.mean(it_learn):.1f}, "
           f"zero network {np.mean(it_zero):.1f}")
     assert np.mean(it_learn) <= 0.85 * np.mean(it_plain), (it_learn, it_plain)
+
+
+def test_energy_fine_tuning(sgm):
+    """learned.anorm_loss_grad: L = e^T A e / (dx^T b) for the start error
+    e = s (y - T) on the MAS rows, against a scipy product of the full
+    matrix; learned.train_anorm lowers the mean of L over its systems."""
+    import types
+    from sgmas import learned, synth
+    from sgmas.sequence import DropScene
+
+    sc = DropScene(seed=3, scale=0.25, device="cuda")
+    ctx = sgm.Context(0, bank=16, precision="bf16")
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    pm, rm = ctx.morton_partition(torch.as_tensor(sc.X, device="cuda"))
+    ctx.mas_init(sc.n, *sgm.vert_neighbors(sc.tets, sc.n), pm, rm)
+    ctx.mas_set_contacts(sc.t_pairs, len(sc.pairs))
+    sc.ctx = ctx
+    ts = learned.TrainingSet("cuda")
+    for _ in range(10):
+        vals, rows, cols, b = sc.system()
+        x = torch.zeros_like(b)
+        ctx.pcg_solve(vals, rows, cols, sc.n, b, x, rel_tol=1e-8)
+        ts.add(ctx, vals, rows, cols, sc.n, b, x, prev=sc.prev, part_map=pm, keep_system=True)
+        sc.advance(x)
+    ts.finalize()
+    ctx.mlp_set_params(learned.init_params(0))
+    learned.train(ctx, ts, epochs=10, batch_banks=64, lr=2e-3, lr_final=2e-4, seed=0)
+    sysd = ts.systems[-1]
+    L, y, g = learned.anorm_loss_grad(ctx, sysd)
+    A = synth.full_matrix(types.SimpleNamespace(vals=sysd["vals"].cpu().numpy(), rows=sysd["rows"].cpu().numpy(),
+                                                cols=sysd["cols"].cpu().numpy(), n_verts=sysd["n"]))
+    Mm = ctx.part_map_size
+    pmn = np.asarray(pm)[:Mm]
+    ok = pmn >= 0
+    e = np.zeros((sysd["n"], 3))
+    e[pmn[ok]] = sysd["s"] * (y.cpu().numpy()[ok].astype(np.float64) - sysd["T"].view(Mm, 3).cpu().numpy()[ok])
+    e = e.ravel()
+    dx, b = sysd["dx"].cpu().numpy(), sysd["b"].cpu().numpy()
+    L_ref = float(e @ (A @ e)) / float(dx @ b)
+    assert abs(L - L_ref) <= 1e-9 * abs(L_ref), (L, L_ref)
+    g_ref = 2.0 * sysd["s"] * (A @ e).reshape(-1, 3)[pmn[ok]] / float(dx @ b)
+    np.testing.assert_allclose(g.cpu().numpy()[ok], g_ref, rtol=1e-9, atol=1e-12 * np.abs(g_ref).max())
+    before = np.mean([learned.anorm_loss_grad(ctx, q)[0] for q in ts.systems])
+    learned.train_anorm(ctx, ts, epochs=4, lr=2e-4, seed=0)
+    after = np.mean([learned.anorm_loss_grad(ctx, q)[0] for q in ts.systems])
+    assert np.isfinite(after) and after < before, (before, after)
+    ctx.close()
