@@ -111,15 +111,23 @@ __device__ __forceinline__ void stamp(const PArgs& a, int k, int slot) {
 // come: the host's fault injection for the timeout path.)
 // acc (thread 0 of each CTA, profiling only): += work and wait cycles of this
 // barrier slot; t_rel carries the previous release time.
+// The split form: grid_arrive by one thread, after a CTA or named barrier that
+// orders the CTA's writes before it; grid_barrier(..., arrive = false) then
+// completes the next barrier without arriving again.
+__device__ __forceinline__ void grid_arrive(unsigned* count) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
+}
+
 __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned& epoch, int* err, int limit, int phantom,
-                                             unsigned long long* acc = nullptr, long long* t_rel = nullptr) {
+                                             unsigned long long* acc = nullptr, long long* t_rel = nullptr,
+                                             bool arrive = true) {
     __shared__ int ok_sh;
     __syncthreads();
     if (threadIdx.x == 0) {
         const long long t_arrive = acc ? clock64() : 0;
         epoch += 1u;
         const unsigned target = epoch * (gridDim.x + (unsigned)phantom);
-        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
+        if (arrive) grid_arrive(count);
         int ok = 0;
         for (int it = 0; it < limit; ++it) {
             unsigned v;
@@ -139,13 +147,19 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, unsigned& epoch, i
     return ok_sh != 0;
 }
 
-// sum of the grid's partials in CTA order (every CTA gets the same value)
-__device__ __forceinline__ double sum_partials(const double* part, double* sh) {
-    double s = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += kPT) s += part[i];
-    s = block_sum<kPT>(s, sh);
+// sum of the grid's partials (every thread of every CTA gets the same value):
+// warp 0 reads them lane-strided and folds them with an xor butterfly, whose
+// additions pair the same operands in every lane and every CTA; one warp per
+// CTA keeps the L2 requests to the shared partial lines few
+__device__ __forceinline__ double sum_partials(const double* part) {
     __shared__ double out;
-    if (threadIdx.x == 0) out = s;
+    if (threadIdx.x < 32) {
+        double s = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) s += __ldcg(part + i);
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) out = s;
+    }
     __syncthreads();
     const double v = out;
     __syncthreads();
@@ -153,32 +167,43 @@ __device__ __forceinline__ double sum_partials(const double* part, double* sh) {
 }
 
 // both sums of the end of an iteration in one pass
-__device__ __forceinline__ void sum_partials2(const double* pa, const double* pb, double* sh, double& va,
-                                              double& vb) {
-    double s0 = 0.0, s1 = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += kPT) { s0 += pa[i]; s1 += pb[i]; }
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s0 += __shfl_down_sync(0xffffffffu, s0, o);
-        s1 += __shfl_down_sync(0xffffffffu, s1, o);
-    }
+__device__ __forceinline__ void sum_partials2(const double* pa, const double* pb, double& va, double& vb) {
     __shared__ double out2[2];
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { sh[w] = s0; sh[16 + w] = s1; }
-    __syncthreads();
     if (threadIdx.x < 32) {
-        double r0 = threadIdx.x < kPT / 32 ? sh[threadIdx.x] : 0.0;
-        double r1 = threadIdx.x < kPT / 32 ? sh[16 + threadIdx.x] : 0.0;
+        double s0 = 0.0, s1 = 0.0;
+        for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) { s0 += __ldcg(pa + i); s1 += __ldcg(pb + i); }
         #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            r0 += __shfl_down_sync(0xffffffffu, r0, o);
-            r1 += __shfl_down_sync(0xffffffffu, r1, o);
+            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
         }
-        if (threadIdx.x == 0) { out2[0] = r0; out2[1] = r1; }
+        if (threadIdx.x == 0) { out2[0] = s0; out2[1] = s1; }
     }
     __syncthreads();
     va = out2[0];
     vb = out2[1];
+    __syncthreads();
+}
+
+// two block sums in one pass (valid in thread 0)
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sh[w] = a; sh[16 + w] = b; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        a = threadIdx.x < kPT / 32 ? sh[threadIdx.x] : 0.0;
+        b = threadIdx.x < kPT / 32 ? sh[16 + threadIdx.x] : 0.0;
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+    }
     __syncthreads();
 }
 
@@ -217,8 +242,7 @@ __device__ void phase_jacobi(const PArgs& a, int mode, double alpha, const doubl
         for (int d = 0; d < 3; ++d) a.z[3 * (size_t)i + d] = zv[d];
         rz += rv[0] * zv[0] + rv[1] * zv[1] + rv[2] * zv[2];
     }
-    rz = block_sum<kPT>(rz, sh);
-    rr = block_sum<kPT>(rr, sh);
+    block_sum2(rz, rr, sh);
     if (threadIdx.x == 0) { part_rz[blockIdx.x] = rz; part_rr[blockIdx.x] = rr; }
 }
 
@@ -366,15 +390,31 @@ __device__ __forceinline__ bool levels_c(const PArgs& a, const Anc& anc, S* tile
 // shared memory, ud_sm, the first a.upw per warp).
 template <int MODE>
 __device__ __forceinline__ double spmv_cta(const PArgs& a, int4 ci, const int4* ud_sm, double* hv,
-                                           const double* src, const double* pold, double beta, double* pnew,
-                                           double* y, const double* rhs) {
-    for (int h = threadIdx.x; h < ci.z; h += kPT) {
-        const int v = a.halo[ci.y + h];
+                                           const int* hidx, const double* src, const double* pold, double beta,
+                                           double* pnew, double* y, const double* rhs) {
+    // two halo vertices per thread and pass: all their loads in flight at once
+    for (int h = threadIdx.x; h < ci.z; h += 2 * kPT) {
+        const int h2 = h + kPT;
+        const bool two = h2 < ci.z;
+        const int v = hidx[h], v2 = two ? hidx[h2] : v;
+        double s0[6], q[6];
         #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            double s0 = ldv<true>(src + 3 * (size_t)v + d);
-            if (MODE == 1 && a.pv.bodies) s0 += patch_z(a.pv, v, d);  // z = MAS part + the patches' parts
-            hv[3 * h + d] = MODE == 1 ? __fma_rn(beta, ldv<true>(pold + 3 * (size_t)v + d), s0) : s0;
+            s0[d] = ldv<true>(src + 3 * (size_t)v + d);
+            s0[3 + d] = ldv<true>(src + 3 * (size_t)v2 + d);
+            if (MODE == 1) {
+                q[d] = ldv<true>(pold + 3 * (size_t)v + d);
+                q[3 + d] = ldv<true>(pold + 3 * (size_t)v2 + d);
+            }
+        }
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (MODE == 1 && a.pv.bodies) {  // z = MAS part + the patches' parts
+                s0[d] += patch_z(a.pv, v, d);
+                s0[3 + d] += patch_z(a.pv, v2, d);
+            }
+            hv[3 * h + d] = MODE == 1 ? __fma_rn(beta, q[d], s0[d]) : s0[d];
+            if (two) hv[3 * h2 + d] = MODE == 1 ? __fma_rn(beta, q[3 + d], s0[3 + d]) : s0[3 + d];
         }
     }
     __syncthreads();
@@ -412,6 +452,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     Acc* R1s = reinterpret_cast<Acc*>(tilesC + (size_t)a.capc * tb);
     __shared__ Anc anc;
     __shared__ int rng[2];
+    __shared__ unsigned short ctab[(kMaxLevels - 2) * kPT];  // a.nc <= 65535 (host check)
     Acc* Z1s = R1s + 3 * (size_t)a.k1 * B;
     Acc* Rc = Z1s + 3 * (size_t)a.k1 * B;
     Acc* Zc = Rc + 3 * (size_t)a.nc;
@@ -421,8 +462,10 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                                                                 smem_raw) + 15) & ~(size_t)15));
     // staged halo of the SpMV: 3 doubles per halo vertex
     double* hv = reinterpret_cast<double*>(udesc + (size_t)(kPT / 32) * a.upw * kRowGroups);
+    // the halo's vertex ids (fixed for the solve)
+    int* hidx = reinterpret_cast<int*>(hv + 3 * (size_t)a.hcap);
     // body-patch scratch: the patch's r and y (12 + 3 kPatchMax each)
-    Acc* prl = reinterpret_cast<Acc*>(hv + 3 * (size_t)a.hcap);
+    Acc* prl = reinterpret_cast<Acc*>(reinterpret_cast<unsigned char*>(hidx) + ((4 * (size_t)a.hcap + 15) & ~(size_t)15));
     Acc* pyl = prl + 12 + 3 * kPatchMax;
     const int4 ci = a.cinfo[blockIdx.x];
     if (a.stamps && blockIdx.x == 0 && threadIdx.x == 0) a.stamps[0] = clock64();
@@ -515,6 +558,10 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                 own = true;
             }
         }
+        if (own)  // coarse nodes of the slot's vertex at levels >= 2 (fixed for the solve)
+            for (int l = 2; l < a.L; ++l)
+                ctab[(l - 2) * kPT + threadIdx.x] =
+                    (unsigned short)(a.coarse_table[(size_t)kMaxLevels * v + l - 1] - a.lvl_begin[2]);
         hw1 = TG ? hw : hw - (kPT / B - ((o.nbk1 + HPW - 1) / HPW) * HPW);
         if (a.L > 2 && hw1 >= 0 && hw1 < o.nbk1) {
             const int i1 = (o.j0 + hw1) * B + lane;
@@ -540,8 +587,14 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
     x0 = 0.0; x1 = 0.0; x2 = 0.0;
     double r0 = 0.0, r1 = 0.0, r2 = 0.0;
     Acc zl0 = 0, zl1 = 0, zl2 = 0;  // level-0 Schwarz of the slot
-    // level-0 (+ level-1) part of the apply on r (registers)
-    auto apply_b = [&]() {
+    // level-1 warps of this CTA (act1): the first of them and their count
+    const int n1w = min(kPT / 32, (o.nbk1 + HPW - 1) / HPW);
+    const int w1first = TG ? 0 : kPT / 32 - n1w;
+    // level-0 (+ level-1) part of the apply on r (registers).  arrive: this
+    // CTA arrives at the next grid barrier as soon as what other CTAs read
+    // after it is written (the level-2 residual pushes, or r for the body
+    // patches), so the Schwarz products run while the other CTAs catch up
+    auto apply_b = [&](bool arrive) {
         // level-0 tiles: shared memory, or global memory when they did not fit
         const S* t0 = TG && a.t0g ? (const S*)a.inv + (size_t)o.lo * tb : tiles0;
         if (act0) {  // the slot's r into the bank exchange, level-0 component sums -> level-1 residuals
@@ -555,9 +608,17 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         }
         if (TG || a.L < 2) {
             if (act0) schwarz_rows<B, S, Acc>(t0 + (size_t)(hw < o.nbk0 ? hw : 0) * tb, lane, bank_slot<B>(xch), zl0, zl1, zl2);
-            if (a.L < 2) return;
+            if (a.L < 2) {
+                if (arrive) {
+                    __syncthreads();
+                    if (threadIdx.x == 0) grid_arrive(a.sync);
+                }
+                return;
+            }
         }
         __syncthreads();  // level-1 residuals complete
+        const bool push_arrive = arrive && a.L > 2 && n1w > 0;  // else thread 0 arrives here
+        if (arrive && !push_arrive && threadIdx.x == 0) grid_arrive(a.sync);
         if (!TG && act0)  // level-0 Schwarz on r (still in the bank exchange)
             schwarz_rows<B, S, Acc>(t0 + (size_t)(hw < o.nbk0 ? hw : 0) * tb, lane, bank_slot<B>(xch), zl0, zl1, zl2);
         if (act1) {  // level-1 banks of this CTA: push to level 2, Schwarz
@@ -576,6 +637,10 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                     Rg[0] = s0; Rg[1] = s1; Rg[2] = s2;
                 }
             }
+            if (push_arrive) {  // the level-1 warps' pushes are complete: arrive
+                asm volatile("bar.sync 1, %0;" ::"r"(32 * n1w) : "memory");
+                if (threadIdx.x == 32 * w1first) grid_arrive(a.sync);
+            }
             Acc z0, z1, z2;
             const S* t1 = TG && a.t1g ? (const S*)a.inv + (size_t)(a.lvl_begin[1] / B + o.j0) * tb : tiles1;
             schwarz_rows<B, S, Acc>(t1 + (size_t)(valid ? hw1 : 0) * tb, lane, xb, z0, z1, z2);
@@ -592,7 +657,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             Acc c0 = zl0, c1 = zl1, c2 = zl2;
             if (a.L >= 2) { c0 += Z1s[3 * n1loc]; c1 += Z1s[3 * n1loc + 1]; c2 += Z1s[3 * n1loc + 2]; }
             for (int l = 2; l < a.L; ++l) {
-                const int n = a.coarse_table[(size_t)kMaxLevels * v + l - 1] - a.lvl_begin[2];
+                const int n = ctab[(l - 2) * kPT + threadIdx.x];
                 c0 += Zc[3 * n]; c1 += Zc[3 * n + 1]; c2 += Zc[3 * n + 2];
             }
             const double z0 = (double)c0, z1 = (double)c1, z2 = (double)c2;
@@ -603,8 +668,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         // body patches (r complete in global memory: stored in phase B, a grid barrier since)
         for (int pb = blockIdx.x; pb < a.pv.bodies; pb += gridDim.x)
             patch_apply_cta<typename PatchS<S>::T, Acc>(a.pv, pb, a.ex.fem_off, a.r, a.z, prl, pyl, rz, rr);
-        rz = block_sum<kPT>(rz, sh);
-        rr = block_sum<kPT>(rr, sh);
+        block_sum2(rz, rr, sh);
         if (threadIdx.x == 0) { part_rz[blockIdx.x] = rz; part_rr[blockIdx.x] = rr; }
     };
 
@@ -617,6 +681,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             if (u < ci.x) d = a.udesc_c[(size_t)(ci.w + u) * kRowGroups + lane32 / kRowLanes];
             if (lane32 % kRowLanes == 0) udesc[(w * a.upw + i) * kRowGroups + lane32 / kRowLanes] = d;
         }
+        for (int h = threadIdx.x; h < ci.z; h += kPT) hidx[h] = a.halo[ci.y + h];
+        __syncthreads();
     }
     // ---- prologue: x = 0, r = b, p_old = 0, z = M^-1 r, r.z, r.r
     for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT) {
@@ -634,7 +700,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         double* part_w = a.partials + 3 * gridDim.x;
         double xax = 0.0, xb = 0.0, bb = 0.0;
         __syncthreads();  // the descriptor cache is complete
-        xax = spmv_cta<1>(a, ci, udesc, hv, a.x, a.x, 0.0, a.p1, a.Ap, nullptr);  // p = x0 (beta 0)
+        xax = spmv_cta<1>(a, ci, udesc, hv, hidx, a.x, a.x, 0.0, a.p1, a.Ap, nullptr);  // p = x0 (beta 0)
         for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT) {
             const double bi = a.b[i];
             xb += a.x[i] * bi;
@@ -646,8 +712,8 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         if (threadIdx.x == 0) { part_pap[blockIdx.x] = xax; part_rz[blockIdx.x] = xb; part_rr[blockIdx.x] = bb; }
         ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
         if (ok) {
-            xax = sum_partials(part_pap, sh);
-            sum_partials2(part_rz, part_rr, sh, xb, bb);
+            xax = sum_partials(part_pap);
+            sum_partials2(part_rz, part_rr, xb, bb);
             w_bb = bb;
             w_alpha = (xax > 0.0 && xb > 0.0) ? xb / xax : 0.0;
             double rr = 0.0;
@@ -662,7 +728,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         }
         ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
         if (ok) {
-            w_rr = sum_partials(part_w, sh);
+            w_rr = sum_partials(part_w);
             const int w_rej = !(w_rr <= w_bb) || w_alpha == 0.0;
             if (blockIdx.x == 0 && threadIdx.x == 0) {  // read back by the same thread at the end
                 a.st->w_alpha = w_alpha; a.st->w_rr = w_rr; a.st->w_reject = w_rej;
@@ -682,9 +748,10 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             r0 = r_in[vo]; r1 = r_in[vo + 1]; r2 = r_in[vo + 2];
             if (a.warm && own) { x0 = a.x[vo]; x1 = a.x[vo + 1]; x2 = a.x[vo + 2]; }
         }
-        if (ok) apply_b();
-        if (a.L > 2 || a.pv.bodies) {  // (the patches read r of other CTAs' rows)
-            ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
+        const bool need = a.L > 2 || a.pv.bodies;  // (the patches read r of other CTAs' rows)
+        if (ok) apply_b(need);
+        if (need) {
+            ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, nullptr, nullptr, false);
             if (ok && a.L > 2) ok = levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch);
         }
         if (ok) collect(0, 0.0, a.p1);
@@ -693,9 +760,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         if (ok) phase_jacobi(a, 0, 0.0, a.p1, part_rz, part_rr, sh);
     }
     ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
-    double rz = ok ? sum_partials(part_rz, sh) : 0.0;
+    double rz = ok ? sum_partials(part_rz) : 0.0;
     const double rz0 = rz;
-    const double rr0_r = ok ? sum_partials(part_rr, sh) : 0.0;
+    const double rr0_r = ok ? sum_partials(part_rr) : 0.0;
     const double rr0 = a.warm ? w_bb : rr0_r;  // a start guess: convergence relative to ||b||
     double rr_last = rr0_r, beta = 0.0;
     int k = 1, iters = 1, converged = 0, breakdown = 0;
@@ -710,7 +777,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         ++passes;
         // A: p_new = z + beta p_old, Ap = A p_new, p.Ap
         stamp(a, k, 0);
-        double dot = spmv_cta<1>(a, ci, udesc, hv, a.z, pold, beta, pnew, a.Ap, nullptr);
+        double dot = spmv_cta<1>(a, ci, udesc, hv, hidx, a.z, pold, beta, pnew, a.Ap, nullptr);
         dot = block_sum<kPT>(dot, sh);
         if (threadIdx.x == 0) part_pap[blockIdx.x] = dot;
         if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(0))) { ok = false; break; }
@@ -722,7 +789,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             if (own) { p0v = pnew[vo]; p1v = pnew[vo + 1]; p2v = pnew[vo + 2]; }
             if (!refresh) { q0 = a.Ap[vo]; q1 = a.Ap[vo + 1]; q2 = a.Ap[vo + 2]; }
         }
-        const double pap = sum_partials(part_pap, sh);
+        const double pap = sum_partials(part_pap);
         if (!(pap > 0.0)) {  // same value in every CTA: all stop here
             // finite p.Ap <= 0: CG breakdown (r = 0 exactly is a solution); NaN: reported as non-finite
             const bool finite = pap == pap && rz == rz;
@@ -749,7 +816,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                     a.x[i] = a.x[i] + alpha * pnew[i];
             }
             if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(1))) { ok = false; break; }
-            spmv_cta<2>(a, ci, udesc, hv, a.x, nullptr, 0.0, nullptr, a.r, a.b);
+            spmv_cta<2>(a, ci, udesc, hv, hidx, a.x, nullptr, 0.0, nullptr, a.r, a.b);
             if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(2))) { ok = false; break; }
             if (mas && v >= 0) { r0 = a.r[vo]; r1 = a.r[vo + 1]; r2 = a.r[vo + 2]; }
         } else {
@@ -766,9 +833,9 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         }
         stamp(a, k, 2);
         if (mas) {
-            apply_b();
+            apply_b(a.L > 2 || a.pv.bodies);
             if (a.L > 2 || a.pv.bodies) {
-                if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(3))) { ok = false; break; }
+                if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(3), false)) { ok = false; break; }
                 stamp(a, k, 3);
                 if (a.L > 2 && !levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch)) ok = false;
             }
@@ -779,7 +846,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(5)) || !ok) { ok = false; break; }
         stamp(a, k, 5);
         double rz_new, rr;
-        sum_partials2(part_rz, part_rr, sh, rz_new, rr);
+        sum_partials2(part_rz, part_rr, rz_new, rr);
         bool conv = false;
         if (k % a.check_every == 0) {
             rr_last = rr;
@@ -1107,7 +1174,8 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
         a.halo = c->d_halo;
     }
     // the staged halo comes first; the subdomain tiles share what is left
-    const size_t hbytes = (3 * sizeof(double) * (size_t)a.hcap + 15) & ~(size_t)15;
+    const size_t hbytes = ((3 * sizeof(double) * (size_t)a.hcap + 15) & ~(size_t)15) +  // halo values, ids
+                          ((4 * (size_t)a.hcap + 15) & ~(size_t)15);
     const size_t pbytes = a.pv.bodies ? 2 * (12 + 3 * kPatchMax) * sizeof(Acc) : 0;  // body-patch scratch
     if (hbytes + pbytes + 256 > budget) return 1;
     const size_t tbudget = budget - hbytes - pbytes;
@@ -1173,6 +1241,7 @@ int launch_t(sgmas_context* c, PArgs& a, float* ms) {
         }
         a.nc = a.L > 2 ? a.total - a.lvl_begin[2] : 0;
         if (a.k0 > kPT / B || a.k1 > kPT / B) return 1;  // one slot per thread: use the graph form
+        if (a.nc > 65535) return 1;                         // coarse indices are cached as 16 bits
         const size_t small = 2 * 3 * (size_t)a.k1 * B * sizeof(Acc) + 2 * 3 * (size_t)a.nc * sizeof(Acc) +
                              (size_t)a.nc * sizeof(int);
         // level-0 tiles stay in shared memory if anything does; level-1 tiles next
