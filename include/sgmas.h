@@ -280,6 +280,32 @@ int sgmas_assembly_plan(sgmas_context* ctx, const int* d_rows, const int* d_cols
                         int* d_out_cols, int* n_unique);
 int sgmas_assemble(sgmas_context* ctx, const double* d_values, int n, double* d_out_values);
 
+/* Element matrices straight into the planned structure: no raw triplet array.
+ * A group is one element type (write_triplet_fem SG/femEnergy.cu:14-62 and
+ * the barrier writers of SG/GIPC.cu:82-139 write one each): d_H [n_elem]
+ * [3k][3k] row-major element matrices, d_nodes [n_elem][k] vertex ids,
+ * k = nodes_per_elem in 1..4.  sgmas_element_plan takes 1..4 groups, lays out
+ * their upper triplets in the order sgmas_write_upper_blocks writes them
+ * (group after group), sorts and merges them as sgmas_assembly_plan does
+ * (d_out_rows / d_out_cols need room for all raw triplets), and keeps, for
+ * each sorted triplet, where its 3x3 block sits in its group's matrices
+ * (d_H is not read).  sgmas_element_assemble then reads that step's element
+ * matrices (same groups, counts and nodes as planned; d_nodes is not read)
+ * and writes the merged values with one kernel, bit-identical to
+ * sgmas_write_upper_blocks of each group followed by sgmas_convert.  A later
+ * sgmas_assembly_plan replaces the element plan.  The project's own (the
+ * reference writes triplets and sorts them every step). */
+typedef struct sgmas_element_group {
+    const double* d_H;
+    const int* d_nodes;
+    int n_elem;
+    int nodes_per_elem;
+} sgmas_element_group;
+int sgmas_element_plan(sgmas_context* ctx, const sgmas_element_group* groups, int n_groups, int* d_out_rows,
+                       int* d_out_cols, int* n_unique);
+int sgmas_element_assemble(sgmas_context* ctx, const sgmas_element_group* groups, int n_groups,
+                           double* d_out_values);
+
 /* Affine-body coupling (ABDSystem::_setup_abd_system_hessian,
  * SG/abd_system/abd_system_function/setup_abd_system_gradient_and_hessian.cu:419-601):
  * vertex-level 3x3 blocks into the 3x3 triplets of the 12-DOF body rows (body b

@@ -85,7 +85,7 @@ void free_all(sgmas_context* c) {
                     c->d_z, c->d_p0, c->d_p1, c->d_Ap, c->d_diag_inv, c->d_abd_inv, c->d_partials, c->d_ticket,
                     c->d_state, c->d_hvals, c->d_hb, c->d_hx, c->d_hrows, c->d_hcols, c->d_sort_scratch,
                     c->d_coarse_ticket, c->bsr.row_list, c->bsr.d_nlong, c->bsr.tcols, c->bsr.tsrc,
-                    c->d_psync, c->d_stamps, c->d_l1_bank, c->d_own1, c->d_tune_x, c->bsr.udesc, c->d_plan_idx,
+                    c->d_psync, c->d_stamps, c->d_l1_bank, c->d_own1, c->d_tune_x, c->bsr.udesc, c->d_plan_idx, c->d_elem_src, c->d_elem_rc,
                     c->d_plan_start, c->d_row_order, c->d_cpre, c->d_udesc_c, c->d_lcols, c->d_halo,
                     c->d_cinfo, c->d_plan_stats, c->d_patch_owner, c->d_patch_ent, c->d_patch_list, c->d_patch_info,
                     c->d_patch_w64, c->d_patch_wcol, c->d_patch_wrow, c->d_patch_zs};
@@ -489,6 +489,22 @@ int sgmas_assemble(sgmas_context* c, const double* d_values, int n, double* d_ou
     if (!c || n < 0 || (n > 0 && (!d_values || !d_out_values))) return SGMAS_ERR_ARG;
     SG_CUDA(c, cudaSetDevice(c->device));
     return assemble_planned(c, d_values, n, d_out_values);
+}
+
+int sgmas_element_plan(sgmas_context* c, const sgmas_element_group* groups, int n_groups, int* d_out_rows,
+                       int* d_out_cols, int* n_unique) {
+    if (!c || !n_unique || n_groups < 1 || n_groups > 4 || !groups) return SGMAS_ERR_ARG;
+    SG_CUDA(c, cudaSetDevice(c->device));
+    int rc = element_plan(c, groups, n_groups, d_out_rows, d_out_cols, n_unique);
+    if (rc) return rc;
+    return check_device_error(c, "sgmas_element_plan");
+}
+
+int sgmas_element_assemble(sgmas_context* c, const sgmas_element_group* groups, int n_groups,
+                           double* d_out_values) {
+    if (!c || n_groups < 1 || n_groups > 4 || !groups) return SGMAS_ERR_ARG;
+    SG_CUDA(c, cudaSetDevice(c->device));
+    return element_assemble(c, groups, n_groups, d_out_values);
 }
 
 int sgmas_write_upper_blocks(sgmas_context* c, const double* d_H, int n_elem, int k, const int* d_nodes,

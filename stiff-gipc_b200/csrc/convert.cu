@@ -9,8 +9,14 @@
 //    project radix sort (LSD, 8-bit digits, stable) on compacted keys and a
 //    segmented sum that walks each key's run in sorted order, so the merged
 //    values are deterministic;
+//  * element_plan / element_assemble: element matrices of fixed groups
+//    straight into the planned merged structure (the sum of
+//    write_upper_blocks + convert_triplets, bit for bit, without the raw
+//    triplet array);
 //  * morton_codes: _calcVertMChash / hash_code(type -1) (SG/GIPC.cu:142-201,
 //    412-461).
+#include <climits>
+
 #include "../../include/sgmas.h"
 #include "ctx.hpp"
 
@@ -148,16 +154,136 @@ __global__ void k_seg_starts(int n, const uint64_t* __restrict__ keys, const int
 }
 // nine threads per merged block, one per component: each sums its component
 // over the block's run in sorted (stable) order -- the order, and so the
-// result, of a per-block sum -- while the nine read one block's 72 bytes together
+// result, of a per-block sum -- while the nine read one block's 72 bytes
+// together.  The run is read kSegBatch triplets at a time, all their loads in
+// flight before the additions, which stay in run order.
+constexpr int kSegBatch = 8;
+
 __global__ void k_seg_sum(int nu, int n, const int* __restrict__ start, const uint32_t* __restrict__ idx,
                           const double* __restrict__ vals, double* out) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 9LL * nu) return;
     const int u = (int)(t / 9), q = (int)(t % 9);
     const int b = start[u], e = (u + 1 < nu) ? start[u + 1] : n;
-    double s = vals[9 * (size_t)idx[b] + q];
-    for (int i = b + 1; i < e; ++i) s += vals[9 * (size_t)idx[i] + q];
+    double s = 0.0;
+    for (int i0 = b; i0 < e; i0 += kSegBatch) {
+        uint32_t ix[kSegBatch];
+        double v[kSegBatch];
+        #pragma unroll
+        for (int j = 0; j < kSegBatch; ++j) ix[j] = i0 + j < e ? idx[i0 + j] : 0u;
+        #pragma unroll
+        for (int j = 0; j < kSegBatch; ++j) v[j] = i0 + j < e ? vals[9 * (size_t)ix[j] + q] : 0.0;
+        #pragma unroll
+        for (int j = 0; j < kSegBatch; ++j)
+            if (i0 + j < e) s = (i0 + j == b) ? v[j] : s + v[j];  // the first value as is (keeps -0.0)
+    }
     out[9 * (size_t)u + q] = s;
+}
+
+// upper block pair q (0 .. k(k+1)/2 - 1) of a k-node element: (ii, jj), ii <= jj, row-major
+__device__ __forceinline__ void upper_pair(int k, int q, int& ii, int& jj) {
+    int off = 0;
+    ii = 0;
+    while (off + (k - ii) <= q) { off += k - ii; ++ii; }
+    jj = ii + (q - off);
+}
+
+// ---- element groups in a planned structure ----------------------------------
+constexpr int kMaxElemGroups = 4;
+struct ElemTab {
+    const double* H[kMaxElemGroups];
+    const int* nodes[kMaxElemGroups];
+    long long off[kMaxElemGroups + 1];  // first raw triplet of each group
+    int k[kMaxElemGroups];
+    int ng;
+};
+
+// group g's matrices and row stride, selected with constant indices (a
+// computed index into the kernel's parameter struct would copy it to local memory)
+__device__ __forceinline__ const double* elem_H(const ElemTab& T, int g, int& w) {
+    const double* h = T.H[0];
+    w = 3 * T.k[0];
+    if (g == 1) { h = T.H[1]; w = 3 * T.k[1]; }
+    if (g == 2) { h = T.H[2]; w = 3 * T.k[2]; }
+    if (g == 3) { h = T.H[3]; w = 3 * T.k[3]; }
+    return h;
+}
+
+__device__ __forceinline__ int elem_group_of(const ElemTab& T, long long o) {
+    int g = 0;
+    while (g + 1 < T.ng && o >= T.off[g + 1]) ++g;
+    return g;
+}
+
+// raw rows / cols of the groups in write order (k_upper_blocks' indices)
+__global__ void k_elem_struct(ElemTab T, int* rows, int* cols) {
+    const long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= T.off[T.ng]) return;
+    const int g = elem_group_of(T, o), k = T.k[g], np = k * (k + 1) / 2;
+    const long long lo = o - T.off[g];
+    const long long e = lo / np;
+    int ii, jj;
+    upper_pair(k, (int)(lo % np), ii, jj);
+    const int row = T.nodes[g][e * k + ii], col = T.nodes[g][e * k + jj];
+    rows[o] = min(row, col);
+    cols[o] = max(row, col);
+}
+
+// for each sorted triplet: the first element of its block in the group's
+// matrices (the transposed block, as k_upper_blocks writes it, when row > col)
+__global__ void k_elem_src(int n, ElemTab T, const uint32_t* __restrict__ idx, long long* src) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long o = idx[i];
+    const int g = elem_group_of(T, o), k = T.k[g], np = k * (k + 1) / 2, w = 3 * k;
+    const long long lo = o - T.off[g];
+    const long long e = lo / np;
+    int ii, jj;
+    upper_pair(k, (int)(lo % np), ii, jj);
+    const bool swap = T.nodes[g][e * k + ii] > T.nodes[g][e * k + jj];
+    const long long base = e * w * w + (swap ? (long long)jj * 3 * w + ii * 3 : (long long)ii * 3 * w + jj * 3);
+    src[i] = ((long long)g << 56) | base;
+}
+
+// k_seg_sum with the values read from the element matrices: three threads
+// per merged block, one per block row a, each summing its row's three
+// components (a, c) -- column-major index a + 3 c, as k_upper_blocks writes
+// them -- = H[base + a w + c] (3 contiguous doubles) over the run in order,
+// kSegBatch triplets' loads in flight before their additions.
+__global__ void k_elem_seg_sum(int nu, int n, const int* __restrict__ start, const long long* __restrict__ src,
+                               ElemTab T, double* out) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3LL * nu) return;
+    const int u = (int)(t / 3), a = (int)(t % 3);
+    const int b = start[u], e = (u + 1 < nu) ? start[u + 1] : n;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int i0 = b; i0 < e; i0 += kSegBatch) {
+        long long sv[kSegBatch];
+        double v[kSegBatch][3];
+        #pragma unroll
+        for (int j = 0; j < kSegBatch; ++j) sv[j] = i0 + j < e ? src[i0 + j] : 0ll;
+        #pragma unroll
+        for (int j = 0; j < kSegBatch; ++j) {
+            int w;
+            const double* h0 = elem_H(T, (int)(sv[j] >> 56) & 3, w);
+            const double* h = h0 + (sv[j] & ((1ll << 56) - 1)) + a * w;
+            const bool in = i0 + j < e;
+            v[j][0] = in ? __ldg(h) : 0.0;
+            v[j][1] = in ? __ldg(h + 1) : 0.0;
+            v[j][2] = in ? __ldg(h + 2) : 0.0;
+        }
+        #pragma unroll
+        for (int j = 0; j < kSegBatch; ++j)
+            if (i0 + j < e) {
+                const bool f = i0 + j == b;  // the first value as is (keeps -0.0)
+                s0 = f ? v[j][0] : s0 + v[j][0];
+                s1 = f ? v[j][1] : s1 + v[j][1];
+                s2 = f ? v[j][2] : s2 + v[j][2];
+            }
+    }
+    out[9 * (size_t)u + a] = s0;
+    out[9 * (size_t)u + a + 3] = s1;
+    out[9 * (size_t)u + a + 6] = s2;
 }
 
 // upper triplets of element matrices: one thread per (element, block pair)
@@ -167,9 +293,8 @@ __global__ void k_upper_blocks(int n_elem, int k, const double* __restrict__ H, 
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)n_elem * np) return;
     const int e = (int)(t / np), q = (int)(t % np);
-    int ii = 0, off = 0;
-    while (off + (k - ii) <= q) { off += k - ii; ++ii; }
-    const int jj = ii + (q - off);
+    int ii, jj;
+    upper_pair(k, q, ii, jj);
     const int row = nodes[(size_t)e * k + ii], col = nodes[(size_t)e * k + jj];
     const bool swap = row > col;
     const int w = 3 * k;
@@ -376,6 +501,7 @@ int assembly_plan(sgmas_context* c, const int* rows, const int* cols, int n, int
                   int* n_unique) {
     *n_unique = 0;
     c->plan_n = -1;
+    c->elem_ng = 0;  // element_plan sets it again after this call
     if (n == 0) {
         c->plan_n = 0;
         c->plan_nu = 0;
@@ -427,6 +553,78 @@ int assemble_planned(sgmas_context* c, const double* vals, int n, double* out_va
     k_seg_sum<<<(int)((9LL * nu + kT - 1) / kT), kT, 0, c->stream>>>(nu, n, c->d_plan_start,
                                                         reinterpret_cast<const uint32_t*>(c->d_plan_idx), vals,
                                                         out_vals);
+    SG_CUDA(c, cudaGetLastError());
+    return 0;
+}
+
+namespace {
+// the group table of a call (an error status for bad groups)
+int elem_tab(sgmas_context* c, const sgmas_element_group* groups, int ng, bool need_nodes, bool need_H, ElemTab& T,
+             const char* fn) {
+    T = ElemTab{};
+    T.ng = ng;
+    for (int g = 0; g < ng; ++g) {
+        const sgmas_element_group& G = groups[g];
+        if (G.n_elem < 0 || G.nodes_per_elem < 1 || G.nodes_per_elem > 4)
+            return ctx_fail(c, SGMAS_ERR_ARG, "%s: group %d has n_elem %d, nodes_per_elem %d (1..4)", fn, g,
+                            G.n_elem, G.nodes_per_elem);
+        if (G.n_elem > 0 && ((need_nodes && !G.d_nodes) || (need_H && !G.d_H)))
+            return ctx_fail(c, SGMAS_ERR_ARG, "%s: group %d has a NULL %s", fn, g, need_H ? "d_H" : "d_nodes");
+        T.H[g] = G.d_H;
+        T.nodes[g] = G.d_nodes;
+        T.k[g] = G.nodes_per_elem;
+        T.off[g + 1] = T.off[g] + (long long)G.n_elem * (G.nodes_per_elem * (G.nodes_per_elem + 1) / 2);
+    }
+    if (T.off[ng] > INT_MAX) return ctx_fail(c, SGMAS_ERR_ARG, "%s: more than 2^31 - 1 triplets", fn);
+    return 0;
+}
+}  // namespace
+
+int element_plan(sgmas_context* c, const sgmas_element_group* groups, int ng, int* out_rows, int* out_cols,
+                 int* n_unique) {
+    *n_unique = 0;
+    c->elem_ng = 0;
+    ElemTab T;
+    int rc = elem_tab(c, groups, ng, true, false, T, "sgmas_element_plan");
+    if (rc) return rc;
+    const int n = (int)T.off[ng];
+    if (n > 0 && (!out_rows || !out_cols)) return SGMAS_ERR_ARG;
+    if (n > 0) {
+        if (ctx_alloc_grow(c, &c->d_elem_rc, &c->elem_rc_cap, 2 * n) ||
+            ctx_alloc_grow(c, &c->d_elem_src, &c->elem_src_cap, n))
+            return SGMAS_ERR_CUDA;
+        k_elem_struct<<<(n + kT - 1) / kT, kT, 0, c->stream>>>(T, c->d_elem_rc, c->d_elem_rc + n);
+        SG_CUDA(c, cudaGetLastError());
+    }
+    rc = assembly_plan(c, c->d_elem_rc, c->d_elem_rc + n, n, out_rows, out_cols, n_unique);
+    if (rc) return rc;
+    if (n > 0) {
+        k_elem_src<<<(n + kT - 1) / kT, kT, 0, c->stream>>>(n, T, reinterpret_cast<const uint32_t*>(c->d_plan_idx),
+                                                              c->d_elem_src);
+        SG_CUDA(c, cudaGetLastError());
+    }
+    c->elem_ng = ng;
+    for (int g = 0; g < ng; ++g) { c->elem_n[g] = groups[g].n_elem; c->elem_k[g] = groups[g].nodes_per_elem; }
+    return 0;
+}
+
+int element_assemble(sgmas_context* c, const sgmas_element_group* groups, int ng, double* out_vals) {
+    if (c->elem_ng == 0 || c->plan_n < 0)
+        return ctx_fail(c, SGMAS_ERR_STATE, "sgmas_element_assemble before sgmas_element_plan");
+    if (ng != c->elem_ng)
+        return ctx_fail(c, SGMAS_ERR_ARG, "sgmas_element_assemble: %d groups, the plan has %d", ng, c->elem_ng);
+    for (int g = 0; g < ng; ++g)
+        if (groups[g].n_elem != c->elem_n[g] || groups[g].nodes_per_elem != c->elem_k[g])
+            return ctx_fail(c, SGMAS_ERR_ARG, "sgmas_element_assemble: group %d is %d x %d nodes, planned %d x %d", g,
+                            groups[g].n_elem, groups[g].nodes_per_elem, c->elem_n[g], c->elem_k[g]);
+    ElemTab T;
+    int rc = elem_tab(c, groups, ng, false, true, T, "sgmas_element_assemble");
+    if (rc) return rc;
+    const int nu = c->plan_nu;
+    if (nu == 0) return 0;
+    if (!out_vals) return SGMAS_ERR_ARG;
+    k_elem_seg_sum<<<(int)((3LL * nu + kT - 1) / kT), kT, 0, c->stream>>>(nu, c->plan_n, c->d_plan_start,
+                                                                          c->d_elem_src, T, out_vals);
     SG_CUDA(c, cudaGetLastError());
     return 0;
 }

@@ -167,6 +167,13 @@ struct sgmas_context {
     int* d_plan_start = nullptr;
     int plan_idx_cap = 0, plan_start_cap = 0;
     int plan_n = -1, plan_nu = 0;         // raw triplets and merged blocks of the plan (-1: none)
+    // element plan (sgmas_element_plan): the plan above built from element groups, plus each sorted
+    // triplet's source block in its group's element matrices (group << 56 | offset in doubles)
+    long long* d_elem_src = nullptr;
+    int* d_elem_rc = nullptr;             // raw rows, cols of the planned groups (the plan's input)
+    int elem_src_cap = 0, elem_rc_cap = 0;
+    int elem_ng = 0;                      // groups of the element plan (0: the plan is not an element plan)
+    int elem_n[4] = {0, 0, 0, 0}, elem_k[4] = {0, 0, 0, 0};
     int tune_cap = 0;
     PcgState* d_state = nullptr;
     // uploaded host systems (sgmas_pcg_solve_host)
@@ -239,6 +246,9 @@ int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* 
 int assembly_plan(sgmas_context* c, const int* rows, const int* cols, int n, int* out_rows, int* out_cols,
                   int* n_unique);
 int assemble_planned(sgmas_context* c, const double* vals, int n, double* out_vals);
+int element_plan(sgmas_context* c, const sgmas_element_group* groups, int ng, int* out_rows, int* out_cols,
+                 int* n_unique);
+int element_assemble(sgmas_context* c, const sgmas_element_group* groups, int ng, double* out_vals);
 void bsr_mark_fresh(sgmas_context* c, const sgmas_bcoo* A);  // the CSR just built is A's
 bool bsr_reuse(sgmas_context* c, const sgmas_bcoo* A);       // true (once) when the fresh CSR is A's
 int bsr_spmv_plain(sgmas_context* c, double a, const double* x, double b, double* y);

@@ -55,6 +55,10 @@ class TuneReport(C.Structure):
                 ("sms", C.c_int)]
 
 
+class ElementGroup(C.Structure):
+    _fields_ = [("d_H", C.c_void_p), ("d_nodes", C.c_void_p), ("n_elem", C.c_int), ("nodes_per_elem", C.c_int)]
+
+
 class Bcoo(C.Structure):
     _fields_ = [("d_values", C.c_void_p), ("d_rows", C.c_void_p), ("d_cols", C.c_void_p),
                 ("n_blocks", C.c_int), ("n_block_rows", C.c_int)]
@@ -69,7 +73,7 @@ EXPORTS = [
     "sgmas_part_maps", "sgmas_morton_codes_noalloc", "sgmas_set_pcg_mode", "sgmas_pcg_last_vectors",
     "sgmas_mtx_write", "sgmas_mtx_read", "sgmas_set_pcg_ctas", "sgmas_set_wait_limit", "sgmas_mlp_set_params", "sgmas_mlp_get_params", "sgmas_mlp_features",
     "sgmas_mlp_gradient", "sgmas_mlp_train_step", "sgmas_mlp_forward", "sgmas_mlp_warm_start",
-    "sgmas_autotune_pcg", "sgmas_assembly_plan", "sgmas_assemble", "sgmas_abd_body_blocks",
+    "sgmas_autotune_pcg", "sgmas_assembly_plan", "sgmas_assemble", "sgmas_element_plan", "sgmas_element_assemble", "sgmas_abd_body_blocks",
     "sgmas_abd_pair_blocks", "sgmas_abd_fem_blocks",
 ]
 MLP_PARAMS = 19462  # SGMAS_MLP_PARAMS in include/sgmas.h
@@ -121,6 +125,8 @@ def lib(build_if_missing: bool = False):
     L.sgmas_pcg_last_vectors.argtypes = [vp, vp, vp]
     L.sgmas_assembly_plan.argtypes = [vp, vp, vp, i, vp, vp, C.POINTER(i)]
     L.sgmas_assemble.argtypes = [vp, vp, i, vp]
+    L.sgmas_element_plan.argtypes = [vp, C.POINTER(ElementGroup), i, vp, vp, C.POINTER(i)]
+    L.sgmas_element_assemble.argtypes = [vp, C.POINTER(ElementGroup), i, vp]
     L.sgmas_abd_body_blocks.argtypes = [vp, vp, i, vp, vp, vp]
     L.sgmas_abd_pair_blocks.argtypes = [vp, vp, vp, vp, i, vp, vp, vp, vp, vp, vp]
     L.sgmas_abd_fem_blocks.argtypes = [vp, vp, vp, vp, i, vp, vp, vp, vp, i, i, vp, vp, vp]
@@ -493,6 +499,28 @@ class Context:
                                                 int(in_rows.shape[0]), _ptr(xbar), _ptr(body_of), _ptr(fixed),
                                                 _ptr(fem_boundary), int(fem_point_offset), int(n_bodies), _ptr(vals),
                                                 _ptr(rows), _ptr(cols)))
+
+    def element_plan(self, nodes_list, out_rows, out_cols):
+        """Plan the merged structure of element groups (sgmas_element_plan):
+        nodes_list = [int32 [n_elem, k] device arrays], group after group;
+        out_rows / out_cols need room for all raw triplets.  Returns the
+        merged count."""
+        G = (ElementGroup * len(nodes_list))()
+        for g, nd in enumerate(nodes_list):
+            G[g] = ElementGroup(None, _ptr(nd), int(nd.shape[0]), int(nd.shape[1]))
+        nu = C.c_int()
+        self._check(self.L.sgmas_element_plan(self.h, G, len(nodes_list), _ptr(out_rows), _ptr(out_cols),
+                                              C.byref(nu)))
+        return nu.value
+
+    def element_assemble(self, H_list, out_vals):
+        """One step's element matrices (float64 [n_elem, 3k, 3k] device
+        arrays, the planned groups in order) -> merged values
+        (sgmas_element_assemble)."""
+        G = (ElementGroup * len(H_list))()
+        for g, H in enumerate(H_list):
+            G[g] = ElementGroup(_ptr(H), None, int(H.shape[0]), int(H.shape[1]) // 3)
+        self._check(self.L.sgmas_element_assemble(self.h, G, len(H_list), _ptr(out_vals)))
 
     def write_upper_blocks(self, H, nodes, vals, rows, cols):
         n_elem, k = int(nodes.shape[0]), int(nodes.shape[1])

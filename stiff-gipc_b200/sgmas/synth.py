@@ -51,6 +51,7 @@ class System:
     raw_rows: np.ndarray = None
     raw_cols: np.ndarray = None
     raw_vals: np.ndarray = None
+    elem_groups: list = None
     info: dict = dataclasses.field(default_factory=dict)
 
 
@@ -190,6 +191,9 @@ def make_grid_system(nx=10, ny=10, nz=10, h=0.01, E=1e5, nu=0.4, rho=1000.0, dt=
     rows = [r_m, r_el]
     cols = [r_m, c_el]
     vals = [v_m, v_el]
+    H_m = np.zeros((n, 3, 3))
+    H_m[:, 0, 0] = H_m[:, 1, 1] = H_m[:, 2, 2] = mass
+    groups = [(H_m, np.arange(n, dtype=np.int32)[:, None]), (He, tets.astype(np.int32))]
     pairs = np.zeros((0, 4), np.int32)
     if n_pairs and blocks == 2:
         nv1 = nx * ny * nz
@@ -225,6 +229,7 @@ def make_grid_system(nx=10, ny=10, nz=10, h=0.01, E=1e5, nu=0.4, rho=1000.0, dt=
         nodes = np.stack([pts[pi], tris[tj, 0], tris[tj, 1], tris[tj, 2]], 1)
         r_c, c_c, v_c = upper_triplets(Hc, nodes)
         rows.append(r_c); cols.append(c_c); vals.append(v_c)
+        groups.append((Hc, nodes.astype(np.int32)))
         pairs = np.stack([-(nodes[:, 0] + 1), nodes[:, 1], nodes[:, 2], nodes[:, 3]], 1).astype(np.int32)
     raw_r = np.concatenate(rows).astype(np.int32)
     raw_c = np.concatenate(cols).astype(np.int32)
@@ -235,8 +240,9 @@ def make_grid_system(nx=10, ny=10, nz=10, h=0.01, E=1e5, nu=0.4, rho=1000.0, dt=
                   info=dict(nx=nx, ny=ny, nz=nz, blocks=blocks, n_pairs=len(pairs), E=E, nu=nu,
                             dt=dt, h=h, eps=eps, kappa=kappa, dhat=dhat, seed=seed, n_tets=len(tets),
                             n_raw=len(raw_r), n_blocks=len(mr)))
-    if keep_raw:
+    if keep_raw:  # raw triplets, and the element groups (matrices [m, 3k, 3k], nodes [m, k]) they come from
         sysm.raw_rows, sysm.raw_cols, sysm.raw_vals = raw_r, raw_c, raw_v
+        sysm.elem_groups = groups
     return sysm
 
 

@@ -545,6 +545,62 @@ def test_assembly_plan_matches_convert(sgm, name):
     ctx.close()
 
 
+@pytest.mark.parametrize("name", ["c1", "c2s"])
+def test_element_assembly_matches_convert(sgm, name):
+    """Element matrices of fixed groups (mass diagonal, tets, and on c2s the
+    barrier pairs) straight into the planned structure: the structure equals
+    sgmas_convert's, and two steps' matrices (the second perturbed
+    asymmetrically, so transposed blocks must be taken as the triplet writer
+    takes them) give values bit-identical to sgmas_write_upper_blocks of
+    every group followed by sgmas_convert."""
+    s = synth.config1(seed=5, keep_raw=True) if name == "c1" else synth.config2(seed=5, scale=0.3, keep_raw=True)
+    groups = s.elem_groups
+    assert len(groups) == (2 if name == "c1" else 3)
+    ctx = sgm.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    npairs = [len(nd) * nd.shape[1] * (nd.shape[1] + 1) // 2 for _, nd in groups]
+    n = sum(npairs)
+    nodes = [dev(nd) for _, nd in groups]
+    pr = torch.zeros(n, dtype=torch.int32, device="cuda")
+    pc = torch.zeros(n, dtype=torch.int32, device="cuda")
+    nu = ctx.element_plan(nodes, pr, pc)
+    rng = np.random.default_rng(2)
+    for step in range(2):
+        Hs = [np.ascontiguousarray(H * (1.0 + 0.25 * step) + rng.normal(size=H.shape) * 1e-3 * step * np.abs(H).max())
+              for H, _ in groups]
+        dH = [dev(H) for H in Hs]
+        out = torch.zeros((n, 9), dtype=torch.float64, device="cuda")
+        ctx.element_assemble(dH, out)
+        rv = torch.zeros((n, 9), dtype=torch.float64, device="cuda")
+        rr = torch.zeros(n, dtype=torch.int32, device="cuda")
+        rc = torch.zeros(n, dtype=torch.int32, device="cuda")
+        o = 0
+        for H, nd, m in zip(dH, nodes, npairs):
+            ctx.write_upper_blocks(H, nd, rv[o:o + m], rr[o:o + m], rc[o:o + m])
+            o += m
+        cv = torch.zeros((n, 9), dtype=torch.float64, device="cuda")
+        cr = torch.zeros(n, dtype=torch.int32, device="cuda")
+        cc = torch.zeros(n, dtype=torch.int32, device="cuda")
+        assert ctx.convert(rv, rr, rc, cv, cr, cc) == nu
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(pr.cpu().numpy()[:nu], cr.cpu().numpy()[:nu])
+        np.testing.assert_array_equal(pc.cpu().numpy()[:nu], cc.cpu().numpy()[:nu])
+        np.testing.assert_array_equal(out.cpu().numpy()[:nu].view(np.uint64), cv.cpu().numpy()[:nu].view(np.uint64))
+        if step == 0:  # the first step's structure is the system's own merge
+            assert nu == len(s.rows)
+            np.testing.assert_array_equal(cr.cpu().numpy()[:nu], s.rows)
+            np.testing.assert_array_equal(cc.cpu().numpy()[:nu], s.cols)
+    with pytest.raises(sgm.SgmasError):  # other group counts than planned
+        ctx.element_assemble(dH[:-1], out)
+    with pytest.raises(sgm.SgmasError):
+        ctx.element_assemble([dH[0][:-1]] + dH[1:], out)
+    # a plain assembly plan replaces the element plan
+    ctx.assembly_plan(rr, rc, pr, pc)
+    with pytest.raises(sgm.SgmasError):
+        ctx.element_assemble(dH, out)
+    ctx.close()
+
+
 def test_assemble_before_plan_refused(sgm):
     ctx = sgm.Context(0)
     with pytest.raises(sgm.SgmasError):
