@@ -236,8 +236,11 @@ def assembly_leg(s, dev, stream, flush, reps=20):
     flushed before each): the reference's composition (upper triplets of each
     group by sgmas_write_upper_blocks, then sgmas_convert: sort + merge every
     step); the same triplets merged in a planned structure (sgmas_assemble);
-    and the element matrices straight into that structure
-    (sgmas_element_assemble), checked bit-identical to the first.  Bytes of
+    the element matrices straight into that structure
+    (sgmas_element_assemble), checked bit-identical to the first; and, for
+    contacts that change every step, the fixed groups (mass, tets) by
+    sgmas_element_assemble with the barrier pairs' triplets written and
+    merged in by sgmas_append_triplets (sorted append), also checked.  Bytes of
     the fused kernel: the upper 3x3 blocks of every element read once (72 B
     per raw triplet) + each sorted triplet's source offset (8 B) + run starts
     (4 B per merged block) + merged values written (72 B per merged block)."""
@@ -297,6 +300,22 @@ def assembly_leg(s, dev, stream, flush, reps=20):
     torch.cuda.synchronize()
     same = bool(torch.equal(ev[:nu].view(torch.int64), cv[:nu].view(torch.int64)) and torch.equal(er[:nu], cr[:nu])
                 and torch.equal(ec[:nu], cc[:nu]))
+    # contacts changing every step: the fixed groups planned, the last group (the barrier pairs)
+    # written as triplets and appended
+    mc = npairs[-1]
+    pv, pr, pc = rv[n - mc:], rr[n - mc:], rc[n - mc:]
+    xv, xr, xc = torch.zeros_like(rv), torch.zeros_like(rr), torch.zeros_like(rr)
+    nel = ctx.element_plan(nodes[:-1], er, ec)
+
+    def step_append():
+        ctx.element_assemble(H[:-1], ev)
+        ctx.write_upper_blocks(H[-1], nodes[-1], pv, pr, pc)
+        return ctx.append_triplets(ev, er, ec, nel, pv, pr, pc, xv, xr, xc)
+    ms_append = tm(step_append)
+    na = step_append()
+    torch.cuda.synchronize()
+    same_append = bool(na == nu and torch.equal(xv[:nu].view(torch.int64), cv[:nu].view(torch.int64))
+                       and torch.equal(xr[:nu], cr[:nu]) and torch.equal(xc[:nu], cc[:nu]))
     ctx.close()
     peak, kind = peaks()
     byts = 72 * n + 8 * n + 4 * nu + 72 * nu
@@ -304,6 +323,8 @@ def assembly_leg(s, dev, stream, flush, reps=20):
             "write_upper_plus_convert_ms": round(ms_conv, 4), "write_upper_ms": round(ms_write, 4),
             "planned_assemble_ms": round(ms_planned, 4), "element_assemble_ms": round(ms_elem, 4),
             "element_plan_s": round(plan_s, 4), "element_bit_identical_to_convert": same,
+            "elastic_element_plus_contact_append_ms": round(ms_append, 4),
+            "append_bit_identical_to_convert": same_append,
             "element_assemble_roofline": {"bytes": byts, "achieved_gbs": round(byts / ms_elem / 1e6, 1),
                                           "peak_gbs": peak, "frac": round(byts / ms_elem / 1e6 / peak, 4),
                                           "peak_kind": f"{kind} HBM copy"}}

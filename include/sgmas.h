@@ -295,6 +295,21 @@ int sgmas_assemble(sgmas_context* ctx, const double* d_values, int n, double* d_
  * sgmas_write_upper_blocks of each group followed by sgmas_convert.  A later
  * sgmas_assembly_plan replaces the element plan.  The project's own (the
  * reference writes triplets and sorts them every step). */
+/* The contact terms of a step into an assembled system: a sorted append.
+ * d_base_* is a merged block list sorted by (row, col) with n_base blocks
+ * (what sgmas_convert, sgmas_assemble or sgmas_element_assemble return); the
+ * n raw triplets d_values / d_rows / d_cols (this step's contact blocks, e.g.
+ * from sgmas_write_upper_blocks) are sorted on their own, each (row, col) run
+ * is added to the base block with that key or becomes a new block, and the
+ * union goes to d_out_* sorted (room for n_base + n blocks; the outputs must
+ * not overlap the inputs), *n_out blocks.  Bit-identical to sgmas_convert of
+ * the base's own raw triplets followed by these n.  The project's own (the
+ * reference converts all triplets every step). */
+int sgmas_append_triplets(sgmas_context* ctx, const double* d_base_values, const int* d_base_rows,
+                          const int* d_base_cols, int n_base, const double* d_values, const int* d_rows,
+                          const int* d_cols, int n, double* d_out_values, int* d_out_rows, int* d_out_cols,
+                          int* n_out);
+
 typedef struct sgmas_element_group {
     const double* d_H;
     const int* d_nodes;

@@ -1,5 +1,6 @@
 // capi.cu -- the extern "C" boundary (include/sgmas.h).  Every entry point
 // validates its arguments, returns a status and never aborts.
+#include <climits>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -489,6 +490,22 @@ int sgmas_assemble(sgmas_context* c, const double* d_values, int n, double* d_ou
     if (!c || n < 0 || (n > 0 && (!d_values || !d_out_values))) return SGMAS_ERR_ARG;
     SG_CUDA(c, cudaSetDevice(c->device));
     return assemble_planned(c, d_values, n, d_out_values);
+}
+
+int sgmas_append_triplets(sgmas_context* c, const double* d_base_values, const int* d_base_rows,
+                          const int* d_base_cols, int n_base, const double* d_values, const int* d_rows,
+                          const int* d_cols, int n, double* d_out_values, int* d_out_rows, int* d_out_cols,
+                          int* n_out) {
+    if (!c || !n_out || n_base < 0 || n < 0) return SGMAS_ERR_ARG;
+    if ((n_base > 0 && (!d_base_values || !d_base_rows || !d_base_cols)) || (n > 0 && (!d_values || !d_rows || !d_cols)) ||
+        (n_base + n > 0 && (!d_out_values || !d_out_rows || !d_out_cols)))
+        return SGMAS_ERR_ARG;
+    if ((long long)n_base + n > INT_MAX) return ctx_fail(c, SGMAS_ERR_ARG, "sgmas_append_triplets: more than 2^31 - 1 blocks");
+    SG_CUDA(c, cudaSetDevice(c->device));
+    int rc = append_triplets(c, d_base_values, d_base_rows, d_base_cols, n_base, d_values, d_rows, d_cols, n,
+                             d_out_values, d_out_rows, d_out_cols, n_out);
+    if (rc) return rc;
+    return check_device_error(c, "sgmas_append_triplets");
 }
 
 int sgmas_element_plan(sgmas_context* c, const sgmas_element_group* groups, int n_groups, int* d_out_rows,

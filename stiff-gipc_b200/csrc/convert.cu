@@ -286,6 +286,88 @@ __global__ void k_elem_seg_sum(int nu, int n, const int* __restrict__ start, con
     out[9 * (size_t)u + a + 6] = s2;
 }
 
+// ---- sorted append: raw triplets into a merged, sorted structure ----------
+__device__ __forceinline__ bool key_less(int r0, int c0, int r1, int c1) {
+    return r0 < r1 || (r0 == r1 && c0 < c1);
+}
+
+// for each distinct appended key u: lb[u] = its insertion point among the base
+// blocks (first base block not below it), nw[u] = 1 when no base block has it
+__global__ void k_append_locate(int nu, const int* __restrict__ urow, const int* __restrict__ ucol,
+                                const int* __restrict__ brow, const int* __restrict__ bcol, int nb, int* lb, int* nw) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= nu) return;
+    const int r = urow[u], c = ucol[u];
+    int lo = 0, hi = nb;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (key_less(brow[mid], bcol[mid], r, c)) lo = mid + 1;
+        else hi = mid;
+    }
+    lb[u] = lo;
+    nw[u] = !(lo < nb && brow[lo] == r && bcol[lo] == c);
+}
+
+// insertion points of the new keys, in order (non-decreasing)
+__global__ void k_append_compact(int nu, const int* __restrict__ lb, const int* __restrict__ nw,
+                                 const int* __restrict__ rank, int* nlb) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u < nu && nw[u]) nlb[rank[u]] = lb[u];
+}
+
+// output place of base block j: j + the new keys inserted at or before it
+__device__ __forceinline__ int base_place(int j, const int* __restrict__ nlb, int nnew) {
+    int lo = 0, hi = nnew;  // upper bound of j in nlb
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (nlb[mid] <= j) lo = mid + 1;
+        else hi = mid;
+    }
+    return j + lo;
+}
+
+// every base block to its output place (nine threads per block, one per component)
+__global__ void k_append_base(int nb, const double* __restrict__ bval, const int* __restrict__ brow,
+                              const int* __restrict__ bcol, const int* __restrict__ nlb, int nnew, double* oval,
+                              int* orow, int* ocol) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 9LL * nb) return;
+    const int j = (int)(t / 9), q = (int)(t % 9);
+    const int o = base_place(j, nlb, nnew);
+    oval[9 * (size_t)o + q] = bval[9 * (size_t)j + q];
+    if (q == 0) { orow[o] = brow[j]; ocol[o] = bcol[j]; }
+}
+
+// every distinct appended key: the base block's value (when the base has the
+// key) followed by the key's run in sorted (stable) order, summed in that
+// order -- the order of a convert of the base's triplets followed by these
+__global__ void k_append_sum(int nu, int n, const int* __restrict__ start, const uint32_t* __restrict__ idx,
+                             const double* __restrict__ vals, const int* __restrict__ urow,
+                             const int* __restrict__ ucol, const int* __restrict__ lb, const int* __restrict__ nw,
+                             const int* __restrict__ rank, const int* __restrict__ nlb, int nnew,
+                             const double* __restrict__ bval, double* oval, int* orow, int* ocol) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 9LL * nu) return;
+    const int u = (int)(t / 9), q = (int)(t % 9);
+    const int b = start[u], e = (u + 1 < nu) ? start[u + 1] : n;
+    const bool fresh = nw[u] != 0;
+    const int o = fresh ? lb[u] + rank[u] : base_place(lb[u], nlb, nnew);
+    double s = fresh ? 0.0 : bval[9 * (size_t)lb[u] + q];
+    for (int i0 = b; i0 < e; i0 += kSegBatch) {
+        uint32_t ix[kSegBatch];
+        double v[kSegBatch];
+        #pragma unroll
+        for (int j = 0; j < kSegBatch; ++j) ix[j] = i0 + j < e ? idx[i0 + j] : 0u;
+        #pragma unroll
+        for (int j = 0; j < kSegBatch; ++j) v[j] = i0 + j < e ? vals[9 * (size_t)ix[j] + q] : 0.0;
+        #pragma unroll
+        for (int j = 0; j < kSegBatch; ++j)
+            if (i0 + j < e) s = (fresh && i0 + j == b) ? v[j] : s + v[j];
+    }
+    oval[9 * (size_t)o + q] = s;
+    if (q == 0 && fresh) { orow[o] = urow[u]; ocol[o] = ucol[u]; }
+}
+
 // upper triplets of element matrices: one thread per (element, block pair)
 __global__ void k_upper_blocks(int n_elem, int k, const double* __restrict__ H, const int* __restrict__ nodes,
                                double* vals, int* rows, int* cols) {
@@ -490,6 +572,71 @@ int convert_triplets(sgmas_context* c, const double* vals, const int* rows, cons
     k_seg_sum<<<(int)((9LL * nu + kT - 1) / kT), kT, 0, s>>>(nu, n, start, idx, vals, out_vals);
     SG_CUDA(c, cudaGetLastError());
     *n_unique = nu;
+    return 0;
+}
+
+// Sorted append: the n raw triplets are sorted and merged on their own (the
+// steps of convert_triplets up to the segment starts), each distinct key is
+// located among the n_base sorted base blocks, and the union is written in
+// order: base blocks shifted by the new keys before them, then every appended
+// key's sum (base value first when the base has the key).
+int append_triplets(sgmas_context* c, const double* bval, const int* brow, const int* bcol, int nb,
+                    const double* vals, const int* rows, const int* cols, int n, double* oval, int* orow, int* ocol,
+                    int* n_out) {
+    *n_out = 0;
+    cudaStream_t s = c->stream;
+    const int nn = std::max(n, 1);
+    const size_t need = (size_t)nn * (8 + 4 * 11) + sort_scratch_size(nn) + 16384;
+    if (ensure_scratch(c, need)) return SGMAS_ERR_CUDA;
+    Scratch S{(unsigned char*)c->d_sort_scratch, 0};
+    uint64_t* keys = S.take<uint64_t>(nn);
+    uint32_t* idx = S.take<uint32_t>(nn);
+    int* head = S.take<int>(nn);
+    int* seg = S.take<int>(nn);
+    int* start = S.take<int>(nn);
+    int* urow = S.take<int>(nn);
+    int* ucol = S.take<int>(nn);
+    int* lb = S.take<int>(nn);
+    int* nw = S.take<int>(nn);
+    int* rank = S.take<int>(nn);
+    int* nlb = S.take<int>(nn);
+    int* misc = S.take<int>(4);
+    int* sums = S.take<int>((nn + 1023) / 1024 + 1);
+    int nu = 0, nnew = 0;
+    if (n > 0) {
+        SG_CUDA(c, cudaMemsetAsync(misc, 0, sizeof(int) * 4, s));
+        k_max_index<<<min(1024, (n + kT - 1) / kT), kT, 0, s>>>(n, rows, cols, misc);
+        int mx = 0;
+        SG_CUDA(c, cudaMemcpyAsync(&mx, misc, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SG_CUDA(c, cudaStreamSynchronize(s));
+        int cb = 1;
+        while ((1ll << cb) <= (long long)mx) ++cb;
+        const int g = (n + kT - 1) / kT;
+        k_make_keys<<<g, kT, 0, s>>>(n, rows, cols, cb, keys, idx, c->d_err);
+        int rc = sort_pairs_impl(c, keys, idx, n, 2 * cb, S);
+        if (rc) return rc;
+        k_heads<<<g, kT, 0, s>>>(n, keys, head);
+        if ((rc = scan_ints(c, head, seg, n, sums, misc + 1))) return rc;
+        int h2[2];
+        SG_CUDA(c, cudaMemcpyAsync(h2, misc, sizeof(int) * 2, cudaMemcpyDeviceToHost, s));
+        SG_CUDA(c, cudaStreamSynchronize(s));
+        nu = h2[1];
+        k_seg_starts<<<g, kT, 0, s>>>(n, keys, head, seg, cb, start, urow, ucol);
+        const int gu = (nu + kT - 1) / kT;
+        k_append_locate<<<gu, kT, 0, s>>>(nu, urow, ucol, brow, bcol, nb, lb, nw);
+        if ((rc = scan_ints(c, nw, rank, nu, sums, misc + 2))) return rc;
+        SG_CUDA(c, cudaMemcpyAsync(&nnew, misc + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SG_CUDA(c, cudaStreamSynchronize(s));
+        k_append_compact<<<gu, kT, 0, s>>>(nu, lb, nw, rank, nlb);
+    }
+    if (nb > 0)
+        k_append_base<<<(int)((9LL * nb + kT - 1) / kT), kT, 0, s>>>(nb, bval, brow, bcol, nlb, nnew, oval, orow,
+                                                                      ocol);
+    if (nu > 0)  // after the base copy: the shared keys' blocks are rewritten with their sums
+        k_append_sum<<<(int)((9LL * nu + kT - 1) / kT), kT, 0, s>>>(nu, n, start, idx, vals, urow, ucol, lb, nw, rank,
+                                                                     nlb, nnew, bval, oval, orow, ocol);
+    SG_CUDA(c, cudaGetLastError());
+    *n_out = nb + nnew;
     return 0;
 }
 

@@ -246,6 +246,9 @@ int bsr_build(sgmas_context* c, const double* vals, const int* rows, const int* 
 int assembly_plan(sgmas_context* c, const int* rows, const int* cols, int n, int* out_rows, int* out_cols,
                   int* n_unique);
 int assemble_planned(sgmas_context* c, const double* vals, int n, double* out_vals);
+int append_triplets(sgmas_context* c, const double* bval, const int* brow, const int* bcol, int nb,
+                    const double* vals, const int* rows, const int* cols, int n, double* oval, int* orow, int* ocol,
+                    int* n_out);
 int element_plan(sgmas_context* c, const sgmas_element_group* groups, int ng, int* out_rows, int* out_cols,
                  int* n_unique);
 int element_assemble(sgmas_context* c, const sgmas_element_group* groups, int ng, double* out_vals);

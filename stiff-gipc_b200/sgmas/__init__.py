@@ -73,7 +73,7 @@ EXPORTS = [
     "sgmas_part_maps", "sgmas_morton_codes_noalloc", "sgmas_set_pcg_mode", "sgmas_pcg_last_vectors",
     "sgmas_mtx_write", "sgmas_mtx_read", "sgmas_set_pcg_ctas", "sgmas_set_wait_limit", "sgmas_mlp_set_params", "sgmas_mlp_get_params", "sgmas_mlp_features",
     "sgmas_mlp_gradient", "sgmas_mlp_train_step", "sgmas_mlp_forward", "sgmas_mlp_warm_start",
-    "sgmas_autotune_pcg", "sgmas_assembly_plan", "sgmas_assemble", "sgmas_element_plan", "sgmas_element_assemble", "sgmas_abd_body_blocks",
+    "sgmas_autotune_pcg", "sgmas_assembly_plan", "sgmas_assemble", "sgmas_element_plan", "sgmas_element_assemble", "sgmas_append_triplets", "sgmas_abd_body_blocks",
     "sgmas_abd_pair_blocks", "sgmas_abd_fem_blocks",
 ]
 MLP_PARAMS = 19462  # SGMAS_MLP_PARAMS in include/sgmas.h
@@ -126,6 +126,7 @@ def lib(build_if_missing: bool = False):
     L.sgmas_assembly_plan.argtypes = [vp, vp, vp, i, vp, vp, C.POINTER(i)]
     L.sgmas_assemble.argtypes = [vp, vp, i, vp]
     L.sgmas_element_plan.argtypes = [vp, C.POINTER(ElementGroup), i, vp, vp, C.POINTER(i)]
+    L.sgmas_append_triplets.argtypes = [vp, vp, vp, vp, i, vp, vp, vp, i, vp, vp, vp, C.POINTER(i)]
     L.sgmas_element_assemble.argtypes = [vp, C.POINTER(ElementGroup), i, vp]
     L.sgmas_abd_body_blocks.argtypes = [vp, vp, i, vp, vp, vp]
     L.sgmas_abd_pair_blocks.argtypes = [vp, vp, vp, vp, i, vp, vp, vp, vp, vp, vp]
@@ -499,6 +500,17 @@ class Context:
                                                 int(in_rows.shape[0]), _ptr(xbar), _ptr(body_of), _ptr(fixed),
                                                 _ptr(fem_boundary), int(fem_point_offset), int(n_bodies), _ptr(vals),
                                                 _ptr(rows), _ptr(cols)))
+
+    def append_triplets(self, base_vals, base_rows, base_cols, n_base, vals, rows, cols, out_vals, out_rows,
+                        out_cols):
+        """Sorted append (sgmas_append_triplets): raw triplets merged into a
+        sorted merged block list; returns the output count."""
+        no = C.c_int()
+        n = int(rows.shape[0]) if rows is not None else 0
+        self._check(self.L.sgmas_append_triplets(self.h, _ptr(base_vals), _ptr(base_rows), _ptr(base_cols),
+                                                 int(n_base), _ptr(vals), _ptr(rows), _ptr(cols), n, _ptr(out_vals),
+                                                 _ptr(out_rows), _ptr(out_cols), C.byref(no)))
+        return no.value
 
     def element_plan(self, nodes_list, out_rows, out_cols):
         """Plan the merged structure of element groups (sgmas_element_plan):

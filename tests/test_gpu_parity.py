@@ -601,6 +601,53 @@ def test_element_assembly_matches_convert(sgm, name):
     ctx.close()
 
 
+def test_sorted_append_matches_convert(sgm):
+    """Contact blocks appended to the assembled elastic system (mass +
+    tets): the union equals sgmas_convert of all raw triplets (elastic first,
+    then the contact pairs' blocks) bit for bit -- shared keys (the contact
+    vertices' diagonal and in-block couplings) and new keys (couplings across
+    the two blocks) alike; an empty append copies the base; an empty base is
+    the convert of the appended triplets."""
+    s = synth.config2(seed=5, scale=0.3, keep_raw=True)
+    nc = 10 * len(s.pairs)
+    n = len(s.raw_rows)
+    ne = n - nc
+    ctx = sgm.Context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    z = lambda m, w=None: torch.zeros((m, 9) if w else m, dtype=torch.float64 if w else torch.int32, device="cuda")
+
+    def convert(v, r, c):
+        ov, orr, oc = z(len(r), 9), z(len(r)), z(len(r))
+        k = ctx.convert(dev(v), dev(r), dev(c), ov, orr, oc)
+        return ov[:k], orr[:k], oc[:k]
+
+    bv, br, bc = convert(s.raw_vals[:ne], s.raw_rows[:ne], s.raw_cols[:ne])
+    av, ar, ac = convert(s.raw_vals, s.raw_rows, s.raw_cols)
+    m = len(br) + nc
+    ov, orr, oc = z(m, 9), z(m), z(m)
+    k = ctx.append_triplets(bv, br, bc, len(br), dev(s.raw_vals[ne:]), dev(s.raw_rows[ne:]), dev(s.raw_cols[ne:]),
+                            ov, orr, oc)
+    torch.cuda.synchronize()
+    assert k == len(ar) and k > len(br)   # the pairs add keys across the two blocks
+    np.testing.assert_array_equal(orr[:k].cpu().numpy(), ar.cpu().numpy())
+    np.testing.assert_array_equal(oc[:k].cpu().numpy(), ac.cpu().numpy())
+    np.testing.assert_array_equal(ov[:k].cpu().numpy().view(np.uint64), av.cpu().numpy().view(np.uint64))
+    # nothing appended: the base, in place
+    k0 = ctx.append_triplets(bv, br, bc, len(br), None, None, None, ov, orr, oc)
+    torch.cuda.synchronize()
+    assert k0 == len(br)
+    np.testing.assert_array_equal(ov[:k0].cpu().numpy().view(np.uint64), bv.cpu().numpy().view(np.uint64))
+    # no base: the convert of the appended triplets
+    cv, cr, cc = convert(s.raw_vals[ne:], s.raw_rows[ne:], s.raw_cols[ne:])
+    k1 = ctx.append_triplets(None, None, None, 0, dev(s.raw_vals[ne:]), dev(s.raw_rows[ne:]), dev(s.raw_cols[ne:]),
+                             ov, orr, oc)
+    torch.cuda.synchronize()
+    assert k1 == len(cr)
+    np.testing.assert_array_equal(orr[:k1].cpu().numpy(), cr.cpu().numpy())
+    np.testing.assert_array_equal(ov[:k1].cpu().numpy().view(np.uint64), cv.cpu().numpy().view(np.uint64))
+    ctx.close()
+
+
 def test_assemble_before_plan_refused(sgm):
     ctx = sgm.Context(0)
     with pytest.raises(sgm.SgmasError):
