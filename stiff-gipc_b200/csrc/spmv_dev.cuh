@@ -26,6 +26,24 @@ __device__ __forceinline__ double ldv(const double* p) {
     return *p;
 }
 
+// a lane's two blocks (v[q].x, v[q].y: row-major component q) times their
+// vector entries x0, x1, added to the row sums with explicit fused
+// multiply-adds in a fixed order, so every SpMV form gives the same bits
+__device__ __forceinline__ void acc_pair(const double2 (&v)[9], const double (&x0)[3], const double (&x1)[3],
+                                         double& a0, double& a1, double& a2) {
+    double* acc[3] = {&a0, &a1, &a2};
+    #pragma unroll
+    for (int r = 0; r < 3; ++r) {  // the pair's six products left to right, then into the row sum
+        double t = __dmul_rn(v[3 * r].x, x0[0]);
+        t = __fma_rn(v[3 * r + 1].x, x0[1], t);
+        t = __fma_rn(v[3 * r + 2].x, x0[2], t);
+        t = __fma_rn(v[3 * r].y, x1[0], t);
+        t = __fma_rn(v[3 * r + 1].y, x1[1], t);
+        t = __fma_rn(v[3 * r + 2].y, x1[2], t);
+        *acc[r] = __dadd_rn(*acc[r], t);
+    }
+}
+
 // lanes per short row (a warp takes 32 / kRowLanes short rows at once)
 constexpr int kRowLanes = 8;
 constexpr int kRowGroups = 32 / kRowLanes;
@@ -95,9 +113,7 @@ __device__ __forceinline__ double spmv_unit_d(const BsrView& A, int4 desc, int l
                     x1[d] = ldv<LIVE>(xin + 3 * (size_t)cc.y + d);
                 }
             }
-            a0 += v[0].x * x0[0] + v[1].x * x0[1] + v[2].x * x0[2] + v[0].y * x1[0] + v[1].y * x1[1] + v[2].y * x1[2];
-            a1 += v[3].x * x0[0] + v[4].x * x0[1] + v[5].x * x0[2] + v[3].y * x1[0] + v[4].y * x1[1] + v[5].y * x1[2];
-            a2 += v[6].x * x0[0] + v[7].x * x0[1] + v[8].x * x0[2] + v[6].y * x1[0] + v[7].y * x1[1] + v[8].y * x1[2];
+            acc_pair(v, x0, x1, a0, a1, a2);
         }
         if (longw) {  // warp-uniform branch
             #pragma unroll
@@ -162,10 +178,8 @@ __device__ __forceinline__ double spmv_unit_h(const BsrView& A, int4 desc, int l
         for (int q = 0; q < 9; ++q) v[q] = __ldg(reinterpret_cast<const double2*>(bvals + q * cap + p));
         const double* h0 = hv + 3 * cc.x;
         const double* h1 = hv + 3 * cc.y;
-        const double x00 = h0[0], x01 = h0[1], x02 = h0[2], x10 = h1[0], x11 = h1[1], x12 = h1[2];
-        a0 += v[0].x * x00 + v[1].x * x01 + v[2].x * x02 + v[0].y * x10 + v[1].y * x11 + v[2].y * x12;
-        a1 += v[3].x * x00 + v[4].x * x01 + v[5].x * x02 + v[3].y * x10 + v[4].y * x11 + v[5].y * x12;
-        a2 += v[6].x * x00 + v[7].x * x01 + v[8].x * x02 + v[6].y * x10 + v[7].y * x11 + v[8].y * x12;
+        const double xa[3] = {h0[0], h0[1], h0[2]}, xb[3] = {h1[0], h1[1], h1[2]};
+        acc_pair(v, xa, xb, a0, a1, a2);
     }
     if (longw) {  // warp-uniform branch
         #pragma unroll
