@@ -566,8 +566,8 @@ def test_element_assembly_matches_convert(sgm, name):
     nu = ctx.element_plan(nodes, pr, pc)
     rng = np.random.default_rng(2)
     for step in range(2):
-        Hs = [np.ascontiguousarray(H * (1.0 + 0.25 * step) + rng.normal(size=H.shape) * 1e-3 * step * np.abs(H).max())
-              for H, _ in groups]
+        Hs = [np.ascontiguousarray(H if step == 0 else
+                                   H * 1.25 + rng.normal(size=H.shape) * 1e-3 * np.abs(H).max()) for H, _ in groups]
         dH = [dev(H) for H in Hs]
         out = torch.zeros((n, 9), dtype=torch.float64, device="cuda")
         ctx.element_assemble(dH, out)
@@ -586,10 +586,12 @@ def test_element_assembly_matches_convert(sgm, name):
         np.testing.assert_array_equal(pr.cpu().numpy()[:nu], cr.cpu().numpy()[:nu])
         np.testing.assert_array_equal(pc.cpu().numpy()[:nu], cc.cpu().numpy()[:nu])
         np.testing.assert_array_equal(out.cpu().numpy()[:nu].view(np.uint64), cv.cpu().numpy()[:nu].view(np.uint64))
-        if step == 0:  # the first step's structure is the system's own merge
+        if step == 0:  # the first step's structure is the system's own merge; values = the oracle's convert
             assert nu == len(s.rows)
             np.testing.assert_array_equal(cr.cpu().numpy()[:nu], s.rows)
             np.testing.assert_array_equal(cc.cpu().numpy()[:nu], s.cols)
+            _, _, v_o = O.convert(s.raw_vals, s.raw_rows, s.raw_cols)
+            np.testing.assert_array_equal(out.cpu().numpy()[:nu].view(np.uint64), v_o.view(np.uint64))
     with pytest.raises(sgm.SgmasError):  # other group counts than planned
         ctx.element_assemble(dH[:-1], out)
     with pytest.raises(sgm.SgmasError):
@@ -632,6 +634,10 @@ def test_sorted_append_matches_convert(sgm):
     np.testing.assert_array_equal(orr[:k].cpu().numpy(), ar.cpu().numpy())
     np.testing.assert_array_equal(oc[:k].cpu().numpy(), ac.cpu().numpy())
     np.testing.assert_array_equal(ov[:k].cpu().numpy().view(np.uint64), av.cpu().numpy().view(np.uint64))
+    # and the oracle's converter of all triplets, directly
+    r_o, c_o, v_o = O.convert(s.raw_vals, s.raw_rows, s.raw_cols)
+    np.testing.assert_array_equal(orr[:k].cpu().numpy(), r_o)
+    np.testing.assert_array_equal(ov[:k].cpu().numpy().view(np.uint64), v_o.view(np.uint64))
     # nothing appended: the base, in place
     k0 = ctx.append_triplets(bv, br, bc, len(br), None, None, None, ov, orr, oc)
     torch.cuda.synchronize()
