@@ -1181,37 +1181,44 @@ int or_mas_apply(or_mas* m, const double* r, double* z)
     const size_t bsym = (size_t)m->bsym;
     if(is_factored(m->precision))
     {
-        /* factored tiles: y = W r (J <= I), z = W^T y (J >= I), J ascending */
+        /* factored tiles: y = W r (J <= I), z = W^T y (J >= I), J ascending
+           within each part; with M = b / 2, pass 1 sums a row I >= M as
+           (J < M) + (M <= J <= I) and pass 2 a row I < M as (I <= J < M) +
+           (J >= M), each part its own chain from 0, the two added last (the
+           library's lane-balanced order) */
+        const int M = b / 2;
 #pragma omp parallel for schedule(static)
         for(int B = 0; B < T / b; B++)
         {
             float y[32][3];
             for(int rl = 0; rl < b; rl++)
             {
-                float a[3] = {0, 0, 0};
+                float a[3] = {0, 0, 0}, h[3] = {0, 0, 0};
                 for(int cl = 0; cl <= rl; cl++)
                 {
                     const float* P = m->inv32 + ((size_t)B * bsym + sym_index(b, cl, rl)) * 9;
                     const float* x = R32 + 3 * (size_t)(B * b + cl);
+                    float* acc = (rl >= M && cl >= M) ? h : a;
                     for(int d = 0; d < 3; d++)
                         for(int k = 0; k < 3; k++)
-                            a[d] = fmaf(P[d + 3 * k], x[k], a[d]);
+                            acc[d] = fmaf(P[d + 3 * k], x[k], acc[d]);
                 }
                 for(int d = 0; d < 3; d++)
-                    y[rl][d] = a[d];
+                    y[rl][d] = rl >= M ? a[d] + h[d] : a[d];
             }
             for(int rl = 0; rl < b; rl++)
             {
-                float a[3] = {0, 0, 0};
+                float a[3] = {0, 0, 0}, l[3] = {0, 0, 0};
                 for(int cl = rl; cl < b; cl++)
                 {
                     const float* P = m->inv32 + ((size_t)B * bsym + sym_index(b, rl, cl)) * 9;
+                    float* acc = (rl < M && cl < M) ? l : a;
                     for(int d = 0; d < 3; d++)
                         for(int k = 0; k < 3; k++)
-                            a[d] = fmaf(P[k + 3 * d], y[cl][k], a[d]);
+                            acc[d] = fmaf(P[k + 3 * d], y[cl][k], acc[d]);
                 }
                 for(int d = 0; d < 3; d++)
-                    Z32[3 * ((size_t)B * b + rl) + d] = a[d];
+                    Z32[3 * ((size_t)B * b + rl) + d] = rl < M ? l[d] + a[d] : a[d];
             }
         }
     }

@@ -55,57 +55,75 @@ __device__ __forceinline__ void xch_get4(const double* xb, int c0, double (&v)[1
 
 // Factored tile (Fact<T>): slot sym_index(J, I), J <= I, holds the 3x3
 // block (I, J) of W = L^-1, column-major.  z = W^T (W r): pass 1 y_I =
-// sum_{J <= I} W_IJ r_J, pass 2 z_I = sum_{J >= I} W_JI^T y_J, J ascending,
-// each component an fma chain (the order the oracle restates).  xb holds r
-// on entry and y on return.
+// sum_{J <= I} W_IJ r_J, pass 2 z_I = sum_{J >= I} W_JI^T y_J, each component
+// an fma chain over J ascending.  The triangles are balanced over the bank's
+// lanes by splitting the long sums at M = B / 2: in pass 1 a row I >= M is
+// (its columns < M) + (its columns >= M), in pass 2 a row I < M is (its
+// columns < M) + (its columns >= M), each part a chain of its own, the two
+// added at the end (the order the oracle restates).  Lane l < M takes row l
+// and then the upper part of row B-1-l in pass 1, its own upper part in
+// pass 2; lane l >= M the reverse; every lane runs M + 1 block steps per pass
+// instead of up to B.  xb holds r on entry and y on return.
+template <typename S, typename Acc>
+__device__ __forceinline__ void fact_step(const S* P, bool tr, Acc x0, Acc x1, Acc x2, Acc& a0, Acc& a1, Acc& a2) {
+    // tr = 0: a += W_block x (element (d, k) at d + 3 k); tr = 1: a += W_block^T x
+    const int s1 = tr ? 1 : 3, s2 = tr ? 3 : 1;
+    a0 = fma_acc(Store<S>::to_acc(P[0]), x0, a0);
+    a0 = fma_acc(Store<S>::to_acc(P[s1]), x1, a0);
+    a0 = fma_acc(Store<S>::to_acc(P[2 * s1]), x2, a0);
+    a1 = fma_acc(Store<S>::to_acc(P[s2]), x0, a1);
+    a1 = fma_acc(Store<S>::to_acc(P[s2 + s1]), x1, a1);
+    a1 = fma_acc(Store<S>::to_acc(P[s2 + 2 * s1]), x2, a1);
+    a2 = fma_acc(Store<S>::to_acc(P[2 * s2]), x0, a2);
+    a2 = fma_acc(Store<S>::to_acc(P[2 * s2 + s1]), x1, a2);
+    a2 = fma_acc(Store<S>::to_acc(P[2 * s2 + 2 * s1]), x2, a2);
+}
+
 template <int B, typename S, typename Acc>
 __device__ __forceinline__ void schwarz_factored(const S* tile, int lane, Acc* xb, Acc& z0, Acc& z1, Acc& z2) {
-    Acc y0 = 0, y1 = 0, y2 = 0;
-    #pragma unroll 2
-    for (int c0 = 0; c0 < B; c0 += 4) {
-        Acc v[12];
-        xch_get4(xb, c0, v);
-        #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int c = c0 + j;
-            if (c <= lane) {
-                const Acc x0 = v[3 * j], x1 = v[3 * j + 1], x2 = v[3 * j + 2];
-                const S* P = tile + sym_index(B, c, lane) * 9;  // block (lane, c)
-                y0 = fma_acc(Store<S>::to_acc(P[0]), x0, y0);
-                y0 = fma_acc(Store<S>::to_acc(P[3]), x1, y0);
-                y0 = fma_acc(Store<S>::to_acc(P[6]), x2, y0);
-                y1 = fma_acc(Store<S>::to_acc(P[1]), x0, y1);
-                y1 = fma_acc(Store<S>::to_acc(P[4]), x1, y1);
-                y1 = fma_acc(Store<S>::to_acc(P[7]), x2, y1);
-                y2 = fma_acc(Store<S>::to_acc(P[2]), x0, y2);
-                y2 = fma_acc(Store<S>::to_acc(P[5]), x1, y2);
-                y2 = fma_acc(Store<S>::to_acc(P[8]), x2, y2);
-            }
+    constexpr int M = B / 2;
+    const bool lo = lane < M;
+    // pass 1: a = the lane's first part, b = its second part (lanes < M only)
+    Acc a0 = 0, a1 = 0, a2 = 0, b0 = 0, b1 = 0, b2 = 0;
+    #pragma unroll 3
+    for (int t = 0; t <= M; ++t) {
+        const bool second = lo && t > lane;
+        const int row = second ? B - 1 - lane : lane;
+        const int c = lo ? (second ? M + t - lane - 1 : t) : t;
+        if (lo || t < M) {
+            const Acc x0 = xb[3 * c], x1 = xb[3 * c + 1], x2 = xb[3 * c + 2];
+            const S* P = tile + sym_index(B, c, row) * 9;  // block (row, c), c <= row
+            Acc c0 = second ? b0 : a0, c1 = second ? b1 : a1, c2 = second ? b2 : a2;
+            fact_step<S, Acc>(P, false, x0, x1, x2, c0, c1, c2);
+            if (second) { b0 = c0; b1 = c1; b2 = c2; } else { a0 = c0; a1 = c1; a2 = c2; }
         }
     }
-    xch_put(xb, lane, y0, y1, y2);
-    Acc a0 = 0, a1 = 0, a2 = 0;
-    #pragma unroll 2
-    for (int c0 = 0; c0 < B; c0 += 4) {
-        Acc v[12];
-        xch_get4(xb, c0, v);
-        #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int c = c0 + j;
-            if (c >= lane) {
-                const Acc w0 = v[3 * j], w1 = v[3 * j + 1], w2 = v[3 * j + 2];
-                const S* P = tile + sym_index(B, lane, c) * 9;  // block (c, lane), used transposed
-                a0 = fma_acc(Store<S>::to_acc(P[0]), w0, a0);
-                a0 = fma_acc(Store<S>::to_acc(P[1]), w1, a0);
-                a0 = fma_acc(Store<S>::to_acc(P[2]), w2, a0);
-                a1 = fma_acc(Store<S>::to_acc(P[3]), w0, a1);
-                a1 = fma_acc(Store<S>::to_acc(P[4]), w1, a1);
-                a1 = fma_acc(Store<S>::to_acc(P[5]), w2, a1);
-                a2 = fma_acc(Store<S>::to_acc(P[6]), w0, a2);
-                a2 = fma_acc(Store<S>::to_acc(P[7]), w1, a2);
-                a2 = fma_acc(Store<S>::to_acc(P[8]), w2, a2);
-            }
+    {  // rows >= M: own lower part + the upper part summed by lane B-1-lane
+        const Acc h0 = shfl_acc(b0, B - 1 - lane, B), h1 = shfl_acc(b1, B - 1 - lane, B),
+                  h2 = shfl_acc(b2, B - 1 - lane, B);
+        if (!lo) { a0 = a0 + h0; a1 = a1 + h1; a2 = a2 + h2; }
+    }
+    xch_put(xb, lane, a0, a1, a2);
+    // pass 2: lane < M: own row's columns >= M; lane >= M: own row (all columns >= lane),
+    // then the columns < M of row B-1-lane
+    a0 = 0; a1 = 0; a2 = 0; b0 = 0; b1 = 0; b2 = 0;
+    #pragma unroll 3
+    for (int t = 0; t <= M; ++t) {
+        const bool second = !lo && t >= B - lane;
+        const int row = second ? B - 1 - lane : lane;
+        const int c = lo ? M + t : (second ? row + t - (B - lane) : lane + t);
+        if (!lo || t < M) {
+            const Acc w0 = xb[3 * c], w1 = xb[3 * c + 1], w2 = xb[3 * c + 2];
+            const S* P = tile + sym_index(B, row, c) * 9;  // block (c, row), used transposed
+            Acc c0 = second ? b0 : a0, c1 = second ? b1 : a1, c2 = second ? b2 : a2;
+            fact_step<S, Acc>(P, true, w0, w1, w2, c0, c1, c2);
+            if (second) { b0 = c0; b1 = c1; b2 = c2; } else { a0 = c0; a1 = c1; a2 = c2; }
         }
+    }
+    {  // rows < M: the lower part summed by lane B-1-lane + own upper part
+        const Acc l0 = shfl_acc(b0, B - 1 - lane, B), l1 = shfl_acc(b1, B - 1 - lane, B),
+                  l2 = shfl_acc(b2, B - 1 - lane, B);
+        if (lo) { a0 = l0 + a0; a1 = l1 + a1; a2 = l2 + a2; }
     }
     z0 = a0; z1 = a1; z2 = a2;
 }
