@@ -722,7 +722,7 @@ int elem_tab(sgmas_context* c, const sgmas_element_group* groups, int ng, bool n
         T.k[g] = G.nodes_per_elem;
         T.off[g + 1] = T.off[g] + (long long)G.n_elem * (G.nodes_per_elem * (G.nodes_per_elem + 1) / 2);
     }
-    if (T.off[ng] > INT_MAX) return ctx_fail(c, SGMAS_ERR_ARG, "%s: more than 2^31 - 1 triplets", fn);
+    if (T.off[ng] > INT_MAX / 2) return ctx_fail(c, SGMAS_ERR_ARG, "%s: more than 2^30 - 1 triplets", fn);
     return 0;
 }
 }  // namespace
