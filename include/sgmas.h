@@ -286,8 +286,9 @@ int sgmas_assemble(sgmas_context* ctx, const double* d_values, int n, double* d_
  * [3k][3k] row-major element matrices, d_nodes [n_elem][k] vertex ids,
  * k = nodes_per_elem in 1..4.  sgmas_element_plan takes 1..4 groups, lays out
  * their upper triplets in the order sgmas_write_upper_blocks writes them
- * (group after group), sorts and merges them as sgmas_assembly_plan does
- * (d_out_rows / d_out_cols need room for all raw triplets), and keeps, for
+ * (group after group; at most 2^30 - 1 of them), sorts and merges them as
+ * sgmas_assembly_plan does (d_out_rows / d_out_cols need room for all raw
+ * triplets), and keeps, for
  * each sorted triplet, where its 3x3 block sits in its group's matrices
  * (d_H is not read).  sgmas_element_assemble then reads that step's element
  * matrices (same groups, counts and nodes as planned; d_nodes is not read)
