@@ -385,7 +385,8 @@ __device__ __forceinline__ bool levels_c(const PArgs& a, const Anc& anc, S* tile
 }
 
 // One SpMV over this CTA's row range: stage the halo (MODE 1: p_new = z +
-// beta p_old from src = z and pold; MODE 2: src = x) in shared memory, then
+// beta p_old from src = z and pold; MODE 2: src = x; MODE 3: x + beta p from
+// src = x and pold = p, y = rhs - A (x + beta p)) in shared memory, then
 // the CTA's work units round-robin over its warps (descriptors cached in
 // shared memory, ud_sm, the first a.upw per warp).
 template <int MODE>
@@ -402,7 +403,7 @@ __device__ __forceinline__ double spmv_cta(const PArgs& a, int4 ci, const int4* 
         for (int d = 0; d < 3; ++d) {
             s0[d] = ldv<true>(src + 3 * (size_t)v + d);
             s0[3 + d] = ldv<true>(src + 3 * (size_t)v2 + d);
-            if (MODE == 1) {
+            if (MODE == 1 || MODE == 3) {
                 q[d] = ldv<true>(pold + 3 * (size_t)v + d);
                 q[3 + d] = ldv<true>(pold + 3 * (size_t)v2 + d);
             }
@@ -413,8 +414,8 @@ __device__ __forceinline__ double spmv_cta(const PArgs& a, int4 ci, const int4* 
                 s0[d] += patch_z(a.pv, v, d);
                 s0[3 + d] += patch_z(a.pv, v2, d);
             }
-            hv[3 * h + d] = MODE == 1 ? __fma_rn(beta, q[d], s0[d]) : s0[d];
-            if (two) hv[3 * h2 + d] = MODE == 1 ? __fma_rn(beta, q[3 + d], s0[3 + d]) : s0[3 + d];
+            hv[3 * h + d] = MODE != 2 ? __fma_rn(beta, q[d], s0[d]) : s0[d];
+            if (two) hv[3 * h2 + d] = MODE != 2 ? __fma_rn(beta, q[3 + d], s0[3 + d]) : s0[3 + d];
         }
     }
     __syncthreads();
@@ -423,7 +424,7 @@ __device__ __forceinline__ double spmv_cta(const PArgs& a, int4 ci, const int4* 
     const int4* ud = ud_sm + w * a.upw * kRowGroups + lane / kRowLanes;
     for (int u = w, i = 0; u < ci.x; u += kPT / 32, ++i) {
         const int4 d = i < a.upw ? ud[kRowGroups * i] : a.udesc_c[(size_t)(ci.w + u) * kRowGroups + lane / kRowLanes];
-        dot += spmv_unit_h<MODE>(a.A, d, lane, a.lcols, hv, pnew, y, rhs);
+        dot += spmv_unit_h<MODE == 3 ? 2 : MODE>(a.A, d, lane, a.lcols, hv, pnew, y, rhs);
     }
     return dot;
 }
@@ -649,7 +650,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         __syncthreads();
     };
     // CollectFinalZ for the owned slot + r.z, r.r partials
-    auto collect = [&](int mode, double alpha, const double* pcur) {
+    auto collect = [&](int mode, double alpha, const double* pcur, bool write_x) {
         double rz = 0.0, rr = 0.0;
         extra_rows_work(a.ex, a.N, mode, alpha, a.x, a.r, pcur, a.Ap, a.z, blockIdx.x * (kPT / 32) + threadIdx.x / 32,
                         gridDim.x * (kPT / 32), threadIdx.x & 31, rz, rr);
@@ -662,6 +663,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             }
             const double z0 = (double)c0, z1 = (double)c1, z2 = (double)c2;
             a.z[vo] = z0; a.z[vo + 1] = z1; a.z[vo + 2] = z2;
+            if (write_x) { a.x[vo] = x0; a.x[vo + 1] = x1; a.x[vo + 2] = x2; }  // the next refresh stages it
             rz += r0 * z0 + r1 * z1 + r2 * z2;
             rr += r0 * r0 + r1 * r1 + r2 * r2;
         }
@@ -754,7 +756,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
             ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, nullptr, nullptr, false);
             if (ok && a.L > 2) ok = levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch);
         }
-        if (ok) collect(0, 0.0, a.p1);
+        if (ok) collect(0, 0.0, a.p1, false);
     } else {
         ok = ok && grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom);
         if (ok) phase_jacobi(a, 0, 0.0, a.p1, part_rz, part_rr, sh);
@@ -800,29 +802,34 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
         }
         const double alpha = rz / pap;
         if (refresh) {
+            // r = b - A x_new with x_new = x + alpha p formed in the halo staging from x in global
+            // memory (the previous iteration's, written by the collect), so no grid barrier is
+            // needed between the x update and the SpMV; the slot's own x is updated with the same
+            // fused multiply-add
+            if (mas && own) {
+                x0 = __fma_rn(alpha, p0v, x0); x1 = __fma_rn(alpha, p1v, x1); x2 = __fma_rn(alpha, p2v, x2);
+            }
+            spmv_cta<3>(a, ci, udesc, hv, hidx, a.x, pnew, alpha, nullptr, a.r, a.b);
+            if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(2))) { ok = false; break; }
+            // rows kept in global memory only (outside the MAS range; every row without MAS): x +=
+            // alpha p once every CTA's staging has read the old x
             if (mas) {
-                if (own) {
-                    x0 += alpha * p0v; x1 += alpha * p1v; x2 += alpha * p2v;
-                    a.x[vo] = x0; a.x[vo + 1] = x1; a.x[vo + 2] = x2;
-                }
-                // rows outside the MAS range
                 const int lo_n = 3 * a.ex.fem_off, hi_n = 3 * (a.ex.fem_off + a.N);
                 for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows - (hi_n - lo_n); i += gridDim.x * kPT) {
                     const int e = i < lo_n ? i : i + (hi_n - lo_n);
-                    a.x[e] = a.x[e] + alpha * pnew[e];
+                    a.x[e] = __fma_rn(alpha, pnew[e], a.x[e]);
                 }
             } else {
                 for (int i = blockIdx.x * kPT + threadIdx.x; i < 3 * a.nrows; i += gridDim.x * kPT)
-                    a.x[i] = a.x[i] + alpha * pnew[i];
+                    a.x[i] = __fma_rn(alpha, pnew[i], a.x[i]);
             }
-            if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(1))) { ok = false; break; }
-            spmv_cta<2>(a, ci, udesc, hv, hidx, a.x, nullptr, 0.0, nullptr, a.r, a.b);
-            if (!grid_barrier(a.sync, epoch, a.err, a.spin_limit, a.phantom, SLOT(2))) { ok = false; break; }
             if (mas && v >= 0) { r0 = a.r[vo]; r1 = a.r[vo + 1]; r2 = a.r[vo + 2]; }
         } else {
             if (mas && v >= 0) {
                 r0 = r0 - alpha * q0; r1 = r1 - alpha * q1; r2 = r2 - alpha * q2;
-                if (own) { x0 += alpha * p0v; x1 += alpha * p1v; x2 += alpha * p2v; }
+                if (own) {
+                    x0 = __fma_rn(alpha, p0v, x0); x1 = __fma_rn(alpha, p1v, x1); x2 = __fma_rn(alpha, p2v, x2);
+                }
                 if (own && a.pv.bodies) { a.r[vo] = r0; a.r[vo + 1] = r1; a.r[vo + 2] = r2; }
             }
             // body rows with patches: updated here, before the patches read them in phase C
@@ -839,7 +846,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PArgs a) {
                 stamp(a, k, 3);
                 if (a.L > 2 && !levels_c<B, S, Acc>(a, anc, tilesC, Rc, Zc, parc, &mbar, mphase, xch)) ok = false;
             }
-            collect(refresh ? 0 : 1, alpha, pnew);
+            collect(refresh ? 0 : 1, alpha, pnew, k % 10 == 9);
         } else {
             phase_jacobi(a, refresh ? 0 : 1, alpha, pnew, part_rz, part_rr, sh);
         }
